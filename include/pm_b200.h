@@ -1,0 +1,199 @@
+/*
+ * pm_b200.h -- C ABI of the B200 particle-mesh step.
+ *
+ * One periodic box of ng^3 cells, particles in cell units [0, ng).  Every
+ * entry point returns an int status (PM_OK = 0); pm_last_error() gives the
+ * message of the calling thread's last failure.  All array arguments are
+ * DEVICE pointers unless the name says host; work is enqueued on the plan's
+ * stream and is asynchronous.  A plan is not thread-safe.
+ *
+ * Mesh layouts (row-major, z fastest):
+ *   mesh      real  [ng][ng][ng+2]     the reference's FFTW in-place stride
+ *                                      (src/core/main.cpp:24-28); the last two
+ *                                      z entries are padding
+ *   spectrum  cplx  [ng][ng][ng/2+1]   the same bytes after pm_fft_r2c*,
+ *                                      kx major, kz fastest
+ *   force     real  [ng][ng][ng]       one array per component
+ *
+ * Reference step (src/core/main.cpp:90-139) and the entry points that
+ * replace its stages:
+ *   init_buf + deposit_particles + reduce_private_to_shared +
+ *   TransposeSlab + ReorderSlab                 -> pm_deposit_f64
+ *   FFT::forward                                -> pm_fft_r2c_f64
+ *   FFT::apply_green                            -> pm_green_f64
+ *   FFT::backward                               -> pm_fft_c2r_f64
+ *   ReorderSlabBack + TransposeSlabBack +
+ *   centered_derivatives                        -> pm_gradient_f64
+ *   update_particles                            -> pm_interp_kick_f64
+ * On one GPU the MPI exchanges disappear: ghost planes become periodic
+ * index wraps inside the kernels.
+ *
+ * Coefficients.  The reference hard-codes its constants
+ * (include/utils/utils_inline.h:13-17).  Here they are arguments:
+ *   c_poisson: phi solves  L phi = c_poisson * delta, L the 7-point
+ *              Laplacian (PM_GREEN_DISCRETE, the reference) or the exact
+ *              -|k|^2 (PM_GREEN_SPECTRAL); the reference value is
+ *              3 Omega_0 / (2 a) with a = 0.9 (src/fft/fftw/fft.cpp:55,79).
+ *   c_kick:    p += c_kick * interpolated force; the reference value is
+ *              Da * function_a(a) (src/utils/utils.cpp:142).
+ */
+#ifndef PM_B200_H
+#define PM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+/* status codes */
+#define PM_OK 0
+#define PM_ERR_ARG 1          /* null pointer, negative count, bad enum   */
+#define PM_ERR_SIZE 2         /* mesh size not supported by this build    */
+#define PM_ERR_CUDA 3         /* CUDA runtime error                        */
+#define PM_ERR_NOMEM 4        /* device allocation failed                  */
+#define PM_ERR_RANGE 5        /* a particle position was NaN or outside
+                                 [0, ng); it was wrapped (NaN -> 0) and the
+                                 step completed.  Reported by pm_plan_check */
+#define PM_ERR_STATE 6        /* call out of order / wrong plan precision  */
+
+/* plan precision */
+#define PM_FP64 0             /* plain FP64 path (reference parity)        */
+#define PM_FP32 1             /* FP32 mesh / FFT / forces, split positions */
+
+/* Green's function */
+#define PM_GREEN_DISCRETE 0   /* inverse 7-point Laplacian (reference)     */
+#define PM_GREEN_SPECTRAL 1   /* -1/|k|^2                                   */
+
+typedef struct pm_plan pm_plan;
+
+/* ------------------------------------------------------------ plans */
+
+/* Creates a plan for an ng^3 mesh.  ng must be a power of two in [8, 1024].
+ * grad_order is 2 (the reference's 2-point centred difference,
+ * src/utils/utils.cpp:115-137) or 4.  stream may be NULL (legacy default
+ * stream).  Replaces the setup of src/core/main.cpp:30-81 and the FFT
+ * constructor src/fft/fftw/fft.cpp:3-59 (plans, Green's table). */
+int pm_plan_create(int ng, int precision, int green_kind, int grad_order, void* stream,
+                   pm_plan** plan);
+int pm_plan_destroy(pm_plan* plan);
+/* Bytes of device memory the plan holds (workspace included). */
+int pm_plan_device_bytes(const pm_plan* plan, size_t* bytes);
+/* Waits for the plan's stream, then returns PM_ERR_RANGE if any kernel since
+ * the last check met a bad position (and clears the flag), else PM_OK. */
+int pm_plan_check(pm_plan* plan);
+/* Message of the calling thread's last failed call ("" if none). */
+const char* pm_last_error(void);
+
+/* ------------------------------------------- FP64 stages (PM_FP64 plan) */
+
+/* delta = -1 + sum_p mass * W_CIC(x_p - c), periodic; writes every cell of
+ * mesh [ng][ng][ng+2] (padding set to 0).
+ * Replaces init_buf, deposit_particles, reduce_private_to_shared
+ * (src/utils/utils.cpp:38-113; cic_deposit include/utils/utils_inline.h:25-49),
+ * TransposeSlab::execute (src/decomp/slab/transpose_slab.cpp:37-39) and
+ * ReorderSlab::execute (src/decomp/slab/reorder_slab.cpp:43-68). */
+int pm_deposit_f64(pm_plan* plan, const double* x, const double* y, const double* z, int64_t np,
+                   double mass, double* mesh);
+
+/* In-place unnormalised R2C, sign -1: mesh -> spectrum.
+ * Replaces FFT::forward (src/fft/fftw/fft.cpp:96; src/fft/ffte1/fft.cpp:61-64). */
+int pm_fft_r2c_f64(pm_plan* plan, double* mesh);
+
+/* spectrum *= G(k) / ng^3 (G per the plan's green_kind, G(0) = 0).
+ * Replaces FFT::apply_green (src/fft/fftw/fft.cpp:75-82) with its table
+ * (fft.cpp:50-57) computed on the fly. */
+int pm_green_f64(pm_plan* plan, double* mesh, double c_poisson);
+
+/* In-place unnormalised C2R, sign +1: spectrum -> mesh (padding zeroed; the
+ * imaginary parts of kz = 0 and kz = ng/2 are ignored, as FFTW does).
+ * Replaces FFT::backward (src/fft/fftw/fft.cpp:97; src/fft/ffte1/fft.cpp:65-68). */
+int pm_fft_c2r_f64(pm_plan* plan, double* mesh);
+
+/* pm_fft_r2c_f64 + pm_green_f64 + pm_fft_c2r_f64 with the x-direction
+ * forward transform, Green multiply and inverse fused into one pass. */
+int pm_poisson_f64(pm_plan* plan, double* mesh, double c_poisson);
+
+/* f = -grad(phi) by the plan's finite difference, periodic.  phi is a mesh
+ * [ng][ng][ng+2]; fx, fy, fz are force arrays [ng][ng][ng].
+ * Replaces ReorderSlabBack::execute (src/decomp/slab/reorder_slab_back.cpp:37-49),
+ * TransposeSlabBack::execute (src/decomp/slab/transpose_slab_back.cpp:47-49)
+ * and centered_derivatives (src/utils/utils.cpp:115-137). */
+int pm_gradient_f64(pm_plan* plan, const double* phi, double* fx, double* fy, double* fz);
+
+/* p += c_kick * (trilinear CIC interpolation of f at x).
+ * Replaces update_particles (src/utils/utils.cpp:141-170; trilerp1
+ * include/utils/utils_inline.h:55-70). */
+int pm_interp_kick_f64(pm_plan* plan, const double* x, const double* y, const double* z,
+                       const double* fx, const double* fy, const double* fz, double* px,
+                       double* py, double* pz, int64_t np, double c_kick);
+
+/* x += dt * p, wrapped into [0, ng).  No counterpart in the reference,
+ * which never moves particles (src/core/main.cpp:90-139). */
+int pm_drift_f64(pm_plan* plan, double* x, double* y, double* z, const double* px,
+                 const double* py, const double* pz, int64_t np, double dt);
+
+/* One full step on the plan's own workspace: deposit, Poisson (r2c, Green,
+ * c2r as separate passes), gradient, interpolate + kick, then drift by dt
+ * (dt = 0: no drift, the reference's step).  The reference's stage loop body,
+ * src/core/main.cpp:91-138. */
+int pm_step_f64(pm_plan* plan, double* x, double* y, double* z, double* px, double* py,
+                double* pz, int64_t np, double mass, double c_poisson, double c_kick, double dt);
+
+/* Device pointer to the plan's own mesh [ng][ng][ng+2] (density after the
+ * deposit of pm_step_*, potential after it returns). */
+int pm_plan_mesh(pm_plan* plan, void** mesh);
+
+/* ---------------------------------- FP32 split-position path (PM_FP32 plan)
+ * Positions are an integer cell plus an FP32 in-cell offset in [0, 1):
+ *   cell = (ix << 20) | (iy << 10) | iz, offsets ox, oy, oz.
+ * Velocities / momenta are FP32.  The drift is accumulated in FP64. */
+
+int pm_split_positions(pm_plan* plan, const double* x, const double* y, const double* z,
+                       int64_t np, uint32_t* cell, float* ox, float* oy, float* oz);
+int pm_join_positions(pm_plan* plan, const uint32_t* cell, const float* ox, const float* oy,
+                      const float* oz, int64_t np, double* x, double* y, double* z);
+
+/* FP32 counterparts of the stages above; mesh is float [ng][ng][ng+2]. */
+int pm_deposit_f32(pm_plan* plan, const uint32_t* cell, const float* ox, const float* oy,
+                   const float* oz, int64_t np, float mass, float* mesh);
+int pm_fft_r2c_f32(pm_plan* plan, float* mesh);
+int pm_green_f32(pm_plan* plan, float* mesh, double c_poisson);
+int pm_fft_c2r_f32(pm_plan* plan, float* mesh);
+int pm_poisson_f32(pm_plan* plan, float* mesh, double c_poisson);
+/* Forces at the particles, gradient fused into the gather: f* [np] FP32. */
+int pm_interp_f32(pm_plan* plan, const float* phi, const uint32_t* cell, const float* ox,
+                  const float* oy, const float* oz, int64_t np, float* fx, float* fy, float* fz);
+/* v += c_kick * force(x) then x += dt * v (FP64 accumulation, re-split);
+ * gradient, interpolation, kick and drift in one pass over the particles. */
+int pm_kick_drift_f32(pm_plan* plan, const float* phi, uint32_t* cell, float* ox, float* oy,
+                      float* oz, float* vx, float* vy, float* vz, int64_t np, double c_kick,
+                      double dt);
+/* One full FP32 step on the plan's workspace: deposit, fused Poisson,
+ * kick + drift. */
+int pm_step_f32(pm_plan* plan, uint32_t* cell, float* ox, float* oy, float* oz, float* vx,
+                float* vy, float* vz, int64_t np, float mass, double c_poisson, double c_kick,
+                double dt);
+
+/* ---------------------------------------------- initial conditions (new)
+ * Zel'dovich particles on an nrow^3 lattice q = (i + 1/2) ng/nrow from a
+ * Gaussian random field with P(k) ~ k^n_s, scaled to an rms 3D displacement
+ * of rms_cells; velocities = vel_factor * displacement.  Lagrangian order,
+ * z fastest.  FP64, generated on the device (needs ~4 nrow^3 doubles of
+ * temporary device memory).  The reference draws uniform positions only
+ * (src/utils/utils.cpp:22-36). */
+int pm_ic_zeldovich(int ng, int nrow, double n_s, double rms_cells, uint64_t seed,
+                    double vel_factor, double* x, double* y, double* z, double* vx, double* vy,
+                    double* vz, void* stream);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+#ifdef __cplusplus
+}
+#endif
+#endif /* PM_B200_H */

@@ -1,0 +1,102 @@
+"""ctypes binding of the C ABI in include/pm_b200.h (libpm_b200.so).
+
+The library is the CUDA build of this package; there is no CPU fallback.
+Loading fails loudly when the library is missing and cannot be built.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpm_b200.so")
+
+PM_OK, PM_ERR_ARG, PM_ERR_SIZE, PM_ERR_CUDA, PM_ERR_NOMEM, PM_ERR_RANGE, PM_ERR_STATE = range(7)
+PM_FP64, PM_FP32 = 0, 1
+PM_GREEN_DISCRETE, PM_GREEN_SPECTRAL = 0, 1
+
+_STATUS = {PM_ERR_ARG: "PM_ERR_ARG", PM_ERR_SIZE: "PM_ERR_SIZE", PM_ERR_CUDA: "PM_ERR_CUDA",
+           PM_ERR_NOMEM: "PM_ERR_NOMEM", PM_ERR_RANGE: "PM_ERR_RANGE", PM_ERR_STATE: "PM_ERR_STATE"}
+
+# Every function of the ABI with its argument types (p = pointer / handle).
+_V, _I, _L, _D, _F, _U64, _SZ = (ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_double,
+                                 ctypes.c_float, ctypes.c_uint64, ctypes.c_size_t)
+SIGNATURES = {
+    "pm_plan_create": [_I, _I, _I, _I, _V, ctypes.POINTER(_V)],
+    "pm_plan_destroy": [_V],
+    "pm_plan_device_bytes": [_V, ctypes.POINTER(_SZ)],
+    "pm_plan_check": [_V],
+    "pm_plan_mesh": [_V, ctypes.POINTER(_V)],
+    "pm_deposit_f64": [_V, _V, _V, _V, _L, _D, _V],
+    "pm_fft_r2c_f64": [_V, _V],
+    "pm_green_f64": [_V, _V, _D],
+    "pm_fft_c2r_f64": [_V, _V],
+    "pm_poisson_f64": [_V, _V, _D],
+    "pm_gradient_f64": [_V, _V, _V, _V, _V],
+    "pm_interp_kick_f64": [_V, _V, _V, _V, _V, _V, _V, _V, _V, _V, _L, _D],
+    "pm_drift_f64": [_V, _V, _V, _V, _V, _V, _V, _L, _D],
+    "pm_step_f64": [_V, _V, _V, _V, _V, _V, _V, _L, _D, _D, _D, _D],
+    "pm_split_positions": [_V, _V, _V, _V, _L, _V, _V, _V, _V],
+    "pm_join_positions": [_V, _V, _V, _V, _V, _L, _V, _V, _V],
+    "pm_deposit_f32": [_V, _V, _V, _V, _V, _L, _F, _V],
+    "pm_fft_r2c_f32": [_V, _V],
+    "pm_green_f32": [_V, _V, _D],
+    "pm_fft_c2r_f32": [_V, _V],
+    "pm_poisson_f32": [_V, _V, _D],
+    "pm_interp_f32": [_V, _V, _V, _V, _V, _V, _L, _V, _V, _V],
+    "pm_kick_drift_f32": [_V, _V, _V, _V, _V, _V, _V, _V, _V, _L, _D, _D],
+    "pm_step_f32": [_V, _V, _V, _V, _V, _V, _V, _V, _L, _F, _D, _D, _D],
+    "pm_ic_zeldovich": [_I, _I, _D, _D, _U64, _D, _V, _V, _V, _V, _V, _V, _V],
+}
+
+_lib = None
+
+
+class PMError(RuntimeError):
+    """A C-ABI call returned a status other than PM_OK."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{_STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+def header_symbols() -> list[str]:
+    """Function names declared in include/pm_b200.h."""
+    import re
+    path = os.path.join(os.path.dirname(HERE), "include", "pm_b200.h")
+    with open(path) as f:
+        text = f.read()
+    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(pm_\w+)\s*\(", text, re.M)))
+
+
+def load(build_if_missing: bool = True) -> ctypes.CDLL:
+    """Loads libpm_b200.so (building it with nvcc if absent or stale)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if build_if_missing:
+        import importlib.util
+        spec = importlib.util.spec_from_file_location("_pm_b200_build", os.path.join(HERE, "build.py"))
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        try:
+            mod.build()
+        except Exception as e:  # noqa: BLE001 -- no nvcc: use the library if it exists
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError(f"libpm_b200.so is missing and could not be built: {e}") from e
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} not found (build with particle-mesh_b200/build.py)")
+    L = ctypes.CDLL(LIB_PATH)
+    for name, args in SIGNATURES.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = ctypes.c_int
+    L.pm_last_error.argtypes = []
+    L.pm_last_error.restype = ctypes.c_char_p
+    _lib = L
+    return L
+
+
+def check(rc: int) -> None:
+    if rc != PM_OK:
+        raise PMError(rc, load().pm_last_error().decode(errors="replace"))

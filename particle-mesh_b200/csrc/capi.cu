@@ -1,0 +1,381 @@
+// C ABI of the particle-mesh step (declared in include/pm_b200.h): argument
+// checks, plan lifetime, workspace, and the per-stage / whole-step entry
+// points.  All checks happen on the host before anything is enqueued; a
+// device-side bad position is recorded in the plan's error word and
+// reported by pm_plan_check.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "pm_internal.cuh"
+
+namespace pmb {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+int cuda_fail(cudaError_t e, const char* what) {
+    return fail(PM_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+namespace {
+
+template <typename T> int upload_tables(Plan& p) {
+    using C = typename Cx<T>::t;
+    const int n = p.ng;
+    std::vector<C> tw(n);
+    std::vector<T> lap(n);
+    const long double pi = 3.141592653589793238462643383279502884L;
+    for (int k = 0; k < n; ++k) {
+        const long double a = -2.0L * pi * (long double)k / (long double)n;
+        tw[k] = cmake<C>((T)cosl(a), (T)sinl(a));
+        const long double s = sinl(pi * (long double)k / (long double)n);
+        lap[k] = (T)(2.0L * s * s);
+    }
+    PMB_CUDA_CHECK(cudaMalloc(&p.tw, n * sizeof(C)));
+    PMB_CUDA_CHECK(cudaMalloc(&p.lap1d, n * sizeof(T)));
+    PMB_CUDA_CHECK(cudaMemcpy(p.tw, tw.data(), n * sizeof(C), cudaMemcpyHostToDevice));
+    PMB_CUDA_CHECK(cudaMemcpy(p.lap1d, lap.data(), n * sizeof(T), cudaMemcpyHostToDevice));
+    p.bytes += n * (sizeof(C) + sizeof(T));
+    return PM_OK;
+}
+
+void release(Plan& p) {
+    if (p.tw) cudaFree(p.tw);
+    if (p.lap1d) cudaFree(p.lap1d);
+    if (p.d_err) cudaFree(p.d_err);
+    if (p.mesh) cudaFree(p.mesh);
+    for (void*& f : p.force)
+        if (f) cudaFree(f), f = nullptr;
+    p.tw = p.lap1d = p.mesh = nullptr;
+    p.d_err = nullptr;
+}
+
+int ensure_workspace(Plan& p, bool forces) {
+    const size_t esz = p.precision == PM_FP64 ? sizeof(double) : sizeof(float);
+    if (!p.mesh) {
+        if (cudaMalloc(&p.mesh, mesh_elems(p.ng) * esz) != cudaSuccess) {
+            cudaGetLastError();
+            p.mesh = nullptr;
+            return fail(PM_ERR_NOMEM, "workspace mesh allocation failed");
+        }
+        p.bytes += mesh_elems(p.ng) * esz;
+    }
+    if (forces && !p.force[0]) {
+        const size_t b = (size_t)p.ng * p.ng * p.ng * sizeof(double);
+        for (void*& f : p.force) {
+            if (cudaMalloc(&f, b) != cudaSuccess) {
+                cudaGetLastError();
+                f = nullptr;
+                return fail(PM_ERR_NOMEM, "workspace force allocation failed");
+            }
+            p.bytes += b;
+        }
+    }
+    return PM_OK;
+}
+
+int check_plan(const pm_plan* plan, int precision) {
+    if (!plan) return fail(PM_ERR_ARG, "plan is NULL");
+    if (plan->p.precision != precision)
+        return fail(PM_ERR_STATE, precision == PM_FP64 ? "entry point needs a PM_FP64 plan"
+                                                       : "entry point needs a PM_FP32 plan");
+    return PM_OK;
+}
+
+int check_np(int64_t np, std::initializer_list<const void*> ptrs) {
+    if (np < 0) return fail(PM_ERR_ARG, "negative particle count");
+    if (np > 0)
+        for (const void* q : ptrs)
+            if (!q) return fail(PM_ERR_ARG, "NULL particle array");
+    return PM_OK;
+}
+
+int set_device(const Plan& p) {
+    int cur = -1;
+    if (cudaGetDevice(&cur) != cudaSuccess) return fail(PM_ERR_CUDA, "cudaGetDevice failed");
+    if (cur != p.device) PMB_CUDA_CHECK(cudaSetDevice(p.device));
+    return PM_OK;
+}
+
+}  // namespace
+}  // namespace pmb
+
+using namespace pmb;
+
+#define PM_TRY(expr)                 \
+    do {                             \
+        int _rc = (expr);            \
+        if (_rc != PM_OK) return _rc; \
+    } while (0)
+
+extern "C" {
+
+const char* pm_last_error(void) { return g_last_error.c_str(); }
+
+int pm_plan_create(int ng, int precision, int green_kind, int grad_order, void* stream, pm_plan** out) {
+    if (!out) return fail(PM_ERR_ARG, "output pointer is NULL");
+    *out = nullptr;
+    if (!fft_size_supported(ng)) return fail(PM_ERR_SIZE, "ng must be a power of two in [8, 1024]");
+    if (precision != PM_FP64 && precision != PM_FP32) return fail(PM_ERR_ARG, "unknown precision");
+    if (green_kind != PM_GREEN_DISCRETE && green_kind != PM_GREEN_SPECTRAL) return fail(PM_ERR_ARG, "unknown green_kind");
+    if (grad_order != 2 && grad_order != 4) return fail(PM_ERR_ARG, "grad_order must be 2 or 4");
+    pm_plan* plan = new (std::nothrow) pm_plan();
+    if (!plan) return fail(PM_ERR_NOMEM, "host allocation failed");
+    Plan& p = plan->p;
+    p.ng = ng;
+    p.precision = precision;
+    p.green_kind = green_kind;
+    p.grad_order = grad_order;
+    p.stream = static_cast<cudaStream_t>(stream);
+    int rc = PM_OK;
+    if (cudaGetDevice(&p.device) != cudaSuccess) rc = fail(PM_ERR_CUDA, "no CUDA device");
+    if (rc == PM_OK && cudaDeviceGetAttribute(&p.num_sms, cudaDevAttrMultiProcessorCount, p.device) != cudaSuccess)
+        rc = fail(PM_ERR_CUDA, "cudaDeviceGetAttribute failed");
+    if (rc == PM_OK) rc = precision == PM_FP64 ? upload_tables<double>(p) : upload_tables<float>(p);
+    if (rc == PM_OK) {
+        if (cudaMalloc(&p.d_err, sizeof(int)) != cudaSuccess || cudaMemset(p.d_err, 0, sizeof(int)) != cudaSuccess)
+            rc = fail(PM_ERR_NOMEM, "error word allocation failed");
+    }
+    if (rc == PM_OK) rc = fft_prepare(p);
+    if (rc != PM_OK) {
+        cudaGetLastError();
+        release(p);
+        delete plan;
+        return rc;
+    }
+    *out = plan;
+    return PM_OK;
+}
+
+int pm_plan_destroy(pm_plan* plan) {
+    if (!plan) return PM_OK;
+    set_device(plan->p);
+    cudaStreamSynchronize(plan->p.stream);
+    release(plan->p);
+    delete plan;
+    return PM_OK;
+}
+
+int pm_plan_device_bytes(const pm_plan* plan, size_t* bytes) {
+    if (!plan || !bytes) return fail(PM_ERR_ARG, "NULL argument");
+    *bytes = plan->p.bytes;
+    return PM_OK;
+}
+
+int pm_plan_check(pm_plan* plan) {
+    if (!plan) return fail(PM_ERR_ARG, "plan is NULL");
+    PM_TRY(set_device(plan->p));
+    int h = 0;
+    PMB_CUDA_CHECK(cudaStreamSynchronize(plan->p.stream));
+    PMB_CUDA_CHECK(cudaMemcpy(&h, plan->p.d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    PMB_CUDA_CHECK(cudaMemset(plan->p.d_err, 0, sizeof(int)));
+    if (h & ERRBIT_RANGE) return fail(PM_ERR_RANGE, "a particle position was NaN or outside [0, ng); it was wrapped");
+    return PM_OK;
+}
+
+int pm_plan_mesh(pm_plan* plan, void** mesh) {
+    if (!plan || !mesh) return fail(PM_ERR_ARG, "NULL argument");
+    PM_TRY(set_device(plan->p));
+    PM_TRY(ensure_workspace(plan->p, false));
+    *mesh = plan->p.mesh;
+    return PM_OK;
+}
+
+// ------------------------------------------------------------------ FP64
+
+int pm_deposit_f64(pm_plan* plan, const double* x, const double* y, const double* z, int64_t np,
+                   double mass, double* mesh) {
+    PM_TRY(check_plan(plan, PM_FP64));
+    PM_TRY(check_np(np, {x, y, z}));
+    if (!mesh) return fail(PM_ERR_ARG, "mesh is NULL");
+    PM_TRY(set_device(plan->p));
+    return deposit_f64(plan->p, x, y, z, np, mass, mesh);
+}
+
+int pm_fft_r2c_f64(pm_plan* plan, double* mesh) {
+    PM_TRY(check_plan(plan, PM_FP64));
+    if (!mesh) return fail(PM_ERR_ARG, "mesh is NULL");
+    PM_TRY(set_device(plan->p));
+    return fft_r2c<double>(plan->p, mesh);
+}
+
+int pm_green_f64(pm_plan* plan, double* mesh, double c_poisson) {
+    PM_TRY(check_plan(plan, PM_FP64));
+    if (!mesh) return fail(PM_ERR_ARG, "mesh is NULL");
+    PM_TRY(set_device(plan->p));
+    return green_apply<double>(plan->p, mesh, c_poisson);
+}
+
+int pm_fft_c2r_f64(pm_plan* plan, double* mesh) {
+    PM_TRY(check_plan(plan, PM_FP64));
+    if (!mesh) return fail(PM_ERR_ARG, "mesh is NULL");
+    PM_TRY(set_device(plan->p));
+    return fft_c2r<double>(plan->p, mesh);
+}
+
+int pm_poisson_f64(pm_plan* plan, double* mesh, double c_poisson) {
+    PM_TRY(check_plan(plan, PM_FP64));
+    if (!mesh) return fail(PM_ERR_ARG, "mesh is NULL");
+    PM_TRY(set_device(plan->p));
+    return poisson_fused<double>(plan->p, mesh, c_poisson);
+}
+
+int pm_gradient_f64(pm_plan* plan, const double* phi, double* fx, double* fy, double* fz) {
+    PM_TRY(check_plan(plan, PM_FP64));
+    if (!phi || !fx || !fy || !fz) return fail(PM_ERR_ARG, "NULL mesh");
+    PM_TRY(set_device(plan->p));
+    return gradient_f64(plan->p, phi, fx, fy, fz);
+}
+
+int pm_interp_kick_f64(pm_plan* plan, const double* x, const double* y, const double* z,
+                       const double* fx, const double* fy, const double* fz, double* px, double* py,
+                       double* pz, int64_t np, double c_kick) {
+    PM_TRY(check_plan(plan, PM_FP64));
+    PM_TRY(check_np(np, {x, y, z, px, py, pz}));
+    if (!fx || !fy || !fz) return fail(PM_ERR_ARG, "NULL force mesh");
+    PM_TRY(set_device(plan->p));
+    return interp_kick_f64(plan->p, x, y, z, fx, fy, fz, px, py, pz, np, c_kick);
+}
+
+int pm_drift_f64(pm_plan* plan, double* x, double* y, double* z, const double* px,
+                 const double* py, const double* pz, int64_t np, double dt) {
+    PM_TRY(check_plan(plan, PM_FP64));
+    PM_TRY(check_np(np, {x, y, z, px, py, pz}));
+    PM_TRY(set_device(plan->p));
+    return drift_f64(plan->p, x, y, z, px, py, pz, np, dt);
+}
+
+int pm_step_f64(pm_plan* plan, double* x, double* y, double* z, double* px, double* py,
+                double* pz, int64_t np, double mass, double c_poisson, double c_kick, double dt) {
+    PM_TRY(check_plan(plan, PM_FP64));
+    PM_TRY(check_np(np, {x, y, z, px, py, pz}));
+    PM_TRY(set_device(plan->p));
+    Plan& p = plan->p;
+    PM_TRY(ensure_workspace(p, true));
+    double* m = static_cast<double*>(p.mesh);
+    double* f[3] = {static_cast<double*>(p.force[0]), static_cast<double*>(p.force[1]),
+                    static_cast<double*>(p.force[2])};
+    PM_TRY(deposit_f64(p, x, y, z, np, mass, m));
+    PM_TRY(fft_r2c<double>(p, m));
+    PM_TRY(green_apply<double>(p, m, c_poisson));
+    PM_TRY(fft_c2r<double>(p, m));
+    PM_TRY(gradient_f64(p, m, f[0], f[1], f[2]));
+    PM_TRY(interp_kick_f64(p, x, y, z, f[0], f[1], f[2], px, py, pz, np, c_kick));
+    if (dt != 0.0) PM_TRY(drift_f64(p, x, y, z, px, py, pz, np, dt));
+    return PM_OK;
+}
+
+// ------------------------------------------------------------------ FP32
+
+int pm_split_positions(pm_plan* plan, const double* x, const double* y, const double* z,
+                       int64_t np, uint32_t* cell, float* ox, float* oy, float* oz) {
+    if (!plan) return fail(PM_ERR_ARG, "plan is NULL");
+    PM_TRY(check_np(np, {x, y, z, cell, ox, oy, oz}));
+    PM_TRY(set_device(plan->p));
+    return split_positions(plan->p, x, y, z, np, cell, ox, oy, oz);
+}
+
+int pm_join_positions(pm_plan* plan, const uint32_t* cell, const float* ox, const float* oy,
+                      const float* oz, int64_t np, double* x, double* y, double* z) {
+    if (!plan) return fail(PM_ERR_ARG, "plan is NULL");
+    PM_TRY(check_np(np, {x, y, z, cell, ox, oy, oz}));
+    PM_TRY(set_device(plan->p));
+    return join_positions(plan->p, cell, ox, oy, oz, np, x, y, z);
+}
+
+int pm_deposit_f32(pm_plan* plan, const uint32_t* cell, const float* ox, const float* oy,
+                   const float* oz, int64_t np, float mass, float* mesh) {
+    PM_TRY(check_plan(plan, PM_FP32));
+    PM_TRY(check_np(np, {cell, ox, oy, oz}));
+    if (!mesh) return fail(PM_ERR_ARG, "mesh is NULL");
+    PM_TRY(set_device(plan->p));
+    return deposit_f32(plan->p, cell, ox, oy, oz, np, mass, mesh);
+}
+
+int pm_fft_r2c_f32(pm_plan* plan, float* mesh) {
+    PM_TRY(check_plan(plan, PM_FP32));
+    if (!mesh) return fail(PM_ERR_ARG, "mesh is NULL");
+    PM_TRY(set_device(plan->p));
+    return fft_r2c<float>(plan->p, mesh);
+}
+
+int pm_green_f32(pm_plan* plan, float* mesh, double c_poisson) {
+    PM_TRY(check_plan(plan, PM_FP32));
+    if (!mesh) return fail(PM_ERR_ARG, "mesh is NULL");
+    PM_TRY(set_device(plan->p));
+    return green_apply<float>(plan->p, mesh, c_poisson);
+}
+
+int pm_fft_c2r_f32(pm_plan* plan, float* mesh) {
+    PM_TRY(check_plan(plan, PM_FP32));
+    if (!mesh) return fail(PM_ERR_ARG, "mesh is NULL");
+    PM_TRY(set_device(plan->p));
+    return fft_c2r<float>(plan->p, mesh);
+}
+
+int pm_poisson_f32(pm_plan* plan, float* mesh, double c_poisson) {
+    PM_TRY(check_plan(plan, PM_FP32));
+    if (!mesh) return fail(PM_ERR_ARG, "mesh is NULL");
+    PM_TRY(set_device(plan->p));
+    return poisson_fused<float>(plan->p, mesh, c_poisson);
+}
+
+int pm_interp_f32(pm_plan* plan, const float* phi, const uint32_t* cell, const float* ox,
+                  const float* oy, const float* oz, int64_t np, float* fx, float* fy, float* fz) {
+    PM_TRY(check_plan(plan, PM_FP32));
+    PM_TRY(check_np(np, {cell, ox, oy, oz, fx, fy, fz}));
+    if (!phi) return fail(PM_ERR_ARG, "phi is NULL");
+    PM_TRY(set_device(plan->p));
+    return interp_f32(plan->p, phi, cell, ox, oy, oz, np, fx, fy, fz);
+}
+
+int pm_kick_drift_f32(pm_plan* plan, const float* phi, uint32_t* cell, float* ox, float* oy,
+                      float* oz, float* vx, float* vy, float* vz, int64_t np, double c_kick,
+                      double dt) {
+    PM_TRY(check_plan(plan, PM_FP32));
+    PM_TRY(check_np(np, {cell, ox, oy, oz, vx, vy, vz}));
+    if (!phi) return fail(PM_ERR_ARG, "phi is NULL");
+    PM_TRY(set_device(plan->p));
+    return kick_drift_f32(plan->p, phi, cell, ox, oy, oz, vx, vy, vz, np, c_kick, dt);
+}
+
+int pm_step_f32(pm_plan* plan, uint32_t* cell, float* ox, float* oy, float* oz, float* vx,
+                float* vy, float* vz, int64_t np, float mass, double c_poisson, double c_kick,
+                double dt) {
+    PM_TRY(check_plan(plan, PM_FP32));
+    PM_TRY(check_np(np, {cell, ox, oy, oz, vx, vy, vz}));
+    PM_TRY(set_device(plan->p));
+    Plan& p = plan->p;
+    PM_TRY(ensure_workspace(p, false));
+    float* m = static_cast<float*>(p.mesh);
+    PM_TRY(deposit_f32(p, cell, ox, oy, oz, np, mass, m));
+    PM_TRY(poisson_fused<float>(p, m, c_poisson));
+    PM_TRY(kick_drift_f32(p, m, cell, ox, oy, oz, vx, vy, vz, np, c_kick, dt));
+    return PM_OK;
+}
+
+// ------------------------------------------------------------------- ICs
+
+int pm_ic_zeldovich(int ng, int nrow, double n_s, double rms_cells, uint64_t seed,
+                    double vel_factor, double* x, double* y, double* z, double* vx, double* vy,
+                    double* vz, void* stream) {
+    if (!fft_size_supported(nrow)) return fail(PM_ERR_SIZE, "nrow must be a power of two in [8, 1024]");
+    if (ng < 1) return fail(PM_ERR_ARG, "ng must be positive");
+    if (!(rms_cells >= 0.0) || !std::isfinite(n_s)) return fail(PM_ERR_ARG, "bad spectrum parameters");
+    PM_TRY(check_np(1, {x, y, z, vx, vy, vz}));
+    pm_plan* plan = nullptr;
+    PM_TRY(pm_plan_create(nrow, PM_FP64, PM_GREEN_DISCRETE, 2, stream, &plan));
+    const int rc = ic_zeldovich(plan->p, n_s, rms_cells, seed, vel_factor, ng, x, y, z, vx, vy, vz);
+    pm_plan_destroy(plan);
+    return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,100 @@
+// Register-resident radix-R DFTs and the mixed-radix Stockham pass schedule
+// used by every FFT kernel of the particle-mesh step.
+//
+// Stockham autosort (decimation in time), line length N = R1 * R2 * ...:
+//   pass with radix R after Ns = product of earlier radices:
+//     thread j in [0, N/R) reads v[r] = in[j + r N/R],
+//     multiplies v[r] by W_N^{r (j mod Ns) N/(Ns R)},  W_N = exp(sign 2 pi i / N),
+//     takes the radix-R DFT of v, and writes
+//     out[(j / Ns) Ns R + (j mod Ns) + k Ns] = V[k].
+// The output is in natural order after the last pass.  This is the same
+// mixed-radix factorisation idea as the reference's FFTE kernels
+// (src/fft/ffte1/fft235.f:20-121, twiddles fft235.f:205-219), reorganised so
+// that one thread owns one radix-R butterfly held in registers.
+#pragma once
+
+#include "pm_internal.cuh"
+
+namespace pmb {
+
+// cos / sin (2 pi k / 64), k = 0..31 (rounded to double).
+__device__ __forceinline__ double cos64(int k) {
+    constexpr double c[32] = {
+        1.0, 0.9951847266721969, 0.9807852804032304, 0.9569403357322088, 0.9238795325112867,
+        0.881921264348355, 0.8314696123025452, 0.773010453362737, 0.7071067811865476,
+        0.6343932841636455, 0.5555702330196022, 0.47139673682599764, 0.3826834323650898,
+        0.2902846772544624, 0.19509032201612828, 0.0980171403295606, 0.0, -0.0980171403295606,
+        -0.19509032201612828, -0.2902846772544624, -0.3826834323650898, -0.47139673682599764,
+        -0.5555702330196022, -0.6343932841636455, -0.7071067811865476, -0.773010453362737,
+        -0.8314696123025452, -0.881921264348355, -0.9238795325112867, -0.9569403357322088,
+        -0.9807852804032304, -0.9951847266721969};
+    return c[k];
+}
+__device__ __forceinline__ double sin64(int k) { return k <= 16 ? cos64(16 - k) : cos64(k - 16); }
+
+// d * exp(DIR 2 pi i k / 64), k a compile-time constant after unrolling.
+template <int DIR, typename C>
+__device__ __forceinline__ C rot64(C d, int k) {
+    using T = decltype(C::x);
+    constexpr T h = (T)0.7071067811865476;
+    if (k == 0) return d;
+    if (k == 16) return DIR < 0 ? cmake<C>(d.y, -d.x) : cmake<C>(-d.y, d.x);
+    if (k == 8)
+        return DIR < 0 ? cmake<C>((d.x + d.y) * h, (d.y - d.x) * h) : cmake<C>((d.x - d.y) * h, (d.x + d.y) * h);
+    if (k == 24)
+        return DIR < 0 ? cmake<C>((d.y - d.x) * h, -(d.x + d.y) * h) : cmake<C>(-(d.x + d.y) * h, (d.x - d.y) * h);
+    const T c = (T)cos64(k), s = (T)(DIR * sin64(k));
+    return cmake<C>(d.x * c - d.y * s, d.x * s + d.y * c);
+}
+
+// Bit reversal of k on log2(R) bits.
+template <int R>
+__host__ __device__ constexpr int brev(int k) {
+    int r = 0;
+    for (int m = R >> 1, b = 1; m >= 1; m >>= 1, b <<= 1)
+        if (k & m) r |= b;
+    return r;
+}
+
+// In-register radix-R DFT (R a power of two <= 32), decimation in frequency;
+// on return V[k] = v[brev<R>(k)].
+template <int R, int DIR, typename C>
+__device__ __forceinline__ void dft(C* v) {
+#pragma unroll
+    for (int half = R / 2; half >= 1; half >>= 1) {
+#pragma unroll
+        for (int b = 0; b < R; b += 2 * half) {
+#pragma unroll
+            for (int i = 0; i < half; ++i) {
+                const C a = v[b + i], c = v[b + i + half];
+                v[b + i] = cadd(a, c);
+                v[b + i + half] = rot64<DIR>(csub(a, c), i * (64 / (2 * half)));
+            }
+        }
+    }
+}
+
+// Twiddle W_N^e from the table tw[e] = exp(-2 pi i e / N) (inverse: conj).
+template <int DIR, typename C>
+__device__ __forceinline__ C twiddle(const C* __restrict__ tw, int e) {
+    const C w = __ldg(tw + e);
+    return DIR < 0 ? w : cconj(w);
+}
+
+// Two-pass radix choice for a line of length L = R1 * R2.
+template <int L> struct Radix;
+template <> struct Radix<4> { static constexpr int R1 = 2, R2 = 2; };
+template <> struct Radix<8> { static constexpr int R1 = 2, R2 = 4; };
+template <> struct Radix<16> { static constexpr int R1 = 4, R2 = 4; };
+template <> struct Radix<32> { static constexpr int R1 = 4, R2 = 8; };
+template <> struct Radix<64> { static constexpr int R1 = 8, R2 = 8; };
+template <> struct Radix<128> { static constexpr int R1 = 8, R2 = 16; };
+template <> struct Radix<256> { static constexpr int R1 = 16, R2 = 16; };
+template <> struct Radix<512> { static constexpr int R1 = 16, R2 = 32; };
+template <> struct Radix<1024> { static constexpr int R1 = 32, R2 = 32; };
+
+template <int L> constexpr int threads_per_line() {
+    return L / (Radix<L>::R1 < Radix<L>::R2 ? Radix<L>::R1 : Radix<L>::R2);
+}
+
+}  // namespace pmb

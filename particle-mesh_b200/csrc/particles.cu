@@ -1,0 +1,428 @@
+// Particle <-> mesh kernels of the particle-mesh step: CIC deposit, mesh
+// gradient, CIC interpolation + kick, drift, and the FP32 split-position
+// forms of the same.
+//
+// Periodic single box: the reference's ghost planes (+1 for the deposit,
+// src/utils/utils.cpp:38-68 and src/decomp/slab/reorder_slab.cpp:3-68;
+// -1/+2 for the gradient, src/decomp/slab/reorder_slab_back.cpp:3-49 and
+// transpose_slab_back.cpp:3-49) become index wraps; ng is a power of two so a
+// wrap is a mask.
+#include "pm_internal.cuh"
+
+namespace pmb {
+
+namespace {
+
+// A position outside [0, n) (or NaN / inf) is recorded in the plan's error
+// word and wrapped (NaN and inf -> 0) so that every access stays in bounds.
+__device__ __forceinline__ double sanitize(double v, double n, int* err) {
+    if (v >= 0.0 && v < n) return v;
+    atomicOr(err, ERRBIT_RANGE);
+    if (!isfinite(v)) return 0.0;
+    double m = v - n * floor(v / n);
+    if (m >= n) m -= n;
+    if (m < 0.0) m = 0.0;
+    return m;
+}
+
+__device__ __forceinline__ double wrap_pos(double v, double n) {
+    v = v - n * floor(v / n);
+    return v >= n ? v - n : v;  // v/n rounding can land exactly on n
+}
+
+template <typename T>
+__global__ void k_mesh_init(T* __restrict__ mesh, int n, T val) {
+    const long long pz = n + 2, total = (long long)n * n * pz;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x)
+        mesh[i] = (i % pz) < n ? val : (T)0;
+}
+
+// ------------------------------------------------------------------- FP64
+
+// CIC deposit, one thread per particle, 8 FP64 atomics into the periodic
+// mesh.  Same weights and operation order as cic_deposit
+// (include/utils/utils_inline.h:25-49); cell = floor(x) as static_cast<int>
+// in deposit_particles (src/utils/utils.cpp:85-97) for x >= 0.
+__global__ void k_deposit_f64(const double* __restrict__ x, const double* __restrict__ y,
+                              const double* __restrict__ z, long long np, double mass,
+                              double* __restrict__ mesh, int n, int* err) {
+    const double dn = (double)n;
+    const long long pz = n + 2;
+    const int msk = n - 1;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np;
+         p += (long long)gridDim.x * blockDim.x) {
+        const double xp = sanitize(x[p], dn, err), yp = sanitize(y[p], dn, err), zp = sanitize(z[p], dn, err);
+        const double fx = floor(xp), fy = floor(yp), fz = floor(zp);
+        const int i0 = (int)fx, j0 = (int)fy, k0 = (int)fz;
+        const int i1 = (i0 + 1) & msk, j1 = (j0 + 1) & msk, k1 = (k0 + 1) & msk;
+        const double tx = xp - fx, ty = yp - fy, tz = zp - fz;
+        const double sx0 = 1.0 - tx, sy0 = 1.0 - ty, sz0 = 1.0 - tz;
+        const double sxy00 = sx0 * sy0, sxy10 = tx * sy0, sxy01 = sx0 * ty, sxy11 = tx * ty;
+        const double m0 = mass * sz0, m1 = mass * tz;
+        const long long r00 = ((long long)i0 * n + j0) * pz, r10 = ((long long)i1 * n + j0) * pz;
+        const long long r01 = ((long long)i0 * n + j1) * pz, r11 = ((long long)i1 * n + j1) * pz;
+        atomicAdd(mesh + r00 + k0, sxy00 * m0);
+        atomicAdd(mesh + r10 + k0, sxy10 * m0);
+        atomicAdd(mesh + r01 + k0, sxy01 * m0);
+        atomicAdd(mesh + r11 + k0, sxy11 * m0);
+        atomicAdd(mesh + r00 + k1, sxy00 * m1);
+        atomicAdd(mesh + r10 + k1, sxy10 * m1);
+        atomicAdd(mesh + r01 + k1, sxy01 * m1);
+        atomicAdd(mesh + r11 + k1, sxy11 * m1);
+    }
+}
+
+// f = -grad phi by centred differences, one thread per cell.
+//   order 2: (phi[i-1] - phi[i+1]) / 2          (src/utils/utils.cpp:130-135)
+//   order 4: (8 (phi[i-1] - phi[i+1]) - (phi[i-2] - phi[i+2])) / 12
+template <int ORDER>
+__global__ void k_gradient_f64(const double* __restrict__ phi, double* __restrict__ fx,
+                               double* __restrict__ fy, double* __restrict__ fz, int n) {
+    const long long total = (long long)n * n * n, pz = n + 2;
+    const int msk = n - 1;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < total;
+         c += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(c & msk), j = (int)((c / n) & msk), i = (int)(c / ((long long)n * n));
+        auto P = [&](int a, int b, int d) { return __ldg(phi + ((long long)(a & msk) * n + (b & msk)) * pz + (d & msk)); };
+        if (ORDER == 4) {
+            fx[c] = (8.0 * (P(i - 1, j, k) - P(i + 1, j, k)) - (P(i - 2, j, k) - P(i + 2, j, k))) / 12.0;
+            fy[c] = (8.0 * (P(i, j - 1, k) - P(i, j + 1, k)) - (P(i, j - 2, k) - P(i, j + 2, k))) / 12.0;
+            fz[c] = (8.0 * (P(i, j, k - 1) - P(i, j, k + 1)) - (P(i, j, k - 2) - P(i, j, k + 2))) / 12.0;
+        } else {
+            fx[c] = (P(i - 1, j, k) - P(i + 1, j, k)) * 0.5;
+            fy[c] = (P(i, j - 1, k) - P(i, j + 1, k)) * 0.5;
+            fz[c] = (P(i, j, k - 1) - P(i, j, k + 1)) * 0.5;
+        }
+    }
+}
+
+// Trilinear gather with the operation order of trilerp1
+// (include/utils/utils_inline.h:55-70).
+__device__ __forceinline__ double trilerp(const double* __restrict__ f, long long b00, long long b10,
+                                          long long b01, long long b11, int k0, int k1, double tx,
+                                          double ty, double tz) {
+    const double mx = 1.0 - tx, my = 1.0 - ty, mz = 1.0 - tz;
+    const double f00 = __ldg(f + b00 + k0) * mx + __ldg(f + b10 + k0) * tx;
+    const double f10 = __ldg(f + b01 + k0) * mx + __ldg(f + b11 + k0) * tx;
+    const double fz0 = f00 * my + f10 * ty;
+    const double g00 = __ldg(f + b00 + k1) * mx + __ldg(f + b10 + k1) * tx;
+    const double g10 = __ldg(f + b01 + k1) * mx + __ldg(f + b11 + k1) * tx;
+    const double fz1 = g00 * my + g10 * ty;
+    return fz0 * mz + fz1 * tz;
+}
+
+// p += c_kick * W^T f (update_particles, src/utils/utils.cpp:141-170).
+__global__ void k_interp_kick_f64(const double* __restrict__ x, const double* __restrict__ y,
+                                  const double* __restrict__ z, const double* __restrict__ fx,
+                                  const double* __restrict__ fy, const double* __restrict__ fz,
+                                  double* __restrict__ px, double* __restrict__ py,
+                                  double* __restrict__ pzv, long long np, double c_kick, int n,
+                                  int* err) {
+    const double dn = (double)n;
+    const int msk = n - 1;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np;
+         p += (long long)gridDim.x * blockDim.x) {
+        const double xp = sanitize(x[p], dn, err), yp = sanitize(y[p], dn, err), zp = sanitize(z[p], dn, err);
+        const double flx = floor(xp), fly = floor(yp), flz = floor(zp);
+        const int i0 = (int)flx, j0 = (int)fly, k0 = (int)flz;
+        const int i1 = (i0 + 1) & msk, j1 = (j0 + 1) & msk, k1 = (k0 + 1) & msk;
+        const double tx = xp - flx, ty = yp - fly, tz = zp - flz;
+        const long long b00 = ((long long)i0 * n + j0) * n, b10 = ((long long)i1 * n + j0) * n;
+        const long long b01 = ((long long)i0 * n + j1) * n, b11 = ((long long)i1 * n + j1) * n;
+        px[p] += trilerp(fx, b00, b10, b01, b11, k0, k1, tx, ty, tz) * c_kick;
+        py[p] += trilerp(fy, b00, b10, b01, b11, k0, k1, tx, ty, tz) * c_kick;
+        pzv[p] += trilerp(fz, b00, b10, b01, b11, k0, k1, tx, ty, tz) * c_kick;
+    }
+}
+
+__global__ void k_drift_f64(double* __restrict__ x, double* __restrict__ y, double* __restrict__ z,
+                            const double* __restrict__ px, const double* __restrict__ py,
+                            const double* __restrict__ pz, long long np, double dt, int n) {
+    const double dn = (double)n;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np;
+         p += (long long)gridDim.x * blockDim.x) {
+        x[p] = wrap_pos(x[p] + px[p] * dt, dn);
+        y[p] = wrap_pos(y[p] + py[p] * dt, dn);
+        z[p] = wrap_pos(z[p] + pz[p] * dt, dn);
+    }
+}
+
+// ------------------------------------------------------ split positions
+
+__device__ __forceinline__ void split1(double v, int msk, int& cell, float& off) {
+    const double f = floor(v);
+    cell = ((int)(long long)f) & msk;
+    off = (float)(v - f);
+    if (off >= 1.0f) {  // rounding to FP32 reached the next cell
+        off = 0.0f;
+        cell = (cell + 1) & msk;
+    }
+}
+
+__device__ __forceinline__ uint32_t pack_cell(int i, int j, int k) {
+    return ((uint32_t)i << 20) | ((uint32_t)j << 10) | (uint32_t)k;
+}
+__device__ __forceinline__ void unpack_cell(uint32_t c, int& i, int& j, int& k) {
+    i = (int)(c >> 20);
+    j = (int)((c >> 10) & 1023u);
+    k = (int)(c & 1023u);
+}
+
+__global__ void k_split(const double* __restrict__ x, const double* __restrict__ y,
+                        const double* __restrict__ z, long long np, uint32_t* __restrict__ cell,
+                        float* __restrict__ ox, float* __restrict__ oy, float* __restrict__ oz, int n,
+                        int* err) {
+    const double dn = (double)n;
+    const int msk = n - 1;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np;
+         p += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        float a, b, c;
+        split1(sanitize(x[p], dn, err), msk, i, a);
+        split1(sanitize(y[p], dn, err), msk, j, b);
+        split1(sanitize(z[p], dn, err), msk, k, c);
+        cell[p] = pack_cell(i, j, k);
+        ox[p] = a;
+        oy[p] = b;
+        oz[p] = c;
+    }
+}
+
+__global__ void k_join(const uint32_t* __restrict__ cell, const float* __restrict__ ox,
+                       const float* __restrict__ oy, const float* __restrict__ oz, long long np,
+                       double* __restrict__ x, double* __restrict__ y, double* __restrict__ z) {
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np;
+         p += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        unpack_cell(cell[p], i, j, k);
+        x[p] = (double)i + (double)ox[p];
+        y[p] = (double)j + (double)oy[p];
+        z[p] = (double)k + (double)oz[p];
+    }
+}
+
+// ------------------------------------------------------------------- FP32
+
+__global__ void k_deposit_f32(const uint32_t* __restrict__ cell, const float* __restrict__ ox,
+                              const float* __restrict__ oy, const float* __restrict__ oz,
+                              long long np, float mass, float* __restrict__ mesh, int n) {
+    const long long pz = n + 2;
+    const int msk = n - 1;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np;
+         p += (long long)gridDim.x * blockDim.x) {
+        int i0, j0, k0;
+        unpack_cell(__ldg(cell + p), i0, j0, k0);
+        i0 &= msk; j0 &= msk; k0 &= msk;
+        const int i1 = (i0 + 1) & msk, j1 = (j0 + 1) & msk, k1 = (k0 + 1) & msk;
+        const float tx = __ldg(ox + p), ty = __ldg(oy + p), tz = __ldg(oz + p);
+        const float sx0 = 1.0f - tx, sy0 = 1.0f - ty, sz0 = 1.0f - tz;
+        const float sxy00 = sx0 * sy0, sxy10 = tx * sy0, sxy01 = sx0 * ty, sxy11 = tx * ty;
+        const float m0 = mass * sz0, m1 = mass * tz;
+        const long long r00 = ((long long)i0 * n + j0) * pz, r10 = ((long long)i1 * n + j0) * pz;
+        const long long r01 = ((long long)i0 * n + j1) * pz, r11 = ((long long)i1 * n + j1) * pz;
+        atomicAdd(mesh + r00 + k0, sxy00 * m0);
+        atomicAdd(mesh + r10 + k0, sxy10 * m0);
+        atomicAdd(mesh + r01 + k0, sxy01 * m0);
+        atomicAdd(mesh + r11 + k0, sxy11 * m0);
+        atomicAdd(mesh + r00 + k1, sxy00 * m1);
+        atomicAdd(mesh + r10 + k1, sxy10 * m1);
+        atomicAdd(mesh + r01 + k1, sxy01 * m1);
+        atomicAdd(mesh + r11 + k1, sxy11 * m1);
+    }
+}
+
+// Force at one particle with the gradient fused into the gather: the
+// trilinear weights of cells (i+a, j+b, k+c), a,b,c in {0,1}, applied to the
+// centred difference of phi at those cells (2- or 4-point).
+template <int ORDER>
+__device__ __forceinline__ void force_at(const float* __restrict__ phi, int n, int i, int j, int k,
+                                         float tx, float ty, float tz, float& gx, float& gy,
+                                         float& gz) {
+    const int msk = n - 1;
+    const long long pz = n + 2;
+    auto P = [&](int a, int b, int c) {
+        return __ldg(phi + ((long long)(a & msk) * n + (b & msk)) * pz + (c & msk));
+    };
+    const float wx[2] = {1.0f - tx, tx}, wy[2] = {1.0f - ty, ty}, wz[2] = {1.0f - tz, tz};
+    auto D = [&](float m2, float m1, float p1, float p2) {
+        return ORDER == 4 ? (8.0f * (m1 - p1) - (m2 - p2)) * (1.0f / 12.0f) : (m1 - p1) * 0.5f;
+    };
+    constexpr int LO = ORDER == 4 ? -2 : -1, HI = ORDER == 4 ? 3 : 2, W = HI - LO + 1;
+    gx = gy = gz = 0.0f;
+#pragma unroll
+    for (int b = 0; b < 2; ++b)
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            float v[W];
+#pragma unroll
+            for (int a = 0; a < W; ++a) v[a] = P(i + LO + a, j + b, k + c);
+            const float f0 = ORDER == 4 ? D(v[0], v[1], v[3], v[4]) : D(0.f, v[0], v[2], 0.f);
+            const float f1 = ORDER == 4 ? D(v[1], v[2], v[4], v[5]) : D(0.f, v[1], v[3], 0.f);
+            gx += wy[b] * wz[c] * (wx[0] * f0 + wx[1] * f1);
+        }
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            float v[W];
+#pragma unroll
+            for (int b = 0; b < W; ++b) v[b] = P(i + a, j + LO + b, k + c);
+            const float f0 = ORDER == 4 ? D(v[0], v[1], v[3], v[4]) : D(0.f, v[0], v[2], 0.f);
+            const float f1 = ORDER == 4 ? D(v[1], v[2], v[4], v[5]) : D(0.f, v[1], v[3], 0.f);
+            gy += wx[a] * wz[c] * (wy[0] * f0 + wy[1] * f1);
+        }
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            float v[W];
+#pragma unroll
+            for (int c = 0; c < W; ++c) v[c] = P(i + a, j + b, k + LO + c);
+            const float f0 = ORDER == 4 ? D(v[0], v[1], v[3], v[4]) : D(0.f, v[0], v[2], 0.f);
+            const float f1 = ORDER == 4 ? D(v[1], v[2], v[4], v[5]) : D(0.f, v[1], v[3], 0.f);
+            gz += wx[a] * wy[b] * (wz[0] * f0 + wz[1] * f1);
+        }
+}
+
+template <int ORDER>
+__global__ void k_interp_f32(const float* __restrict__ phi, const uint32_t* __restrict__ cell,
+                             const float* __restrict__ ox, const float* __restrict__ oy,
+                             const float* __restrict__ oz, long long np, float* __restrict__ fx,
+                             float* __restrict__ fy, float* __restrict__ fz, int n) {
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np;
+         p += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        unpack_cell(__ldg(cell + p), i, j, k);
+        float gx, gy, gz;
+        force_at<ORDER>(phi, n, i, j, k, __ldg(ox + p), __ldg(oy + p), __ldg(oz + p), gx, gy, gz);
+        fx[p] = gx;
+        fy[p] = gy;
+        fz[p] = gz;
+    }
+}
+
+// v += c_kick * force; x += dt * v accumulated in FP64 and re-split.
+template <int ORDER>
+__global__ void k_kick_drift_f32(const float* __restrict__ phi, uint32_t* __restrict__ cell,
+                                 float* __restrict__ ox, float* __restrict__ oy, float* __restrict__ oz,
+                                 float* __restrict__ vx, float* __restrict__ vy, float* __restrict__ vz,
+                                 long long np, float c_kick, double dt, int n) {
+    const int msk = n - 1;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np;
+         p += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        unpack_cell(cell[p], i, j, k);
+        const float tx = ox[p], ty = oy[p], tz = oz[p];
+        float gx, gy, gz;
+        force_at<ORDER>(phi, n, i, j, k, tx, ty, tz, gx, gy, gz);
+        const float ux = vx[p] + gx * c_kick, uy = vy[p] + gy * c_kick, uz = vz[p] + gz * c_kick;
+        vx[p] = ux;
+        vy[p] = uy;
+        vz[p] = uz;
+        if (dt != 0.0) {
+            int a, b, c;
+            float qa, qb, qc;
+            split1((double)i + (double)tx + (double)ux * dt, msk, a, qa);
+            split1((double)j + (double)ty + (double)uy * dt, msk, b, qb);
+            split1((double)k + (double)tz + (double)uz * dt, msk, c, qc);
+            cell[p] = pack_cell(a, b, c);
+            ox[p] = qa;
+            oy[p] = qb;
+            oz[p] = qc;
+        }
+    }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------- launchers
+static constexpr int kThreads = 256;
+
+int deposit_f64(const Plan& p, const double* x, const double* y, const double* z, int64_t np,
+                double mass, double* mesh) {
+    k_mesh_init<double><<<grid_for(p, (long long)mesh_elems(p.ng), kThreads), kThreads, 0, p.stream>>>(mesh, p.ng, -1.0);
+    if (np > 0)
+        k_deposit_f64<<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(x, y, z, np, mass, mesh, p.ng, p.d_err);
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+int gradient_f64(const Plan& p, const double* phi, double* fx, double* fy, double* fz) {
+    const long long total = (long long)p.ng * p.ng * p.ng;
+    if (p.grad_order == 4)
+        k_gradient_f64<4><<<grid_for(p, total, kThreads), kThreads, 0, p.stream>>>(phi, fx, fy, fz, p.ng);
+    else
+        k_gradient_f64<2><<<grid_for(p, total, kThreads), kThreads, 0, p.stream>>>(phi, fx, fy, fz, p.ng);
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+int interp_kick_f64(const Plan& p, const double* x, const double* y, const double* z,
+                    const double* fx, const double* fy, const double* fz, double* px, double* py,
+                    double* pz, int64_t np, double c_kick) {
+    if (np == 0) return PM_OK;
+    k_interp_kick_f64<<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(x, y, z, fx, fy, fz, px, py, pz, np,
+                                                                          c_kick, p.ng, p.d_err);
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+int drift_f64(const Plan& p, double* x, double* y, double* z, const double* px, const double* py,
+              const double* pz, int64_t np, double dt) {
+    if (np == 0) return PM_OK;
+    k_drift_f64<<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(x, y, z, px, py, pz, np, dt, p.ng);
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+int split_positions(const Plan& p, const double* x, const double* y, const double* z, int64_t np,
+                    uint32_t* cell, float* ox, float* oy, float* oz) {
+    if (np == 0) return PM_OK;
+    k_split<<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(x, y, z, np, cell, ox, oy, oz, p.ng, p.d_err);
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+int join_positions(const Plan& p, const uint32_t* cell, const float* ox, const float* oy,
+                   const float* oz, int64_t np, double* x, double* y, double* z) {
+    if (np == 0) return PM_OK;
+    k_join<<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(cell, ox, oy, oz, np, x, y, z);
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+int deposit_f32(const Plan& p, const uint32_t* cell, const float* ox, const float* oy,
+                const float* oz, int64_t np, float mass, float* mesh) {
+    k_mesh_init<float><<<grid_for(p, (long long)mesh_elems(p.ng), kThreads), kThreads, 0, p.stream>>>(mesh, p.ng, -1.0f);
+    if (np > 0)
+        k_deposit_f32<<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(cell, ox, oy, oz, np, mass, mesh, p.ng);
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+int interp_f32(const Plan& p, const float* phi, const uint32_t* cell, const float* ox,
+               const float* oy, const float* oz, int64_t np, float* fx, float* fy, float* fz) {
+    if (np == 0) return PM_OK;
+    if (p.grad_order == 4)
+        k_interp_f32<4><<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, np, fx, fy, fz, p.ng);
+    else
+        k_interp_f32<2><<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, np, fx, fy, fz, p.ng);
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+int kick_drift_f32(const Plan& p, const float* phi, uint32_t* cell, float* ox, float* oy, float* oz,
+                   float* vx, float* vy, float* vz, int64_t np, double c_kick, double dt) {
+    if (np == 0) return PM_OK;
+    if (p.grad_order == 4)
+        k_kick_drift_f32<4><<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz, np,
+                                                                                (float)c_kick, dt, p.ng);
+    else
+        k_kick_drift_f32<2><<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz, np,
+                                                                                (float)c_kick, dt, p.ng);
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+}  // namespace pmb

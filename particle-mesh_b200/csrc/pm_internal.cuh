@@ -1,0 +1,113 @@
+// Internal declarations shared by the CUDA translation units of the
+// particle-mesh step.  Not part of the C ABI (that is include/pm_b200.h).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/pm_b200.h"
+
+namespace pmb {
+
+// ------------------------------------------------------------ complex types
+template <typename T> struct Cx;
+template <> struct Cx<float> { using t = float2; };
+template <> struct Cx<double> { using t = double2; };
+
+template <typename C> __host__ __device__ __forceinline__ C cmake(decltype(C::x) a, decltype(C::x) b) {
+    C c;
+    c.x = a;
+    c.y = b;
+    return c;
+}
+template <typename C> __device__ __forceinline__ C cadd(C a, C b) { return cmake<C>(a.x + b.x, a.y + b.y); }
+template <typename C> __device__ __forceinline__ C csub(C a, C b) { return cmake<C>(a.x - b.x, a.y - b.y); }
+template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
+    return cmake<C>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+template <typename C> __device__ __forceinline__ C cconj(C a) { return cmake<C>(a.x, -a.y); }
+template <typename C> __device__ __forceinline__ C cscale(C a, decltype(C::x) s) { return cmake<C>(a.x * s, a.y * s); }
+
+// ------------------------------------------------------------------- errors
+enum : int { ERRBIT_RANGE = 1 };
+
+// Thread-local last-error message, set by the C-ABI layer.
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+
+#define PMB_CUDA_CHECK(expr)                                            \
+    do {                                                                \
+        cudaError_t _e = (expr);                                        \
+        if (_e != cudaSuccess) return ::pmb::cuda_fail(_e, #expr);      \
+    } while (0)
+
+// ---------------------------------------------------------------- the plan
+struct Plan {
+    int ng = 0;
+    int precision = PM_FP64;
+    int green_kind = PM_GREEN_DISCRETE;
+    int grad_order = 2;
+    cudaStream_t stream = nullptr;
+    int device = 0;
+    int num_sms = 148;
+    // Tables of length ng in the plan's precision:
+    //   tw[k]    = exp(-2 pi i k / ng)          (twiddles, Green cosines)
+    //   lap1d[k] = 2 sin^2(pi k / ng)           (7-point Laplacian, 1D part)
+    void* tw = nullptr;
+    void* lap1d = nullptr;
+    int* d_err = nullptr;           // device error bits
+    void* mesh = nullptr;           // workspace mesh [ng][ng][ng+2]
+    void* force[3] = {nullptr, nullptr, nullptr};  // FP64 force arrays
+    size_t bytes = 0;
+};
+
+inline size_t mesh_elems(int ng) { return (size_t)ng * ng * (ng + 2); }
+
+// FFT passes (fft.cu).  Each returns a PM_* status.
+template <typename T> int fft_r2c(const Plan& p, T* mesh);
+template <typename T> int fft_c2r(const Plan& p, T* mesh);
+template <typename T> int green_apply(const Plan& p, T* mesh, double c_poisson);
+template <typename T> int poisson_fused(const Plan& p, T* mesh, double c_poisson);
+bool fft_size_supported(int ng);
+int fft_prepare(const Plan& p);  // one-time kernel attributes (large smem)
+
+// Particle and mesh kernels (particles.cu).
+int deposit_f64(const Plan& p, const double* x, const double* y, const double* z, int64_t np,
+                double mass, double* mesh);
+int gradient_f64(const Plan& p, const double* phi, double* fx, double* fy, double* fz);
+int interp_kick_f64(const Plan& p, const double* x, const double* y, const double* z,
+                    const double* fx, const double* fy, const double* fz, double* px, double* py,
+                    double* pz, int64_t np, double c_kick);
+int drift_f64(const Plan& p, double* x, double* y, double* z, const double* px, const double* py,
+              const double* pz, int64_t np, double dt);
+int split_positions(const Plan& p, const double* x, const double* y, const double* z, int64_t np,
+                    uint32_t* cell, float* ox, float* oy, float* oz);
+int join_positions(const Plan& p, const uint32_t* cell, const float* ox, const float* oy,
+                   const float* oz, int64_t np, double* x, double* y, double* z);
+int deposit_f32(const Plan& p, const uint32_t* cell, const float* ox, const float* oy,
+                const float* oz, int64_t np, float mass, float* mesh);
+int interp_f32(const Plan& p, const float* phi, const uint32_t* cell, const float* ox,
+               const float* oy, const float* oz, int64_t np, float* fx, float* fy, float* fz);
+int kick_drift_f32(const Plan& p, const float* phi, uint32_t* cell, float* ox, float* oy, float* oz,
+                   float* vx, float* vy, float* vz, int64_t np, double c_kick, double dt);
+
+// Zel'dovich initial conditions (ic.cu); p is an FP64 plan of size nrow.
+int ic_zeldovich(const Plan& p, double n_s, double rms_cells, uint64_t seed, double vel_factor, int ng,
+                 double* x, double* y, double* z, double* vx, double* vy, double* vz);
+
+// Grid size for a grid-stride loop over n items: whole waves of the SM count.
+inline unsigned grid_for(const Plan& p, long long n, int threads, int blocks_per_sm = 8) {
+    long long need = (n + threads - 1) / threads;
+    long long cap = (long long)p.num_sms * blocks_per_sm;
+    if (need < 1) need = 1;
+    return (unsigned)(need < cap ? need : cap);
+}
+
+}  // namespace pmb
+
+struct pm_plan {
+    pmb::Plan p;
+};

@@ -1,0 +1,346 @@
+"""GPU parity of every stage of the particle-mesh step against the CPU oracle.
+
+Tolerances (relative L2 unless stated):
+  FP64 path vs oracle / golden fixtures:  1e-12 (density 1e-13)
+  FP32 split path vs the FP64 oracle:     forces 1e-4 (the target), potential 1e-4
+All calls go through the C ABI (libpm_b200.so) via the package's ctypes layer.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden_cases, load_golden
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+DEV = "cuda:0"
+
+
+def rel(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def T(a, dtype=torch.float64):
+    return torch.tensor(np.ascontiguousarray(a), dtype=dtype, device=DEV)
+
+
+def H(t):
+    return t.detach().cpu().numpy()
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+def uniform(ng, n, seed):
+    rng = np.random.default_rng(seed)
+    return [rng.uniform(0, ng, n) for _ in range(3)]
+
+
+# ------------------------------------------------------------------- FFT
+
+@pytest.mark.parametrize("ng", [8, 16, 32, 64, 128])
+def test_fft_r2c_c2r_f64(pmpkg, O, ng):
+    rng = np.random.default_rng(ng)
+    m = O.padded(ng)
+    m[:, :, :ng] = rng.standard_normal((ng, ng, ng))
+    plan = pmpkg.Plan(ng, "fp64")
+    d = T(m)
+    plan.fft_r2c(d)
+    spec = H(d).view(np.complex128)
+    ref = np.fft.rfftn(m[:, :, :ng])
+    assert rel(spec, ref) < 1e-13
+    if ng <= 32:
+        mm = m.copy()
+        O.rfft3d_forward(mm)
+        assert rel(spec, O.spectrum_view(mm)) < 1e-13
+    plan.fft_c2r(d)
+    assert rel(H(d)[:, :, :ng], ng ** 3 * m[:, :, :ng]) < 1e-13
+    assert np.all(H(d)[:, :, ng:] == 0)
+
+
+@pytest.mark.parametrize("ng", [256, 512])
+def test_fft_round_trip_large_f64(pmpkg, ng):
+    g = torch.Generator(device=DEV).manual_seed(ng)
+    plan = pmpkg.Plan(ng, "fp64")
+    d = plan.new_mesh()
+    d[:, :, :ng] = torch.randn((ng, ng, ng), generator=g, device=DEV, dtype=torch.float64)
+    x = d[:, :, :ng].clone()
+    plan.fft_r2c(d)
+    # Parseval for the half spectrum: sum|x|^2 N^3 = |X0|^2 + 2 sum_mid |X|^2 + |XN|^2
+    s = torch.view_as_complex(d.view(ng, ng, ng // 2 + 1, 2))
+    e = (s[:, :, 0].abs() ** 2).sum() + (s[:, :, -1].abs() ** 2).sum() + 2 * (s[:, :, 1:-1].abs() ** 2).sum()
+    assert float(e / ((x * x).sum() * ng ** 3)) == pytest.approx(1.0, abs=1e-12)
+    plan.fft_c2r(d)
+    assert float((d[:, :, :ng] / ng ** 3 - x).norm() / x.norm()) < 1e-13
+
+
+@pytest.mark.parametrize("ng", [16, 64, 1024])
+def test_fft_f32(pmpkg, ng):
+    rng = np.random.default_rng(3)
+    m = np.zeros((ng, ng, ng + 2), np.float32)
+    m[:, :, :ng] = rng.standard_normal((ng, ng, ng)).astype(np.float32)
+    plan = pmpkg.Plan(ng, "fp32")
+    d = T(m, torch.float32)
+    plan.fft_r2c(d)
+    if ng <= 64:
+        assert rel(H(d).view(np.complex64), np.fft.rfftn(m[:, :, :ng].astype(np.float64))) < 2e-6
+    plan.fft_c2r(d)
+    assert rel(H(d)[:, :, :ng] / ng ** 3, m[:, :, :ng]) < 2e-6
+
+
+@pytest.mark.parametrize("kind", ["discrete", "spectral"])
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_green_and_fused_poisson(pmpkg, O, kind, prec):
+    ng = 32
+    rng = np.random.default_rng(11)
+    m = O.padded(ng)
+    m[:, :, :ng] = rng.standard_normal((ng, ng, ng))
+    kid = 0 if kind == "discrete" else 1
+    ref = m.copy()
+    O.rfft3d_forward(ref)
+    O.green(ref, 2.5, kid)
+    spec_ref = O.spectrum_view(ref).copy()
+    O.rfft3d_inverse(ref)
+    dt = torch.float64 if prec == "fp64" else torch.float32
+    tol = 1e-12 if prec == "fp64" else 2e-6
+    plan = pmpkg.Plan(ng, prec, kind)
+    d = T(m, dt)
+    plan.fft_r2c(d)
+    plan.green(d, 2.5)
+    got = H(d).astype(np.float64) if prec == "fp32" else H(d)
+    assert rel(got.view(np.complex128), spec_ref) < tol
+    plan.fft_c2r(d)
+    assert rel(H(d)[:, :, :ng], ref[:, :, :ng]) < tol
+    e = T(m, dt)
+    plan.poisson(e, 2.5)
+    assert rel(H(e)[:, :, :ng], ref[:, :, :ng]) < tol
+
+
+# ------------------------------------------------------ particle stages
+
+@pytest.mark.parametrize("ng,np_", [(8, 100), (16, 5000), (64, 64 ** 3)])
+def test_deposit_f64(pmpkg, O, ng, np_):
+    x, y, z = uniform(ng, np_, ng)
+    mass = ng ** 3 / np_
+    plan = pmpkg.Plan(ng, "fp64")
+    got = H(plan.deposit(T(x), T(y), T(z), mass))
+    ref = O.deposit(ng, x, y, z, mass)
+    assert rel(got, ref) < 1e-13
+    assert np.all(got[:, :, ng:] == 0)
+
+
+@pytest.mark.parametrize("order", [2, 4])
+def test_gradient_f64(pmpkg, O, order):
+    ng = 32
+    rng = np.random.default_rng(order)
+    phi = O.padded(ng)
+    phi[:, :, :ng] = rng.standard_normal((ng, ng, ng))
+    plan = pmpkg.Plan(ng, "fp64", grad_order=order)
+    f = plan.gradient(T(phi))
+    ref = O.gradient(phi, order)
+    for a in range(3):
+        assert rel(H(f[a]), ref[a]) < 1e-14
+
+
+def test_interp_kick_and_drift_f64(pmpkg, O):
+    ng, np_ = 32, 20000
+    x, y, z = uniform(ng, np_, 5)
+    rng = np.random.default_rng(6)
+    f = [rng.standard_normal((ng, ng, ng)) for _ in range(3)]
+    p = [rng.standard_normal(np_) for _ in range(3)]
+    plan = pmpkg.Plan(ng, "fp64")
+    tp = [T(a) for a in p]
+    tx = [T(a) for a in (x, y, z)]
+    plan.interp_kick(*tx, [T(a) for a in f], *tp, 0.37)
+    O.interp_kick(x, y, z, f, *p, 0.37)
+    for a in range(3):
+        assert rel(H(tp[a]), p[a]) < 1e-14
+    plan.drift(*tx, *tp, 3.1)
+    O.drift(ng, x, y, z, *p, 3.1)
+    for a, b in zip(tx, (x, y, z)):
+        assert np.abs(H(a) - b).max() < 1e-12
+        assert H(a).min() >= 0 and H(a).max() < ng
+
+
+# --------------------------------------- whole reference step vs golden
+
+@pytest.mark.parametrize("name", golden_cases())
+def test_reference_step_matches_golden(pmpkg, name):
+    g = load_golden(name)
+    ng, mass = int(g["ng"]), float(g["mass"])
+    cp, ck = pmpkg.reference_coefficients(float(g["a"]))
+    plan = pmpkg.Plan(ng, "fp64")
+    x, y, z = (T(g["pos"][i]) for i in range(3))
+    p = [torch.zeros_like(x) for _ in range(3)]
+    mesh = plan.deposit(x, y, z, mass)
+    assert rel(H(mesh)[:, :, :ng], g["delta"]) < 1e-13
+    plan.fft_r2c(mesh)
+    plan.green(mesh, cp)
+    plan.fft_c2r(mesh)
+    if "phi" in g:
+        assert rel(H(mesh)[:, :, :ng], g["phi"]) < 1e-12
+    f = plan.gradient(mesh)
+    if "force" in g:
+        assert rel(np.stack([H(a) for a in f]), g["force"]) < 1e-12
+    plan.interp_kick(x, y, z, f, *p, ck)
+    assert rel(np.stack([H(a) for a in p]), g["mom"]) < 1e-12
+    # the one-call step gives the same momenta
+    q = [torch.zeros_like(x) for _ in range(3)]
+    plan.step(x, y, z, *q, mass, cp, ck, 0.0)
+    assert rel(np.stack([H(a) for a in q]), g["mom"]) < 1e-12
+
+
+def test_reference_mirrors(pmpkg):
+    """The reference-named functions reproduce the golden step."""
+    g = load_golden("ref_step_ng16_np16.npz")
+    ng = int(g["ng"])
+    x, y, z = (T(g["pos"][i]) for i in range(3))
+    buf = torch.zeros((ng, ng, ng + 2), dtype=torch.float64, device=DEV)
+    pmpkg.deposit_particles(x, y, z, buf, float(g["mass"]))
+    fft = pmpkg.FFT(ng, buf)
+    fft.forward()
+    fft.apply_green(float(g["a"]))
+    fft.backward()
+    d = [torch.empty((ng, ng, ng), dtype=torch.float64, device=DEV) for _ in range(3)]
+    pmpkg.centered_derivatives(buf, *d)
+    p = [torch.zeros_like(x) for _ in range(3)]
+    pmpkg.update_particles(x, y, z, *d, *p, float(g["a"]))
+    assert rel(np.stack([H(a) for a in p]), g["mom"]) < 1e-12
+
+
+@pytest.mark.parametrize("ng,nrow,kind,order", [(64, 64, "discrete", 2), (128, 64, "spectral", 4),
+                                                (256, 256, "discrete", 2)])
+def test_full_step_f64_vs_oracle(pmpkg, O, ng, nrow, kind, order):
+    x, y, z = uniform(ng, nrow ** 3, ng + nrow)
+    mass = ng ** 3 / nrow ** 3
+    cp, ck = 4 * np.pi, 0.01
+    kid = 0 if kind == "discrete" else 1
+    p = [np.zeros(nrow ** 3) for _ in range(3)]
+    delta, phi, f = O.force_step(ng, x, y, z, *p, mass, cp, ck, kid, order)
+    plan = pmpkg.Plan(ng, "fp64", kind, order)
+    tx = [T(a) for a in (x, y, z)]
+    tp = [torch.zeros_like(tx[0]) for _ in range(3)]
+    plan.step(*tx, *tp, mass, cp, ck, 0.0)
+    phi_g = H(plan.workspace_mesh())
+    assert rel(phi_g[:, :, :ng], phi[:, :, :ng]) < 1e-12
+    assert rel(np.stack([H(a) for a in tp]), np.stack(p)) < 1e-12
+
+
+# ------------------------------------------------------------- FP32 split
+
+def test_split_join(pmpkg, O):
+    ng, np_ = 64, 100000
+    x, y, z = uniform(ng, np_, 2)
+    x[:3] = [0.0, ng - 1e-12, 5.0 - 1e-17]
+    plan = pmpkg.Plan(ng, "fp32")
+    cell, off = plan.split(T(x), T(y), T(z))
+    ocell, ooff = O.split_positions(ng, x, y, z)
+    back = plan.join(cell, off)
+    for a, b in zip(back, (x, y, z)):
+        d = np.abs(H(a) - b)
+        d = np.minimum(d, ng - d)
+        assert d.max() <= 2 ** -24
+    assert np.all(H(off[0]) < 1.0) and np.all(H(off[0]) >= 0.0)
+
+
+@pytest.mark.parametrize("ng,nrow,kind,order", [(64, 64, "discrete", 2), (64, 32, "spectral", 4),
+                                                (128, 64, "spectral", 4)])
+def test_split_forces_within_1e4_of_fp64(pmpkg, O, ng, nrow, kind, order):
+    pos, vel = O.zeldovich_ic(ng, nrow, -2.0, 0.5, seed=ng + nrow)
+    mass = ng ** 3 / nrow ** 3
+    cp = 4 * np.pi
+    kid = 0 if kind == "discrete" else 1
+    fr = [np.zeros(nrow ** 3) for _ in range(3)]
+    delta, phi, f = O.force_step(ng, *pos, *fr, mass, cp, 1.0, kid, order)
+    plan = pmpkg.Plan(ng, "fp32", kind, order)
+    cell, off = plan.split(*(T(a) for a in pos))
+    mesh = plan.deposit_split(cell, off, mass)
+    assert rel(H(mesh)[:, :, :ng], delta[:, :, :ng]) < 1e-6
+    plan.poisson(mesh, cp)
+    assert rel(H(mesh)[:, :, :ng], phi[:, :, :ng]) < 1e-4
+    g = plan.interp_split(mesh, cell, off)
+    err = rel(np.stack([H(a) for a in g]), np.stack(fr))
+    assert err < 1e-4, err
+
+
+def test_split_step_kick_drift(pmpkg, O):
+    ng, nrow = 64, 32
+    pos, vel = O.zeldovich_ic(ng, nrow, -2.0, 0.5, seed=3)
+    mass = ng ** 3 / nrow ** 3
+    cp, dt = 4 * np.pi, 0.5
+    # oracle: force at x, v += f dt, x += v dt
+    x, y, z = (a.copy() for a in pos)
+    v = [a.copy() for a in vel]
+    O.force_step(ng, x, y, z, *v, mass, cp, dt, 1, 4)
+    O.drift(ng, x, y, z, *v, dt)
+    plan = pmpkg.Plan(ng, "fp32", "spectral", 4)
+    cell, off = plan.split(*(T(a) for a in pos))
+    tv = [T(a, torch.float32) for a in vel]
+    plan.step_split(cell, off, tv, mass, cp, dt, dt)
+    assert rel(np.stack([H(a) for a in tv]), np.stack(v)) < 1e-5
+    got = plan.join(cell, off)
+    for a, b in zip(got, (x, y, z)):
+        d = np.abs(H(a) - b)
+        d = np.minimum(d, ng - d)
+        assert d.max() < 1e-4
+
+
+# ---------------------------------------------------- initial conditions
+
+@pytest.mark.parametrize("ng,nrow,ns,rms", [(16, 16, -2.0, 0.3), (64, 32, -1.5, 1.0)])
+def test_zeldovich_ic_matches_oracle(pmpkg, O, ng, nrow, ns, rms):
+    pos, vel = pmpkg.zeldovich_ic(ng, nrow, ns, rms, seed=42, device=DEV)
+    opos, ovel = O.zeldovich_ic(ng, nrow, ns, rms, seed=42)
+    assert rel(np.stack([H(a) for a in vel]), np.stack(ovel)) < 1e-12
+    for a, b in zip(pos, opos):
+        d = np.abs(H(a) - b)
+        d = np.minimum(d, ng - d)
+        assert d.max() < 1e-11
+
+
+def test_kdk_run_f64_matches_oracle(pmpkg, O):
+    """10 KDK steps (spectral Poisson, 4-point gradient), 32^3 on 32^3."""
+    ng = nrow = 32
+    pos, vel = O.zeldovich_ic(ng, nrow, -2.0, 0.3, seed=1)
+    cp, dt, steps = 4 * np.pi, 0.01, 10
+    x, y, z = (a.copy() for a in pos)
+    v = [a.copy() for a in vel]
+    O.kdk(ng, x, y, z, *v, 1.0, cp, dt, steps, 1, 4)
+    plan = pmpkg.Plan(ng, "fp64", "spectral", 4)
+    tx = [T(a) for a in pos]
+    tv = [T(a) for a in vel]
+    for s in range(steps + 1):
+        ck = 0.5 * dt if s in (0, steps) else dt
+        plan.step(*tx, *tv, 1.0, cp, ck, dt if s < steps else 0.0)
+    assert rel(np.stack([H(a) for a in tv]), np.stack(v)) < 1e-11
+    for a, b in zip(tx, (x, y, z)):
+        d = np.abs(H(a) - b)
+        assert np.minimum(d, ng - d).max() < 1e-11
+
+
+# --------------------------------------------------------------- errors
+
+def test_errors_are_reported(pmpkg):
+    plan = pmpkg.Plan(16, "fp64")
+    x = torch.full((4,), 3.0, dtype=torch.float64, device=DEV)
+    x[1] = float("nan")
+    x[2] = 17.5
+    y = torch.ones_like(x)
+    z = torch.ones_like(x)
+    plan.deposit(x, y, z, 1.0)
+    with pytest.raises(pmpkg.PMError) as e:
+        plan.check()
+    assert e.value.code == 5  # PM_ERR_RANGE
+    plan.check()  # flag was cleared
+    with pytest.raises(pmpkg.PMError) as e:
+        pmpkg.Plan(12, "fp64")
+    assert e.value.code == 2  # PM_ERR_SIZE
+    p32 = pmpkg.Plan(16, "fp32")
+    with pytest.raises(pmpkg.PMError):
+        p32.deposit(x, y, z, 1.0)  # FP64 entry point on an FP32 plan
+    with pytest.raises(pmpkg.PMError):
+        plan.deposit(x.float(), y, z, 1.0)
