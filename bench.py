@@ -1,0 +1,420 @@
+#!/usr/bin/env python
+"""Throughput of the particle-mesh step on B200: particle-updates/s.
+
+Workload (default): 512^3 particles on a 1024^3 periodic mesh, Zel'dovich
+initial conditions (P(k) ~ k^-1.5, rms displacement 1.0 cell, seeded,
+synthetic), spectral Poisson, 4-point gradient, leapfrog step of dt = 0.005.
+One step = deposit, Poisson solve, gradient + interpolation + kick + drift
+over every particle; particle-updates/s = particles x steps / time.
+
+  value      the FP32 split-position path (the fast path), inputs resident in
+             HBM, K steps timed with CUDA events (max over ranks)
+  fp64       the plain FP64 path on the same initial state
+  force_err  relative L2 of FP32 vs FP64 particle forces on that state
+  e2e        the FP32 step through the C ABI with the particle state copied
+             from pinned host memory and back every step
+  roofline   dominant kernel, algorithmic bytes / CUDA-event time, vs the
+             measured HBM copy bandwidth
+  cpu_baseline the reference's CPU code on a bounded sample (rank 0, N = 1)
+
+Multi-GPU (torchrun): every rank advances its own box (seed + rank) with no
+collective on the data path; the timing is the max over ranks (weak scaling).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "particle-mesh_b200"))
+
+METRIC = "PM particle-updates/s, 512^3 on 1024^3 mesh: FP32 vs FP64 at force err <=1e-4"
+UNIT = "particle-updates/s"
+N_S, RMS, DT, SEED = -1.5, 1.0, 0.005, 1000
+CPU_SAMPLE = (256, 128)  # (mesh, particles per side): 1/64 of the workload
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ng", type=int, default=1024)
+    ap.add_argument("--nrow", type=int, default=512)
+    ap.add_argument("--skip-fp64", action="store_true")
+    ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples every 200 ms while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, bus_id=None):
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"]
+        if bus_id:
+            cmd += ["-i", bus_id]
+        try:
+            self.p = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        out, _ = self.p.communicate(timeout=10)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in out.strip().splitlines():
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def bus_id(torch, dev):
+    try:
+        p = torch.cuda.get_device_properties(dev)
+        return f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"
+    except Exception:  # noqa: BLE001
+        return None
+
+
+# ------------------------------------------------------------- byte model
+def stage_bytes(stage: str, ng: int, np_: int, esz: int) -> float:
+    """Algorithmic bytes of one launch of a stage (the minimum it must move).
+
+    mesh passes read and write the padded mesh once; particle stages read
+    (and write) their particle arrays once and read each mesh cell once."""
+    mesh = ng * ng * (ng + 2) * esz
+    cells = ng ** 3
+    if stage == "mesh_init":
+        return mesh
+    if stage.startswith("fft_") or stage == "green":
+        return 2.0 * mesh
+    if esz == 4:  # split positions: cell 4 + offsets 12 (+ velocity 12)
+        return {"deposit": 16 * np_ + 2 * mesh, "kick_drift": 56 * np_ + cells * 4,
+                "interp": 16 * np_ + 12 * np_ + cells * 4}.get(stage, 0.0)
+    return {"deposit": 24 * np_ + 2 * mesh, "gradient": mesh + 3 * cells * 8,
+            "interp_kick": 72 * np_ + 3 * cells * 8, "drift": 72 * np_}.get(stage, 0.0)
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            j = json.load(f)
+        return float(j["hbm_gbs"]), "measured"
+    except Exception:  # noqa: BLE001
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(stage: str, ng: int):
+    """DRAM bytes per launch of a stage from the committed ncu summary, if any."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
+            j = json.load(f)
+        e = j.get(f"{stage}@{ng}")
+        return float(e["dram_bytes_per_launch"]) if e else None
+    except Exception:  # noqa: BLE001
+        return None
+
+
+# -------------------------------------------------------------- CPU side
+def cpu_reference_steps(steps: int, warmup: int, budget_s: float | None = None):
+    """The reference's CPU step (its own compiled kernels from oracle/_ref,
+    scipy.fft with all cores standing in for FFTW) plus a drift, on the
+    bounded sample: 128^3 particles on a 256^3 periodic mesh with the same
+    initial-condition recipe -- 1/64 of the workload, one rank's share of a
+    64-rank run.  The OpenMP thread count is the fastest of a few candidates
+    found in the warm-up.  Returns (particle-updates/s, threads, seconds)."""
+    import numpy as np
+    import scipy.fft
+    from oracle import oracle as O
+
+    ng, nrow = CPU_SAMPLE
+    R = O.ref_lib()
+    kind = "reference" if R is not None else "port"
+    cores = len(os.sched_getaffinity(0))
+    pos, vel = O.zeldovich_ic(ng, nrow, N_S, RMS, SEED)
+    x, y, z = (np.ascontiguousarray(a) for a in pos)
+    v = [np.ascontiguousarray(a) for a in vel]
+    mass = ng ** 3 / nrow ** 3
+    a_ref = O.START_A
+    rfftn = lambda a, **k: scipy.fft.rfftn(a, workers=cores, **k)  # noqa: E731
+    irfftn = lambda a, **k: scipy.fft.irfftn(a, workers=cores, **k)  # noqa: E731
+    steppers = {}
+
+    def one(threads):
+        t0 = time.perf_counter()
+        if R is not None:
+            if threads not in steppers:
+                steppers[threads] = O.ReferenceStepper(ng, a_ref, threads, rfftn, irfftn)
+                steppers[threads].keep = False
+            steppers[threads].step(x, y, z, *v, mass)
+        else:
+            cp, ck = O.reference_coefficients(a_ref)
+            O.force_step(ng, x, y, z, *v, mass, cp, ck, fft="numpy")
+        O.drift(ng, x, y, z, *v, DT)
+        return time.perf_counter() - t0
+
+    try:
+        cands = sorted({cores, max(1, cores // 2), max(1, cores // 4), min(cores, 16), min(cores, 8)}, reverse=True)
+        if R is not None:
+            for c in cands:  # first call of each pays its setup
+                one(c)
+            best = min(cands, key=one)
+        else:
+            best = 1
+        for _ in range(max(0, warmup - 1)):
+            one(best)
+        ts = []
+        t_start = time.perf_counter()
+        for _ in range(steps):
+            ts.append(one(best))
+            if budget_s and time.perf_counter() - t_start > budget_s:
+                break
+        stage_s = None
+        if R is not None:
+            st = steppers[best]
+            stage_s = dict(st.timers)
+    finally:
+        for st in steppers.values():
+            st.close()
+    t = sum(ts) / len(ts)
+    per_step = {k: v / (len(ts) + max(0, warmup - 1) + 2) for k, v in (stage_s or {}).items()}
+    return {"value": nrow ** 3 / t, "omp_threads": best, "cores": cores, "seconds": t, "steps": len(ts),
+            "kind": kind, "stage_s_approx": per_step}
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    steps = max(1, args.steps)
+    r = cpu_reference_steps(steps, args.warmup)
+    val, t, n, kind = r["value"], r["seconds"], r["steps"], r["kind"]
+    ng, nrow = CPU_SAMPLE
+    sample = (f"{nrow}^3 particles on a {ng}^3 periodic mesh (1/64 of the workload: one rank's share of a "
+              f"64-rank run), same Zel'dovich recipe; reference kernels from oracle/_ref, scipy.fft for FFTW")
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": n, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{args.nrow}^3 particles on {args.ng}^3 mesh, sampled on the CPU as {sample}"},
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": r["cores"], "omp_threads": r["omp_threads"],
+                             "kind": kind, "sample": sample},
+            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# -------------------------------------------------------------- GPU side
+def ours(args):
+    import torch
+    import torch.distributed as dist
+    from loader import load_package
+
+    pm = load_package()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(v: float) -> float:
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    ng, nrow = args.ng, args.nrow
+    np_ = nrow ** 3
+    mass = ng ** 3 / np_
+    cp, ck = pm.unit_box_coefficients(DT)
+    stream = torch.cuda.current_stream(dev)
+
+    pos, vel = pm.zeldovich_ic(ng, nrow, N_S, RMS, SEED + rank, device=dev)
+    p32 = pm.Plan(ng, "fp32", "spectral", 4, stream=stream, device=dev)
+    cell, off = p32.split(*pos)
+    v32 = [a.float() for a in vel]
+    torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        p32.step_split(cell, off, v32, mass, cp, ck, DT)
+    p32.check()
+    p32.read_timing(reset=True)
+    p32.set_timing(True)
+    barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(bus_id(torch, dev))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        p32.step_split(cell, off, v32, mass, cp, ck, DT)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    barrier()
+    p32.set_timing(False)
+    t_ms = max_over_ranks(e0.elapsed_time(e1))
+    stages = p32.read_timing(reset=True)
+    p32.check()
+    value = world * np_ * args.steps / (t_ms / 1e3)
+    launches = sum(n for _, n in stages.values())
+
+    peak, peak_kind = measured_peaks()
+    dom = max(stages, key=lambda s: stages[s][0])
+    dom_ms = stages[dom][0] / stages[dom][1]
+    dom_bytes = stage_bytes(dom, ng, np_, 4)
+    achieved = dom_bytes / (dom_ms / 1e3) / 1e9
+    traffic = ncu_traffic(dom, ng)
+    step_bytes = sum(stage_bytes(s, ng, np_, 4) * n / args.steps for s, (_, n) in stages.items())
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs (copy bandwidth)",
+                "traffic": traffic, "algorithmic_bytes_per_launch": dom_bytes, "ms_per_launch": dom_ms,
+                "step": {"algorithmic_bytes": step_bytes, "achieved": step_bytes / (t_ms / args.steps / 1e3) / 1e9,
+                         "frac": step_bytes / (t_ms / args.steps / 1e3) / 1e9 / peak}}
+    per_stage = {s: {"ms_per_step": ms / args.steps, "launches": n,
+                     "gbs": stage_bytes(s, ng, np_, 4) * n / (ms / 1e3) / 1e9 if ms > 0 else None}
+                 for s, (ms, n) in stages.items()}
+
+    # ---- FP64 plain path on the same initial state + force error
+    fp64 = None
+    force_err = None
+    if not args.skip_fp64:
+        p64 = pm.Plan(ng, "fp64", "spectral", 4, stream=stream, device=dev)
+        x, y, z = (a.clone() for a in pos)
+        pv = [a.clone() for a in vel]
+        # forces at the initial state: FP64 plain vs FP32 split
+        zero = [torch.zeros_like(x) for _ in range(3)]
+        p64.step(x, y, z, *zero, mass, cp, 1.0, 0.0)
+        c0, o0 = p32.split(*pos)
+        m32 = p32.deposit_split(c0, o0, mass, p32.workspace_mesh())
+        p32.poisson(m32, cp)
+        f32 = p32.interp_split(m32, c0, o0)
+        num = sum(float(((a.double() - b) ** 2).sum()) for a, b in zip(f32, zero))
+        den = sum(float((b ** 2).sum()) for b in zero)
+        force_err = math.sqrt(num / den)
+        del zero, c0, o0, f32
+        for _ in range(args.warmup):
+            p64.step(x, y, z, *pv, mass, cp, ck, DT)
+        barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            p64.step(x, y, z, *pv, mass, cp, ck, DT)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        t64 = max_over_ranks(e0.elapsed_time(e1))
+        fp64 = {"value": world * np_ * args.steps / (t64 / 1e3), "unit": UNIT, "ms_per_step": t64 / args.steps,
+                "dtype": "f64"}
+        p64.close()
+        del p64, x, y, z, pv
+        torch.cuda.empty_cache()
+
+    # ---- end to end through the C ABI with host buffers
+    e2e = None
+    if not args.skip_e2e:
+        host = [torch.empty(np_, dtype=t.dtype, pin_memory=True) for t in [cell, *off, *v32]]
+        for h, d in zip(host, [cell, *off, *v32]):
+            h.copy_(d)
+        dbuf = [cell, *off, *v32]
+        nbytes = sum(h.numel() * h.element_size() for h in host)
+
+        def e2e_step():
+            for h, d in zip(host, dbuf):
+                d.copy_(h, non_blocking=True)
+            p32.step_split(cell, off, v32, mass, cp, ck, DT)
+            for h, d in zip(host, dbuf):
+                h.copy_(d, non_blocking=True)
+
+        for _ in range(max(1, args.warmup)):
+            e2e_step()
+        barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            e2e_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        te = max_over_ranks(e0.elapsed_time(e1))
+        e2e = {"value": world * np_ * args.steps / (te / 1e3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
+               "d2h_bytes_per_step": nbytes, "ms_per_step": te / args.steps,
+               "path": "pm_step_f32 through the C ABI; particle state copied from pinned host memory and back "
+                       "every step"}
+        del host
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        r = cpu_reference_steps(3, 1, budget_s=30.0)
+        ng_s, nrow_s = CPU_SAMPLE
+        cpu = {"value": r["value"], "unit": UNIT, "cores": r["cores"], "omp_threads": r["omp_threads"],
+               "kind": r["kind"],
+               "sample": f"{nrow_s}^3 particles on a {ng_s}^3 periodic mesh (1/64 of the workload: one rank's "
+                         f"share of a 64-rank run), {r['steps']} steps of {r['seconds']:.3f} s; reference kernels "
+                         f"(oracle/_ref) with the OpenMP thread count that ran fastest, scipy.fft on all cores "
+                         f"standing in for FFTW"}
+
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{nrow}^3 particles on {ng}^3 mesh, FP32 mesh/FFT/forces, split positions, "
+                                   f"spectral Poisson, 4-point gradient, KDK dt={DT}, Zel'dovich P(k)~k^{N_S} "
+                                   f"rms {RMS} cell",
+                       "particles_per_gpu": np_, "mesh": ng, "l2": "inputs larger than L2 (mesh 4.3 GB)",
+                       "parallelism": f"{world} independent boxes, one per GPU"},
+            "fp64": fp64, "force_err": force_err,
+            "speedup_fp32_vs_fp64": (value / fp64["value"]) if fp64 else None,
+            "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "stages": per_stage,
+            "cpu_baseline": cpu, "clocks": clocks}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return reference_arm(args)
+    return ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -89,6 +89,18 @@ int pm_plan_check(pm_plan* plan);
 /* Message of the calling thread's last failed call ("" if none). */
 const char* pm_last_error(void);
 
+/* Per-kernel stage timers: the B200 form of the reference's per-stage
+ * wall-clock buckets (src/utils/utils.cpp:3-20, src/core/main.cpp:88-143).
+ * Launch counts per stage are always kept; with timing on, every kernel is
+ * bracketed by CUDA events on the plan's stream.  pm_plan_read_timing waits
+ * for the stream and fills ms[PM_STAGE_COUNT] (summed milliseconds) and
+ * launches[PM_STAGE_COUNT] (either may be NULL); reset != 0 zeroes both. */
+#define PM_STAGE_COUNT 16
+int pm_plan_set_timing(pm_plan* plan, int on);
+int pm_plan_read_timing(pm_plan* plan, double* ms, int64_t* launches, int reset);
+/* Name of stage i ("mesh_init", "deposit", "fft_z_r2c", ...), "" if out of range. */
+const char* pm_stage_name(int stage);
+
 /* ------------------------------------------- FP64 stages (PM_FP64 plan) */
 
 /* delta = -1 + sum_p mass * W_CIC(x_p - c), periodic; writes every cell of

@@ -261,75 +261,121 @@ def green_table_reference(ng: int, c_poisson: float) -> np.ndarray:
     return g
 
 
-def reference_force_step(ng, x, y, z, px, py, pz, mass, a=START_A, threads=None, timers=None):
-    """The reference step at P = 1 through the reference's own compiled code.
+class ReferenceStepper:
+    """The reference step at P = 1 through the reference's own compiled code,
+    with its setup done once as in src/core/main.cpp:42-69 (buffers, FFT /
+    Green's table, ReorderSlab / ReorderSlabBack plans).
 
-    Stages (src/core/main.cpp:90-139):
+    Stages of step() (src/core/main.cpp:90-139):
       init_buf + deposit_particles + reduce_private_to_shared   (reference code)
       TransposeSlab: at P = 1 the exchange is the identity on the (ng+1)^3
         cube; ReorderSlab folds the x = ng ghost plane as its own chunk
         (the single-rank form of transpose_slab.cpp:23-27)      (reference code)
-      FFT forward / Green / FFT backward: numpy.fft stands in for FFTW,
-        Green restated from fft.cpp:50-57,75-82
+      FFT forward / Green / FFT backward: numpy.fft (or a drop-in such as
+        scipy.fft) stands in for FFTW; Green's table of fft.cpp:50-57
       ReorderSlabBack (y, z ghosts)                             (reference code)
       TransposeSlabBack: x ghosts -1/+2 as periodic planes (the single-rank
         form of transpose_slab_back.cpp:22-44)
       centered_derivatives + update_particles                   (reference code)
-    Returns dict with delta (slab), phi (slab), forces ((ng+1)^3 each)."""
-    import time
-    R = ref_lib()
-    if R is None:
-        raise RuntimeError("oracle/_ref is not built")
-    T = int(threads or R.ref_max_threads())
-    R.ref_set_threads(T)
-    clock = time.perf_counter
-    t = [clock()]
+    The per-stage wall times accumulate in .timers (seconds), the reference's
+    own 9 buckets (main.cpp:88-143)."""
 
-    def mark(name):
-        t.append(clock())
+    BUCKETS = ("cic", "alltoallv", "reorder", "fft", "green", "ifft", "reorder_back", "alltoallv_back", "update")
+
+    def __init__(self, ng, a=START_A, threads=None, rfftn=None, irfftn=None):
+        R = ref_lib()
+        if R is None:
+            raise RuntimeError("oracle/_ref is not built")
+        self.R, self.ng, self.a = R, ng, a
+        self.T = int(threads or R.ref_max_threads())
+        self.rfftn = rfftn or np.fft.rfftn
+        self.irfftn = irfftn or (lambda s_, **k: np.fft.irfftn(s_, **k))
+        n = ng
+        self.nx = n + 1
+        self.ncell = self.nx ** 3
+        self.buf = np.empty(self.T * self.ncell, np.float64)
+        self.stride = n + 2
+        rc = (ctypes.c_int * 2)(n * self.nx * self.nx, self.nx * self.nx)
+        rd = (ctypes.c_int * 2)(0, n * self.nx * self.nx)
+        dims = (ctypes.c_int * 3)(2, 1, 1)
+        self.h = R.ref_reorder_slab_create(n, self.nx, self.nx, n, self.stride, rc, rd, 2, dims)
+        dims1 = (ctypes.c_int * 3)(1, 1, 1)
+        self.hb = R.ref_reorder_slab_back_create(n, n, n, self.stride, dims1, n)
+        self.green = green_table_reference(n, 3.0 * OMEGA_0 / (2.0 * a))
+        self.slab = np.zeros((n, n, self.stride), np.float64)
+        self.phi = np.zeros((n, n, self.stride), np.float64)
+        self.yz = np.zeros((n, n + 3, n + 3), np.float64)
+        self.ghost_index = (np.arange(n + 3) - 1) % n
+        self.d = [np.zeros(self.ncell, np.float64) for _ in range(3)]
+        self.timers = {b: 0.0 for b in self.BUCKETS}
+
+    def close(self):
+        if self.h:
+            self.R.ref_reorder_slab_destroy(self.h)
+            self.R.ref_reorder_slab_back_destroy(self.hb)
+            self.h = self.hb = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001
+            pass
+
+    def step(self, x, y, z, px, py, pz, mass):
+        import time
+        R, n, T = self.R, self.ng, self.T
+        R.ref_set_threads(T)
+        clock = time.perf_counter
+        t = [clock()]
+
+        def mark(name):
+            t.append(clock())
+            self.timers[name] += t[-1] - t[-2]
+
+        nx = self.nx
+        R.ref_init_buf(_ptr(self.buf), nx, nx, nx, self.ncell, T)
+        R.ref_deposit_particles(_ptr(x), _ptr(y), _ptr(z), x.size, _ptr(self.buf), self.ncell, nx, nx, nx,
+                                0, 0, 0, float(mass))
+        R.ref_reduce_private_to_shared(_ptr(self.buf), self.ncell, T)
+        mark("cic")
+        mark("alltoallv")  # identity at P = 1: the recv buffer is the cube itself
+        R.ref_reorder_slab_execute(self.h, _ptr(self.buf), _ptr(self.slab))
+        mark("reorder")
+        delta = self.slab.copy() if self.keep else None
+        spec = self.rfftn(self.slab[:, :, :n])
+        mark("fft")
+        spec *= self.green
+        mark("green")
+        self.phi[:, :, :n] = self.irfftn(spec, s=(n, n, n), axes=(0, 1, 2))
+        self.phi[:, :, :n] *= float(n) ** 3
+        mark("ifft")
+        R.ref_reorder_slab_back_execute(self.hb, _ptr(self.phi), _ptr(self.yz))
+        mark("reorder_back")
+        ghost = np.ascontiguousarray(self.yz[self.ghost_index])
+        mark("alltoallv_back")
+        R.ref_centered_derivatives(_ptr(ghost), *(_ptr(a) for a in self.d), n + 3, n + 3, n + 3)
+        R.ref_update_particles(_ptr(x), _ptr(y), _ptr(z), *(_ptr(a) for a in self.d), _ptr(px), _ptr(py),
+                               _ptr(pz), float(self.a), x.size, nx, nx, 0, 0, 0)
+        mark("update")
+        if not self.keep:
+            return None
+        return {"delta": delta, "phi": self.phi.copy(), "forces": [a.reshape(nx, nx, nx).copy() for a in self.d]}
+
+    keep = True
+
+
+def reference_force_step(ng, x, y, z, px, py, pz, mass, a=START_A, threads=None, timers=None):
+    """One reference step at P = 1 (see ReferenceStepper); returns dict with
+    delta (slab), phi (slab), forces ((ng+1)^3 each)."""
+    st = ReferenceStepper(ng, a, threads)
+    try:
+        r = st.step(x, y, z, px, py, pz, mass)
         if timers is not None:
-            timers[name] = timers.get(name, 0.0) + t[-1] - t[-2]
-
-    n = ng
-    nx = ny = nz = n + 1
-    ncell = nx * ny * nz
-    buf = np.empty(T * ncell, np.float64)
-    R.ref_init_buf(_ptr(buf), nx, ny, nz, ncell, T)
-    R.ref_deposit_particles(_ptr(x), _ptr(y), _ptr(z), x.size, _ptr(buf), ncell, nx, ny, nz, 0, 0, 0, float(mass))
-    R.ref_reduce_private_to_shared(_ptr(buf), ncell, T)
-    mark("cic")
-    stride = n + 2
-    rc = (ctypes.c_int * 2)(n * ny * nz, ny * nz)
-    rd = (ctypes.c_int * 2)(0, n * ny * nz)
-    dims = (ctypes.c_int * 3)(2, 1, 1)
-    h = R.ref_reorder_slab_create(n, ny, nz, n, stride, rc, rd, 2, dims)
-    slab = np.zeros((n, n, stride), np.float64)
-    mark("setup")
-    R.ref_reorder_slab_execute(h, _ptr(buf), _ptr(slab))
-    R.ref_reorder_slab_destroy(h)
-    mark("reorder")
-    delta = slab.copy()
-    spec = np.fft.rfftn(slab[:, :, :n])
-    mark("fft")
-    spec *= green_table_reference(n, 3.0 * OMEGA_0 / (2.0 * a))
-    mark("green")
-    phi = np.zeros((n, n, stride), np.float64)
-    phi[:, :, :n] = np.fft.irfftn(spec, s=(n, n, n), axes=(0, 1, 2)) * float(n) ** 3
-    mark("ifft")
-    dims1 = (ctypes.c_int * 3)(1, 1, 1)
-    hb = R.ref_reorder_slab_back_create(n, n, n, stride, dims1, n)
-    yz = np.zeros((n, n + 3, n + 3), np.float64)
-    R.ref_reorder_slab_back_execute(hb, _ptr(phi), _ptr(yz))
-    R.ref_reorder_slab_back_destroy(hb)
-    mark("reorder_back")
-    ghost = np.ascontiguousarray(yz[(np.arange(n + 3) - 1) % n])
-    mark("transpose_back")
-    d = [np.zeros(ncell, np.float64) for _ in range(3)]
-    R.ref_centered_derivatives(_ptr(ghost), *(_ptr(a) for a in d), n + 3, n + 3, n + 3)
-    R.ref_update_particles(_ptr(x), _ptr(y), _ptr(z), *(_ptr(a) for a in d), _ptr(px), _ptr(py), _ptr(pz),
-                           float(a), x.size, ny, nz, 0, 0, 0)
-    mark("update")
-    return {"delta": delta, "phi": phi, "forces": [a.reshape(nx, ny, nz) for a in d]}
+            for k, v in st.timers.items():
+                timers[k] = timers.get(k, 0.0) + v
+        return r
+    finally:
+        st.close()
 
 
 def reference_init_particles(ng: int, nrow: int, rank: int = 0):

@@ -27,6 +27,8 @@ SIGNATURES = {
     "pm_plan_device_bytes": [_V, ctypes.POINTER(_SZ)],
     "pm_plan_check": [_V],
     "pm_plan_mesh": [_V, ctypes.POINTER(_V)],
+    "pm_plan_set_timing": [_V, _I],
+    "pm_plan_read_timing": [_V, _V, _V, _I],
     "pm_deposit_f64": [_V, _V, _V, _V, _L, _D, _V],
     "pm_fft_r2c_f64": [_V, _V],
     "pm_green_f64": [_V, _V, _D],
@@ -69,6 +71,9 @@ def header_symbols() -> list[str]:
     return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(pm_\w+)\s*\(", text, re.M)))
 
 
+STAGE_COUNT = 16
+
+
 def load(build_if_missing: bool = True) -> ctypes.CDLL:
     """Loads libpm_b200.so (building it with nvcc if absent or stale)."""
     global _lib
@@ -93,6 +98,8 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
         fn.restype = ctypes.c_int
     L.pm_last_error.argtypes = []
     L.pm_last_error.restype = ctypes.c_char_p
+    L.pm_stage_name.argtypes = [_I]
+    L.pm_stage_name.restype = ctypes.c_char_p
     _lib = L
     return L
 

@@ -25,6 +25,32 @@ int cuda_fail(cudaError_t e, const char* what) {
     return fail(PM_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+static const char* kStageNames[ST_COUNT] = {
+    "mesh_init", "deposit", "fft_z_r2c", "fft_y_fwd", "fft_x_fwd", "green", "fft_x_green",
+    "fft_x_inv", "fft_y_inv", "fft_z_c2r", "gradient", "interp_kick", "drift", "kick_drift",
+    "interp", "split"};
+
+const char* stage_name(int st) { return st >= 0 && st < ST_COUNT ? kStageNames[st] : ""; }
+
+cudaEvent_t StageTimers::get() {
+    if (pool.empty()) {
+        cudaEvent_t e = nullptr;
+        cudaEventCreate(&e);
+        return e;
+    }
+    cudaEvent_t e = pool.back();
+    pool.pop_back();
+    return e;
+}
+
+StageTimers::~StageTimers() {
+    for (auto& r : pending) {
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    for (auto e : pool) cudaEventDestroy(e);
+}
+
 namespace {
 
 template <typename T> int upload_tables(Plan& p) {
@@ -56,6 +82,8 @@ void release(Plan& p) {
         if (f) cudaFree(f), f = nullptr;
     p.tw = p.lap1d = p.mesh = nullptr;
     p.d_err = nullptr;
+    delete p.timers;
+    p.timers = nullptr;
 }
 
 int ensure_workspace(Plan& p, bool forces) {
@@ -145,6 +173,10 @@ int pm_plan_create(int ng, int precision, int green_kind, int grad_order, void* 
             rc = fail(PM_ERR_NOMEM, "error word allocation failed");
     }
     if (rc == PM_OK) rc = fft_prepare(p);
+    if (rc == PM_OK) {
+        p.timers = new (std::nothrow) StageTimers();
+        if (!p.timers) rc = fail(PM_ERR_NOMEM, "host allocation failed");
+    }
     if (rc != PM_OK) {
         cudaGetLastError();
         release(p);
@@ -180,6 +212,37 @@ int pm_plan_check(pm_plan* plan) {
     if (h & ERRBIT_RANGE) return fail(PM_ERR_RANGE, "a particle position was NaN or outside [0, ng); it was wrapped");
     return PM_OK;
 }
+
+int pm_plan_set_timing(pm_plan* plan, int on) {
+    if (!plan) return fail(PM_ERR_ARG, "plan is NULL");
+    plan->p.timers->on = on != 0;
+    return PM_OK;
+}
+
+int pm_plan_read_timing(pm_plan* plan, double* ms, int64_t* launches, int reset) {
+    if (!plan) return fail(PM_ERR_ARG, "plan is NULL");
+    PM_TRY(set_device(plan->p));
+    StageTimers& t = *plan->p.timers;
+    if (!t.pending.empty()) PMB_CUDA_CHECK(cudaStreamSynchronize(plan->p.stream));
+    for (auto& r : t.pending) {
+        float e = 0.f;
+        if (cudaEventElapsedTime(&e, r.a, r.b) == cudaSuccess) t.ms[r.stage] += e;
+        t.pool.push_back(r.a);
+        t.pool.push_back(r.b);
+    }
+    t.pending.clear();
+    for (int i = 0; i < ST_COUNT; ++i) {
+        if (ms) ms[i] = t.ms[i];
+        if (launches) launches[i] = t.launches[i];
+        if (reset) {
+            t.ms[i] = 0.0;
+            t.launches[i] = 0;
+        }
+    }
+    return PM_OK;
+}
+
+const char* pm_stage_name(int stage) { return stage_name(stage); }
 
 int pm_plan_mesh(pm_plan* plan, void** mesh) {
     if (!plan || !mesh) return fail(PM_ERR_ARG, "NULL argument");

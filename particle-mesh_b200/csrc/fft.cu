@@ -321,6 +321,7 @@ template <typename T, int N> struct Launch {
         const unsigned grid = (unsigned)((rows + z_rows_per_block<N>() - 1) / z_rows_per_block<N>());
         const int thr = z_threads_per_row<N>() * z_rows_per_block<N>();
         const C* tw = static_cast<const C*>(p.tw);
+        Timed t(p, forward ? ST_FFT_Z_R2C : ST_FFT_Z_C2R);
         if (forward)
             k_fft_z_r2c<T, N><<<grid, thr, smem_z(), p.stream>>>(mesh, rows, tw);
         else
@@ -332,6 +333,7 @@ template <typename T, int N> struct Launch {
         const long long es = axis == 1 ? H : (long long)N * H, os = axis == 1 ? (long long)N * H : H;
         dim3 grid((H + tk_cols<T>() - 1) / tk_cols<T>(), N);
         const C* tw = static_cast<const C*>(p.tw);
+        Timed t(p, axis == 1 ? (dir < 0 ? ST_FFT_Y_FWD : ST_FFT_Y_INV) : (dir < 0 ? ST_FFT_X_FWD : ST_FFT_X_INV));
         if (dir < 0)
             k_fft_strided<T, N, -1><<<grid, strided_threads<T, N>(), smem_s(), p.stream>>>(d, es, os, H, tw);
         else
@@ -340,6 +342,7 @@ template <typename T, int N> struct Launch {
     static void xgreen(const Plan& p, T* mesh, double cg) {
         C* d = reinterpret_cast<C*>(mesh);
         dim3 grid((H + tk_cols<T>() - 1) / tk_cols<T>(), N);
+        Timed t(p, ST_FFT_X_GREEN);
         k_fft_x_green<T, N><<<grid, strided_threads<T, N>(), smem_s(), p.stream>>>(
             d, (long long)N * H, H, H, static_cast<const C*>(p.tw), static_cast<const T*>(p.lap1d), cg, p.green_kind);
     }
@@ -400,6 +403,7 @@ static double green_scale(const Plan& p, double c) {
 template <typename T> int green_apply(const Plan& p, T* mesh, double c_poisson) {
     using C = typename Cx<T>::t;
     const long long total = (long long)p.ng * p.ng * (p.ng / 2 + 1);
+    Timed t(p, ST_GREEN);
     k_green<T><<<grid_for(p, total, 256), 256, 0, p.stream>>>(
         reinterpret_cast<C*>(mesh), p.ng, static_cast<const C*>(p.tw), static_cast<const T*>(p.lap1d),
         green_scale(p, c_poisson), p.green_kind);

@@ -341,9 +341,12 @@ static constexpr int kThreads = 256;
 
 int deposit_f64(const Plan& p, const double* x, const double* y, const double* z, int64_t np,
                 double mass, double* mesh) {
-    k_mesh_init<double><<<grid_for(p, (long long)mesh_elems(p.ng), kThreads), kThreads, 0, p.stream>>>(mesh, p.ng, -1.0);
+    { Timed t(p, ST_MESH_INIT); k_mesh_init<double><<<grid_for(p, (long long)mesh_elems(p.ng), kThreads), kThreads, 0, p.stream>>>(mesh, p.ng, -1.0); }
     if (np > 0)
-        k_deposit_f64<<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(x, y, z, np, mass, mesh, p.ng, p.d_err);
+        {
+            Timed t(p, ST_DEPOSIT);
+            k_deposit_f64<<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(x, y, z, np, mass, mesh, p.ng, p.d_err);
+        }
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;
 }
@@ -351,9 +354,15 @@ int deposit_f64(const Plan& p, const double* x, const double* y, const double* z
 int gradient_f64(const Plan& p, const double* phi, double* fx, double* fy, double* fz) {
     const long long total = (long long)p.ng * p.ng * p.ng;
     if (p.grad_order == 4)
-        k_gradient_f64<4><<<grid_for(p, total, kThreads), kThreads, 0, p.stream>>>(phi, fx, fy, fz, p.ng);
+        {
+            Timed t(p, ST_GRADIENT);
+            k_gradient_f64<4><<<grid_for(p, total, kThreads), kThreads, 0, p.stream>>>(phi, fx, fy, fz, p.ng);
+        }
     else
-        k_gradient_f64<2><<<grid_for(p, total, kThreads), kThreads, 0, p.stream>>>(phi, fx, fy, fz, p.ng);
+        {
+            Timed t(p, ST_GRADIENT);
+            k_gradient_f64<2><<<grid_for(p, total, kThreads), kThreads, 0, p.stream>>>(phi, fx, fy, fz, p.ng);
+        }
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;
 }
@@ -362,8 +371,11 @@ int interp_kick_f64(const Plan& p, const double* x, const double* y, const doubl
                     const double* fx, const double* fy, const double* fz, double* px, double* py,
                     double* pz, int64_t np, double c_kick) {
     if (np == 0) return PM_OK;
-    k_interp_kick_f64<<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(x, y, z, fx, fy, fz, px, py, pz, np,
+    {
+        Timed t(p, ST_INTERP_KICK);
+        k_interp_kick_f64<<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(x, y, z, fx, fy, fz, px, py, pz, np,
                                                                           c_kick, p.ng, p.d_err);
+    }
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;
 }
@@ -371,7 +383,10 @@ int interp_kick_f64(const Plan& p, const double* x, const double* y, const doubl
 int drift_f64(const Plan& p, double* x, double* y, double* z, const double* px, const double* py,
               const double* pz, int64_t np, double dt) {
     if (np == 0) return PM_OK;
-    k_drift_f64<<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(x, y, z, px, py, pz, np, dt, p.ng);
+    {
+        Timed t(p, ST_DRIFT);
+        k_drift_f64<<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(x, y, z, px, py, pz, np, dt, p.ng);
+    }
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;
 }
@@ -379,7 +394,10 @@ int drift_f64(const Plan& p, double* x, double* y, double* z, const double* px, 
 int split_positions(const Plan& p, const double* x, const double* y, const double* z, int64_t np,
                     uint32_t* cell, float* ox, float* oy, float* oz) {
     if (np == 0) return PM_OK;
-    k_split<<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(x, y, z, np, cell, ox, oy, oz, p.ng, p.d_err);
+    {
+        Timed t(p, ST_SPLIT);
+        k_split<<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(x, y, z, np, cell, ox, oy, oz, p.ng, p.d_err);
+    }
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;
 }
@@ -387,16 +405,22 @@ int split_positions(const Plan& p, const double* x, const double* y, const doubl
 int join_positions(const Plan& p, const uint32_t* cell, const float* ox, const float* oy,
                    const float* oz, int64_t np, double* x, double* y, double* z) {
     if (np == 0) return PM_OK;
-    k_join<<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(cell, ox, oy, oz, np, x, y, z);
+    {
+        Timed t(p, ST_SPLIT);
+        k_join<<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(cell, ox, oy, oz, np, x, y, z);
+    }
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;
 }
 
 int deposit_f32(const Plan& p, const uint32_t* cell, const float* ox, const float* oy,
                 const float* oz, int64_t np, float mass, float* mesh) {
-    k_mesh_init<float><<<grid_for(p, (long long)mesh_elems(p.ng), kThreads), kThreads, 0, p.stream>>>(mesh, p.ng, -1.0f);
+    { Timed t(p, ST_MESH_INIT); k_mesh_init<float><<<grid_for(p, (long long)mesh_elems(p.ng), kThreads), kThreads, 0, p.stream>>>(mesh, p.ng, -1.0f); }
     if (np > 0)
-        k_deposit_f32<<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(cell, ox, oy, oz, np, mass, mesh, p.ng);
+        {
+            Timed t(p, ST_DEPOSIT);
+            k_deposit_f32<<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(cell, ox, oy, oz, np, mass, mesh, p.ng);
+        }
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;
 }
@@ -405,9 +429,15 @@ int interp_f32(const Plan& p, const float* phi, const uint32_t* cell, const floa
                const float* oy, const float* oz, int64_t np, float* fx, float* fy, float* fz) {
     if (np == 0) return PM_OK;
     if (p.grad_order == 4)
-        k_interp_f32<4><<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, np, fx, fy, fz, p.ng);
+        {
+            Timed t(p, ST_INTERP);
+            k_interp_f32<4><<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, np, fx, fy, fz, p.ng);
+        }
     else
-        k_interp_f32<2><<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, np, fx, fy, fz, p.ng);
+        {
+            Timed t(p, ST_INTERP);
+            k_interp_f32<2><<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, np, fx, fy, fz, p.ng);
+        }
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;
 }
@@ -416,11 +446,17 @@ int kick_drift_f32(const Plan& p, const float* phi, uint32_t* cell, float* ox, f
                    float* vx, float* vy, float* vz, int64_t np, double c_kick, double dt) {
     if (np == 0) return PM_OK;
     if (p.grad_order == 4)
-        k_kick_drift_f32<4><<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz, np,
+        {
+            Timed t(p, ST_KICK_DRIFT);
+            k_kick_drift_f32<4><<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz, np,
                                                                                 (float)c_kick, dt, p.ng);
+        }
     else
-        k_kick_drift_f32<2><<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz, np,
+        {
+            Timed t(p, ST_KICK_DRIFT);
+            k_kick_drift_f32<2><<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz, np,
                                                                                 (float)c_kick, dt, p.ng);
+        }
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;
 }

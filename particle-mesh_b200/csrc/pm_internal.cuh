@@ -6,6 +6,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <vector>
 
 #include "../../include/pm_b200.h"
 
@@ -44,6 +45,29 @@ int cuda_fail(cudaError_t e, const char* what);
         if (_e != cudaSuccess) return ::pmb::cuda_fail(_e, #expr);      \
     } while (0)
 
+// ------------------------------------------------------------ stage timers
+// Per-kernel CUDA-event timers and launch counters of a plan (the B200 form
+// of the reference's per-stage wall-clock buckets, src/utils/utils.cpp:3-20
+// and src/core/main.cpp:88-143).  Launch counts are always kept; events are
+// recorded only while timing is switched on.
+enum Stage : int {
+    ST_MESH_INIT, ST_DEPOSIT, ST_FFT_Z_R2C, ST_FFT_Y_FWD, ST_FFT_X_FWD, ST_GREEN, ST_FFT_X_GREEN,
+    ST_FFT_X_INV, ST_FFT_Y_INV, ST_FFT_Z_C2R, ST_GRADIENT, ST_INTERP_KICK, ST_DRIFT, ST_KICK_DRIFT,
+    ST_INTERP, ST_SPLIT, ST_COUNT
+};
+const char* stage_name(int st);
+
+struct StageTimers {
+    bool on = false;
+    struct Rec { int stage; cudaEvent_t a, b; };
+    std::vector<Rec> pending;
+    std::vector<cudaEvent_t> pool;
+    double ms[ST_COUNT] = {};
+    long long launches[ST_COUNT] = {};
+    cudaEvent_t get();
+    ~StageTimers();
+};
+
 // ---------------------------------------------------------------- the plan
 struct Plan {
     int ng = 0;
@@ -62,6 +86,29 @@ struct Plan {
     void* mesh = nullptr;           // workspace mesh [ng][ng][ng+2]
     void* force[3] = {nullptr, nullptr, nullptr};  // FP64 force arrays
     size_t bytes = 0;
+    StageTimers* timers = nullptr;  // owned by the C-ABI plan object
+};
+
+// Brackets one kernel launch with the plan's stage timer.
+struct Timed {
+    const Plan& p;
+    int st;
+    cudaEvent_t a = nullptr;
+    Timed(const Plan& plan, int stage) : p(plan), st(stage) {
+        if (!p.timers) return;
+        p.timers->launches[st]++;
+        if (p.timers->on) {
+            a = p.timers->get();
+            cudaEventRecord(a, p.stream);
+        }
+    }
+    ~Timed() {
+        if (a) {
+            cudaEvent_t b = p.timers->get();
+            cudaEventRecord(b, p.stream);
+            p.timers->pending.push_back({st, a, b});
+        }
+    }
 };
 
 inline size_t mesh_elems(int ng) { return (size_t)ng * ng * (ng + 2); }

@@ -79,7 +79,7 @@ class Plan:
         if precision not in _PREC or green not in _GREEN:
             raise PMError(L.PM_ERR_ARG, f"bad precision {precision!r} or green {green!r}")
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
-        self.ng, self.precision, self.green, self.grad_order = ng, precision, green, grad_order
+        self.ng, self.precision, self.green_kind, self.grad_order = ng, precision, green, grad_order
         self.dtype = torch.float64 if precision == "fp64" else torch.float32
         with torch.cuda.device(self.device):
             self.stream = stream if stream is not None else torch.cuda.current_stream(self.device)
@@ -118,6 +118,16 @@ class Plan:
         b = ctypes.c_size_t()
         check(self.lib.pm_plan_device_bytes(self._h, ctypes.byref(b)))
         return b.value
+
+    def set_timing(self, on: bool = True):
+        check(self.lib.pm_plan_set_timing(self._h, 1 if on else 0))
+
+    def read_timing(self, reset: bool = True) -> dict:
+        """{stage: (milliseconds, launches)} since the last reset."""
+        ms = (ctypes.c_double * L.STAGE_COUNT)()
+        n = (ctypes.c_int64 * L.STAGE_COUNT)()
+        check(self.lib.pm_plan_read_timing(self._h, ms, n, 1 if reset else 0))
+        return {self.lib.pm_stage_name(i).decode(): (ms[i], n[i]) for i in range(L.STAGE_COUNT) if n[i]}
 
     def new_mesh(self) -> torch.Tensor:
         return torch.zeros((self.ng, self.ng, self.ng + 2), dtype=self.dtype, device=self.device)

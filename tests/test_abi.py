@@ -17,7 +17,8 @@ def test_header_symbols_all_exported(pmpkg, lib):
     for n in names:
         assert hasattr(lib, n), n
     # and the ctypes table covers the whole header
-    assert set(names) - {"pm_last_error"} == set(_lib.SIGNATURES)
+    assert set(names) - {"pm_last_error", "pm_stage_name"} == set(_lib.SIGNATURES)
+    assert lib.pm_stage_name(0) == b"mesh_init" and lib.pm_stage_name(99) == b""
 
 
 def test_null_arguments_rejected(lib):

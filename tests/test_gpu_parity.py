@@ -17,8 +17,10 @@ DEV = "cuda:0"
 
 
 def rel(a, b):
-    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
-    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+    a, b = np.asarray(a), np.asarray(b)
+    a = a.astype(np.complex128 if np.iscomplexobj(a) else np.float64)
+    b = b.astype(np.complex128 if np.iscomplexobj(b) else np.float64)
+    return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
 
 
 def T(a, dtype=torch.float64):
