@@ -57,30 +57,36 @@ template <typename T> int upload_tables(Plan& p) {
     using C = typename Cx<T>::t;
     const int n = p.ng;
     std::vector<C> tw(n);
-    std::vector<T> lap(n);
+    std::vector<T> g1d(n);
     const long double pi = 3.141592653589793238462643383279502884L;
     for (int k = 0; k < n; ++k) {
         const long double a = -2.0L * pi * (long double)k / (long double)n;
         tw[k] = cmake<C>((T)cosl(a), (T)sinl(a));
-        const long double s = sinl(pi * (long double)k / (long double)n);
-        lap[k] = (T)(2.0L * s * s);
+        if (p.green_kind == PM_GREEN_DISCRETE) {
+            const long double s = sinl(pi * (long double)k / (long double)n);
+            g1d[k] = (T)(4.0L * s * s);
+        } else {
+            const long double m = k <= n / 2 ? (long double)k : (long double)(k - n);
+            const long double w = 2.0L * pi * m / (long double)n;
+            g1d[k] = (T)(w * w);
+        }
     }
     PMB_CUDA_CHECK(cudaMalloc(&p.tw, n * sizeof(C)));
-    PMB_CUDA_CHECK(cudaMalloc(&p.lap1d, n * sizeof(T)));
+    PMB_CUDA_CHECK(cudaMalloc(&p.g1d, n * sizeof(T)));
     PMB_CUDA_CHECK(cudaMemcpy(p.tw, tw.data(), n * sizeof(C), cudaMemcpyHostToDevice));
-    PMB_CUDA_CHECK(cudaMemcpy(p.lap1d, lap.data(), n * sizeof(T), cudaMemcpyHostToDevice));
+    PMB_CUDA_CHECK(cudaMemcpy(p.g1d, g1d.data(), n * sizeof(T), cudaMemcpyHostToDevice));
     p.bytes += n * (sizeof(C) + sizeof(T));
     return PM_OK;
 }
 
 void release(Plan& p) {
     if (p.tw) cudaFree(p.tw);
-    if (p.lap1d) cudaFree(p.lap1d);
+    if (p.g1d) cudaFree(p.g1d);
     if (p.d_err) cudaFree(p.d_err);
     if (p.mesh) cudaFree(p.mesh);
     for (void*& f : p.force)
         if (f) cudaFree(f), f = nullptr;
-    p.tw = p.lap1d = p.mesh = nullptr;
+    p.tw = p.g1d = p.mesh = nullptr;
     p.d_err = nullptr;
     delete p.timers;
     p.timers = nullptr;

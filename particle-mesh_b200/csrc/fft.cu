@@ -17,63 +17,79 @@
 
 namespace pmb {
 
-template <typename T> constexpr int tk_cols() { return sizeof(T) == 4 ? 16 : 8; }
-
-// ---------------------------------------------------------------- z passes
-// Real rows of N (+2 padding) at row stride N+2 reals; as complex a row is
-// N/2+1 entries.  LPB rows per block, NTZ threads per row.
-template <int N> constexpr int z_threads_per_row() { return threads_per_line<N / 2>(); }
-template <int N> constexpr int z_rows_per_block() {
-    constexpr int t = z_threads_per_row<N>();
-    constexpr int l = 256 / t;
-    return l < 1 ? 1 : (l > 64 ? 64 : l);
+// Columns per block of the strided passes.  Each warp phase (128 B of
+// shared memory) covers whole rows; at N = 1024 (and FP64 N = 512) the tile
+// is narrowed so two blocks share an SM and one block's loads overlap the
+// other's arithmetic.
+template <typename T, int N> constexpr int tk_cols() {
+    return sizeof(T) == 4 ? (N >= 1024 ? 8 : 16) : (N >= 1024 ? 4 : 8);
 }
 
+// Shared-memory index padding.  z passes: one pad entry after every R1
+// entries, so the pass-1 writes j*R1 + k of consecutive j hit distinct
+// banks.  Strided passes: TK pad entries after every R1 rows, so the rows
+// j*R1 + k of the neighbouring j that share a warp phase differ in bank.
+template <int R1> __device__ __forceinline__ int zpad(int i) { return i + i / R1; }
+template <int R1, int TK> __device__ __forceinline__ int spad(int row, int tx) {
+    return row * TK + tx + TK * (row / R1);
+}
+// The same padded positions written as base + compile-time offset, for the
+// three access patterns of the two-pass schedule (L = R1 R2, R2 % R1 == 0):
+//   pass-1 input  j + r R2      pass-1 output  j R1 + k
+//   pass-2 input  j + r R1      pass-2 output  j + k R1       (j < R1)
+template <int R1, int R2> struct ZIdx {  // z passes, unit stride, pad 1 per R1
+    static __device__ __forceinline__ int in1(int j, int r) { return j + j / R1 + r * (R2 + R2 / R1); }
+    static __device__ __forceinline__ int out1(int j, int k) { return j * (R1 + 1) + k; }
+    static __device__ __forceinline__ int p2(int j, int r) { return j + r * (R1 + 1); }
+};
+template <int R1, int R2, int TK> struct SIdx {  // strided passes, row stride TK, pad TK per R1 rows
+    static __device__ __forceinline__ int in1(int j, int r, int tx) {
+        return (j + j / R1) * TK + tx + r * (R2 + R2 / R1) * TK;
+    }
+    static __device__ __forceinline__ int out1(int j, int k, int tx) { return j * (R1 + 1) * TK + tx + k * TK; }
+    static __device__ __forceinline__ int p2(int j, int r, int tx) { return j * TK + tx + r * (R1 + 1) * TK; }
+};
+
+// ---------------------------------------------------------------- z passes
+// Real rows of N (+2 padding) at a row stride of N+2 reals; as complex a row
+// is M+1 = N/2+1 entries.  NT threads per row, LPB rows per block.
+template <int N> constexpr int z_threads_per_row() { return threads_per_line<N / 2>(); }
+template <typename T, int N> constexpr int z_rows_per_block() {
+    constexpr int l = (sizeof(T) == 4 ? 256 : 128) / z_threads_per_row<N>();
+    return l < 1 ? 1 : (l > 64 ? 64 : l);
+}
+template <typename T, int N> constexpr int z_threads() { return z_threads_per_row<N>() * z_rows_per_block<T, N>(); }
+template <int N> constexpr int z_row_stride() { return (N / 2 + 1) + (N / 2 + 1) / Radix<N / 2>::R1 + 1; }
+
+// R2C along z: complex FFT of the M packed pairs (x[2n], x[2n+1]), then
+// X[k] = E[k] + W_N^k O[k], E = (Z[k] + conj Z[M-k]) / 2, O = -i (Z[k] - conj Z[M-k]) / 2.
 template <typename T, int N>
-__global__ void __launch_bounds__(z_threads_per_row<N>() * z_rows_per_block<N>())
+__global__ void __launch_bounds__(z_threads<T, N>(), 2)
 k_fft_z_r2c(T* __restrict__ mesh, long long nrows, const typename Cx<T>::t* __restrict__ tw) {
     using C = typename Cx<T>::t;
     constexpr int M = N / 2, R1 = Radix<M>::R1, R2 = Radix<M>::R2;
-    constexpr int NT = z_threads_per_row<N>(), LPB = z_rows_per_block<N>();
+    constexpr int NT = z_threads_per_row<N>(), LPB = z_rows_per_block<T, N>();
     extern __shared__ __align__(16) unsigned char smraw[];
-    C* S = reinterpret_cast<C*>(smraw) + (threadIdx.x / NT) * (M + 1);
+    C* S = reinterpret_cast<C*>(smraw) + (threadIdx.x / NT) * z_row_stride<N>();
     const int tj = threadIdx.x % NT;
     const long long row = (long long)blockIdx.x * LPB + threadIdx.x / NT;
     const bool active = row < nrows;
     C* crow = reinterpret_cast<C*>(mesh + (active ? row : 0) * (long long)(N + 2));
 
-    // pass 1 (Ns = 1): global -> registers -> shared
-    for (int j = tj; j < M / R1; j += NT) {
-        C v[R1];
-#pragma unroll
-        for (int r = 0; r < R1; ++r) v[r] = active ? crow[j + r * (M / R1)] : cmake<C>(0, 0);
-        dft<R1, -1>(v);
-#pragma unroll
-        for (int k = 0; k < R1; ++k) S[j * R1 + k] = v[brev<R1>(k)];
-    }
+    using I = ZIdx<R1, R2>;
+    auto sld = [&](int i) { return S[zpad<R1>(i)]; };
+    stockham_pass1<R1, R2, -1, false, C>(
+        tj, [&](int j, int r) { return active ? crow[j + r * R2] : cmake<C>(0, 0); },
+        [&](int j, int k, C v) { S[I::out1(j, k)] = v; });
     __syncthreads();
-    // pass 2 (Ns = R1): shared -> registers -> shared (natural order)
-    C v2[R2];
-    const int j2 = tj;
-    const bool has2 = j2 < M / R2;
-    if (has2) {
-#pragma unroll
-        for (int r = 0; r < R2; ++r) v2[r] = S[j2 + r * (M / R2)];
-#pragma unroll
-        for (int r = 1; r < R2; ++r) v2[r] = cmul(v2[r], twiddle<-1>(tw, 2 * r * j2));  // W_M^{r j}
-        dft<R2, -1>(v2);
-    }
+    stockham_pass2<R1, R2, -1, true, C>(
+        tj, [&](int j, int r) { return S[I::p2(j, r)]; }, [&](int j, int k, C v) { S[I::p2(j, k)] = v; },
+        [&](int e) { return twiddle<-1>(tw, 2 * e); });
     __syncthreads();
-    if (has2) {
-#pragma unroll
-        for (int k = 0; k < R2; ++k) S[j2 + k * R1] = v2[brev<R2>(k)];
-    }
-    __syncthreads();
-    // real post-processing: X[k] = E[k] + W_N^k O[k], k = 0..M
     if (active) {
         for (int k = tj; k <= M; k += NT) {
-            const C zk = S[k == M ? 0 : k];
-            const C zc = cconj(S[k == 0 ? 0 : M - k]);
+            const C zk = sld(k == M ? 0 : k);
+            const C zc = cconj(sld(k == 0 ? 0 : M - k));
             const C e = cscale(cadd(zk, zc), (T)0.5);
             const C d = csub(zk, zc);
             const C o = cmake<C>((T)0.5 * d.y, (T)-0.5 * d.x);  // -i d / 2
@@ -82,72 +98,67 @@ k_fft_z_r2c(T* __restrict__ mesh, long long nrows, const typename Cx<T>::t* __re
     }
 }
 
+// C2R along z: Z[k] = (X[k] + conj X[M-k]) + i (X[k] - conj X[M-k]) W_N^-k,
+// inverse complex FFT of M, unpacked to reals.  The imaginary parts of X[0]
+// and X[M] are ignored (FFTW c2r semantics); the row padding is zeroed.
 template <typename T, int N>
-__global__ void __launch_bounds__(z_threads_per_row<N>() * z_rows_per_block<N>())
+__global__ void __launch_bounds__(z_threads<T, N>(), 2)
 k_fft_z_c2r(T* __restrict__ mesh, long long nrows, const typename Cx<T>::t* __restrict__ tw) {
     using C = typename Cx<T>::t;
     constexpr int M = N / 2, R1 = Radix<M>::R1, R2 = Radix<M>::R2;
-    constexpr int NT = z_threads_per_row<N>(), LPB = z_rows_per_block<N>();
+    constexpr int NT = z_threads_per_row<N>(), LPB = z_rows_per_block<T, N>();
     extern __shared__ __align__(16) unsigned char smraw[];
-    C* S = reinterpret_cast<C*>(smraw) + (threadIdx.x / NT) * (M + 1);
+    C* S = reinterpret_cast<C*>(smraw) + (threadIdx.x / NT) * z_row_stride<N>();
     const int tj = threadIdx.x % NT;
     const long long row = (long long)blockIdx.x * LPB + threadIdx.x / NT;
     const bool active = row < nrows;
     C* crow = reinterpret_cast<C*>(mesh + (active ? row : 0) * (long long)(N + 2));
 
-    for (int k = tj; k <= M; k += NT) {
-        C x = active ? crow[k] : cmake<C>(0, 0);
-        if (k == 0 || k == M) x.y = 0;  // FFTW c2r ignores these imaginary parts
-        S[k] = x;
-    }
-    __syncthreads();
-    // pre-processing + pass 1: Z[k] = (a + b) + i (a - b) W_N^{-k}, a = X[k], b = conj(X[M-k])
-    C v[R1];
-    const int j1 = tj;
-    const bool has1 = j1 < M / R1;
-    if (has1) {
+    auto sld = [&](int i) { return S[zpad<R1>(i)]; };
+    auto sst = [&](int i, C v) { S[zpad<R1>(i)] = v; };
+    {
+        constexpr int IT = M / NT + 1;  // covers k = 0..M
+        C x[IT];
 #pragma unroll
-        for (int r = 0; r < R1; ++r) {
-            const int k = j1 + r * (M / R1);
-            const C a = S[k], b = cconj(S[M - k]);
-            const C s = cadd(a, b), d = cmul(csub(a, b), twiddle<+1>(tw, k));
-            v[r] = cmake<C>(s.x - d.y, s.y + d.x);
+        for (int it = 0; it < IT; ++it) {
+            const int k = tj + it * NT;
+            x[it] = (active && k <= M) ? crow[k] : cmake<C>(0, 0);
         }
-        dft<R1, +1>(v);
-    }
-    __syncthreads();
-    if (has1) {
 #pragma unroll
-        for (int k = 0; k < R1; ++k) S[j1 * R1 + k] = v[brev<R1>(k)];
-    }
-    __syncthreads();
-    for (int j = tj; j < M / R2; j += NT) {
-        C w[R2];
-#pragma unroll
-        for (int r = 0; r < R2; ++r) w[r] = S[j + r * (M / R2)];
-#pragma unroll
-        for (int r = 1; r < R2; ++r) w[r] = cmul(w[r], twiddle<+1>(tw, 2 * r * j));
-        dft<R2, +1>(w);
-        if (active) {
-#pragma unroll
-            for (int k = 0; k < R2; ++k) crow[j + k * R1] = w[brev<R2>(k)];
+        for (int it = 0; it < IT; ++it) {
+            const int k = tj + it * NT;
+            if (k == 0 || k == M) x[it].y = 0;
+            if (k <= M) sst(k, x[it]);
         }
     }
+    __syncthreads();
+    using I = ZIdx<R1, R2>;
+    auto pre = [&](int j, int r) {
+        const int k = j + r * R2;
+        const C a = S[I::in1(j, r)], b = cconj(sld(M - k));
+        const C s = cadd(a, b), d = cmul(csub(a, b), twiddle<+1>(tw, k));
+        return cmake<C>(s.x - d.y, s.y + d.x);
+    };
+    stockham_pass1<R1, R2, +1, true, C>(tj, pre, [&](int j, int k, C v) { S[I::out1(j, k)] = v; });
+    __syncthreads();
+    stockham_pass2<R1, R2, +1, false, C>(
+        tj, [&](int j, int r) { return S[I::p2(j, r)]; },
+        [&](int j, int k, C v) { if (active) crow[j + k * R1] = v; }, [&](int e) { return twiddle<+1>(tw, 2 * e); });
     if (active && tj == 0) crow[M] = cmake<C>(0, 0);  // padding
 }
 
 // ------------------------------------------------------ strided C2C passes
 // Lines of N complex at element stride `es`; block (bx, by) owns columns
 // [bx*TK, bx*TK+TK) of plane `by` (plane base = by * os).
-template <typename T, int N>
-constexpr int strided_threads() { return tk_cols<T>() * threads_per_line<N>(); }
+template <typename T, int N> constexpr int strided_threads() { return tk_cols<T, N>() * threads_per_line<N>(); }
+template <typename T, int N> constexpr int strided_smem_elems() { return (N + N / Radix<N>::R1) * tk_cols<T, N>(); }
 
 template <typename T, int N, int DIR>
-__global__ void __launch_bounds__(strided_threads<T, N>())
+__global__ void __launch_bounds__(strided_threads<T, N>(), 2)
 k_fft_strided(typename Cx<T>::t* __restrict__ data, long long es, long long os, int ncols,
               const typename Cx<T>::t* __restrict__ tw) {
     using C = typename Cx<T>::t;
-    constexpr int R1 = Radix<N>::R1, R2 = Radix<N>::R2, TK = tk_cols<T>(), NT = threads_per_line<N>();
+    constexpr int R1 = Radix<N>::R1, R2 = Radix<N>::R2, TK = tk_cols<T, N>();
     extern __shared__ __align__(16) unsigned char smraw[];
     C* S = reinterpret_cast<C*>(smraw);
     const int tx = threadIdx.x % TK, ty = threadIdx.x / TK;
@@ -155,62 +166,49 @@ k_fft_strided(typename Cx<T>::t* __restrict__ data, long long es, long long os, 
     const bool active = col < ncols;
     C* base = data + (long long)blockIdx.y * os + (active ? col : 0);
 
-    for (int j = ty; j < N / R1; j += NT) {
-        C v[R1];
-#pragma unroll
-        for (int r = 0; r < R1; ++r) v[r] = active ? base[(long long)(j + r * (N / R1)) * es] : cmake<C>(0, 0);
-        dft<R1, DIR>(v);
-#pragma unroll
-        for (int k = 0; k < R1; ++k) S[(j * R1 + k) * TK + tx] = v[brev<R1>(k)];
-    }
+    using I = SIdx<R1, R2, TK>;
+    const long long es1 = es * R2, es2 = es * R1;
+    stockham_pass1<R1, R2, DIR, false, C>(
+        ty, [&](int j, int r) { return active ? base[j * es + r * es1] : cmake<C>(0, 0); },
+        [&](int j, int k, C v) { S[I::out1(j, k, tx)] = v; });
     __syncthreads();
-    for (int j = ty; j < N / R2; j += NT) {
-        C v[R2];
-#pragma unroll
-        for (int r = 0; r < R2; ++r) v[r] = S[(j + r * (N / R2)) * TK + tx];
-#pragma unroll
-        for (int r = 1; r < R2; ++r) v[r] = cmul(v[r], twiddle<DIR>(tw, r * j));
-        dft<R2, DIR>(v);
-        if (active) {
-#pragma unroll
-            for (int k = 0; k < R2; ++k) base[(long long)(j + k * R1) * es] = v[brev<R2>(k)];
-        }
-    }
+    stockham_pass2<R1, R2, DIR, false, C>(
+        ty, [&](int j, int r) { return S[I::p2(j, r, tx)]; },
+        [&](int j, int k, C v) { if (active) base[j * es + k * es2] = v; },
+        [&](int e) { return twiddle<DIR>(tw, e); });
 }
 
-// Green's function G(kx, ky, kz) / N^3 times c (cg = c / N^3).
-//   discrete (reference, src/fft/fftw/fft.cpp:55): -cg / (2 (3 - cos - cos - cos));
-//     FP64 evaluates exactly that expression from the rounded cosines; FP32
-//     uses 3 - sum cos = sum 2 sin^2(pi k/N) to avoid cancellation.
-//   spectral: -cg / |k|^2, k = 2 pi m / N with m the signed frequency.
+// Green's function times c / N^3 (cg = c / N^3) at (kx, ky, kz).
+//   FP64 discrete: -cg / (2 (3 - cos - cos - cos)), the reference's own
+//     expression (src/fft/fftw/fft.cpp:55) on the rounded cosines.
+//   otherwise: -cg / (g1d[kx] + g1d[ky] + g1d[kz]) with the plan's 1D table
+//     g1d = 4 sin^2(pi k/N) (discrete: 2 (3 - sum cos) without cancellation)
+//     or (2 pi m/N)^2, m the signed frequency (spectral).
 template <typename T>
-__device__ __forceinline__ T green_value(int kx, int ky, int kz, int n, int kind, double cg,
+__device__ __forceinline__ T green_value(int kx, int ky, int kz, int kind, double cg,
                                          const typename Cx<T>::t* __restrict__ tw,
-                                         const T* __restrict__ lap1d) {
+                                         const T* __restrict__ g1d) {
     if ((kx | ky | kz) == 0) return (T)0;
-    if (kind == PM_GREEN_DISCRETE) {
-        if constexpr (sizeof(T) == 8) {
+    if constexpr (sizeof(T) == 8) {
+        if (kind == PM_GREEN_DISCRETE) {
             const double s = ((3.0 - (double)__ldg(&tw[kx].x)) - (double)__ldg(&tw[ky].x)) - (double)__ldg(&tw[kz].x);
             return (T)(-cg / (2.0 * s));
-        } else {
-            const T s = __ldg(lap1d + kx) + __ldg(lap1d + ky) + __ldg(lap1d + kz);
-            return (T)(-cg) / ((T)2 * s);
         }
+        return (T)(-cg / ((double)__ldg(g1d + kx) + (double)__ldg(g1d + ky) + (double)__ldg(g1d + kz)));
+    } else {
+        const float s = __ldg(g1d + kx) + __ldg(g1d + ky) + __ldg(g1d + kz);
+        return (float)(-cg) * __frcp_rn(s);
     }
-    const int mx = kx <= n / 2 ? kx : kx - n, my = ky <= n / 2 ? ky : ky - n;
-    const double w = 6.283185307179586476925286766559 / n;
-    const double k2 = w * w * (double)(mx * mx + my * my + kz * kz);
-    return (T)(-cg / k2);
 }
 
-// Fused x pass of the Poisson solve: forward FFT along x, multiply by G, and
+// Fused x pass of the Poisson solve: forward FFT along x, multiply by G,
 // inverse FFT along x, for TK kz columns of one ky plane.
 template <typename T, int N>
-__global__ void __launch_bounds__(strided_threads<T, N>())
+__global__ void __launch_bounds__(strided_threads<T, N>(), 2)
 k_fft_x_green(typename Cx<T>::t* __restrict__ data, long long es, long long os, int ncols,
-              const typename Cx<T>::t* __restrict__ tw, const T* __restrict__ lap1d, double cg, int kind) {
+              const typename Cx<T>::t* __restrict__ tw, const T* __restrict__ g1d, double cg, int kind) {
     using C = typename Cx<T>::t;
-    constexpr int R1 = Radix<N>::R1, R2 = Radix<N>::R2, TK = tk_cols<T>(), NT = threads_per_line<N>();
+    constexpr int R1 = Radix<N>::R1, R2 = Radix<N>::R2, TK = tk_cols<T, N>();
     extern __shared__ __align__(16) unsigned char smraw[];
     C* S = reinterpret_cast<C*>(smraw);
     const int tx = threadIdx.x % TK, ty = threadIdx.x / TK;
@@ -219,75 +217,32 @@ k_fft_x_green(typename Cx<T>::t* __restrict__ data, long long es, long long os, 
     const int ky = blockIdx.y;
     C* base = data + (long long)ky * os + (active ? col : 0);
 
-    // forward pass 1: global -> shared
-    for (int j = ty; j < N / R1; j += NT) {
-        C v[R1];
-#pragma unroll
-        for (int r = 0; r < R1; ++r) v[r] = active ? base[(long long)(j + r * (N / R1)) * es] : cmake<C>(0, 0);
-        dft<R1, -1>(v);
-#pragma unroll
-        for (int k = 0; k < R1; ++k) S[(j * R1 + k) * TK + tx] = v[brev<R1>(k)];
-    }
+    using I = SIdx<R1, R2, TK>;
+    const long long es1 = es * R2, es2 = es * R1;
+    auto p2ld = [&](int j, int r) { return S[I::p2(j, r, tx)]; };
+    stockham_pass1<R1, R2, -1, false, C>(
+        ty, [&](int j, int r) { return active ? base[j * es + r * es1] : cmake<C>(0, 0); },
+        [&](int j, int k, C v) { S[I::out1(j, k, tx)] = v; });
     __syncthreads();
-    // forward pass 2 + Green, back into shared (natural kx order)
-    {
-        C v[R2];
-        const int j = ty;
-        const bool has = j < N / R2;
-        if (has) {
-#pragma unroll
-            for (int r = 0; r < R2; ++r) v[r] = S[(j + r * (N / R2)) * TK + tx];
-#pragma unroll
-            for (int r = 1; r < R2; ++r) v[r] = cmul(v[r], twiddle<-1>(tw, r * j));
-            dft<R2, -1>(v);
-        }
-        __syncthreads();
-        if (has) {
-#pragma unroll
-            for (int k = 0; k < R2; ++k) {
-                const int kx = j + k * R1;
-                const T g = active ? green_value<T>(kx, ky, col, N, kind, cg, tw, lap1d) : (T)0;
-                S[kx * TK + tx] = cscale(v[brev<R2>(k)], g);
-            }
-        }
-    }
+    stockham_pass2<R1, R2, -1, true, C>(
+        ty, p2ld,
+        [&](int j, int k, C v) {
+            S[I::p2(j, k, tx)] = cscale(v, active ? green_value<T>(j + k * R1, ky, col, kind, cg, tw, g1d) : (T)0);
+        },
+        [&](int e) { return twiddle<-1>(tw, e); });
     __syncthreads();
-    // inverse pass 1: shared -> shared
-    {
-        C v[R1];
-        const int j = ty;
-        const bool has = j < N / R1;
-        if (has) {
-#pragma unroll
-            for (int r = 0; r < R1; ++r) v[r] = S[(j + r * (N / R1)) * TK + tx];
-            dft<R1, +1>(v);
-        }
-        __syncthreads();
-        if (has) {
-#pragma unroll
-            for (int k = 0; k < R1; ++k) S[(j * R1 + k) * TK + tx] = v[brev<R1>(k)];
-        }
-    }
+    stockham_pass1<R1, R2, +1, true, C>(
+        ty, [&](int j, int r) { return S[I::in1(j, r, tx)]; }, [&](int j, int k, C v) { S[I::out1(j, k, tx)] = v; });
     __syncthreads();
-    // inverse pass 2: shared -> global
-    for (int j = ty; j < N / R2; j += NT) {
-        C v[R2];
-#pragma unroll
-        for (int r = 0; r < R2; ++r) v[r] = S[(j + r * (N / R2)) * TK + tx];
-#pragma unroll
-        for (int r = 1; r < R2; ++r) v[r] = cmul(v[r], twiddle<+1>(tw, r * j));
-        dft<R2, +1>(v);
-        if (active) {
-#pragma unroll
-            for (int k = 0; k < R2; ++k) base[(long long)(j + k * R1) * es] = v[brev<R2>(k)];
-        }
-    }
+    stockham_pass2<R1, R2, +1, false, C>(
+        ty, p2ld, [&](int j, int k, C v) { if (active) base[j * es + k * es2] = v; },
+        [&](int e) { return twiddle<+1>(tw, e); });
 }
 
 // Separate Green multiply over the spectrum [kx][ky][kz] (the plain path).
 template <typename T>
 __global__ void k_green(typename Cx<T>::t* __restrict__ spec, int n, const typename Cx<T>::t* __restrict__ tw,
-                        const T* __restrict__ lap1d, double cg, int kind) {
+                        const T* __restrict__ g1d, double cg, int kind) {
     using C = typename Cx<T>::t;
     const int h = n / 2 + 1;
     const long long total = (long long)n * n * h;
@@ -296,9 +251,7 @@ __global__ void k_green(typename Cx<T>::t* __restrict__ spec, int n, const typen
         const int kz = (int)(i % h);
         const long long r = i / h;
         const int ky = (int)(r % n), kx = (int)(r / n);
-        const T g = green_value<T>(kx, ky, kz, n, kind, cg, tw, lap1d);
-        C v = spec[i];
-        spec[i] = cscale(v, g);
+        spec[i] = cscale(spec[i], green_value<T>(kx, ky, kz, kind, cg, tw, g1d));
     }
 }
 
@@ -306,8 +259,8 @@ __global__ void k_green(typename Cx<T>::t* __restrict__ spec, int n, const typen
 template <typename T, int N> struct Launch {
     using C = typename Cx<T>::t;
     static constexpr int H = N / 2 + 1;
-    static size_t smem_z() { return (size_t)z_rows_per_block<N>() * (N / 2 + 1) * sizeof(C); }
-    static size_t smem_s() { return (size_t)N * tk_cols<T>() * sizeof(C); }
+    static size_t smem_z() { return (size_t)z_rows_per_block<T, N>() * z_row_stride<N>() * sizeof(C); }
+    static size_t smem_s() { return (size_t)strided_smem_elems<T, N>() * sizeof(C); }
     static int prepare() {
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_z_r2c<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_z()));
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_z_c2r<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_z()));
@@ -318,8 +271,8 @@ template <typename T, int N> struct Launch {
     }
     static void z(const Plan& p, T* mesh, bool forward) {
         const long long rows = (long long)N * N;
-        const unsigned grid = (unsigned)((rows + z_rows_per_block<N>() - 1) / z_rows_per_block<N>());
-        const int thr = z_threads_per_row<N>() * z_rows_per_block<N>();
+        const unsigned grid = (unsigned)((rows + z_rows_per_block<T, N>() - 1) / z_rows_per_block<T, N>());
+        const int thr = z_threads_per_row<N>() * z_rows_per_block<T, N>();
         const C* tw = static_cast<const C*>(p.tw);
         Timed t(p, forward ? ST_FFT_Z_R2C : ST_FFT_Z_C2R);
         if (forward)
@@ -331,7 +284,7 @@ template <typename T, int N> struct Launch {
     static void strided(const Plan& p, T* mesh, int axis, int dir) {
         C* d = reinterpret_cast<C*>(mesh);
         const long long es = axis == 1 ? H : (long long)N * H, os = axis == 1 ? (long long)N * H : H;
-        dim3 grid((H + tk_cols<T>() - 1) / tk_cols<T>(), N);
+        dim3 grid((H + tk_cols<T, N>() - 1) / tk_cols<T, N>(), N);
         const C* tw = static_cast<const C*>(p.tw);
         Timed t(p, axis == 1 ? (dir < 0 ? ST_FFT_Y_FWD : ST_FFT_Y_INV) : (dir < 0 ? ST_FFT_X_FWD : ST_FFT_X_INV));
         if (dir < 0)
@@ -341,10 +294,10 @@ template <typename T, int N> struct Launch {
     }
     static void xgreen(const Plan& p, T* mesh, double cg) {
         C* d = reinterpret_cast<C*>(mesh);
-        dim3 grid((H + tk_cols<T>() - 1) / tk_cols<T>(), N);
+        dim3 grid((H + tk_cols<T, N>() - 1) / tk_cols<T, N>(), N);
         Timed t(p, ST_FFT_X_GREEN);
         k_fft_x_green<T, N><<<grid, strided_threads<T, N>(), smem_s(), p.stream>>>(
-            d, (long long)N * H, H, H, static_cast<const C*>(p.tw), static_cast<const T*>(p.lap1d), cg, p.green_kind);
+            d, (long long)N * H, H, H, static_cast<const C*>(p.tw), static_cast<const T*>(p.g1d), cg, p.green_kind);
     }
 };
 
@@ -405,7 +358,7 @@ template <typename T> int green_apply(const Plan& p, T* mesh, double c_poisson) 
     const long long total = (long long)p.ng * p.ng * (p.ng / 2 + 1);
     Timed t(p, ST_GREEN);
     k_green<T><<<grid_for(p, total, 256), 256, 0, p.stream>>>(
-        reinterpret_cast<C*>(mesh), p.ng, static_cast<const C*>(p.tw), static_cast<const T*>(p.lap1d),
+        reinterpret_cast<C*>(mesh), p.ng, static_cast<const C*>(p.tw), static_cast<const T*>(p.g1d),
         green_scale(p, c_poisson), p.green_kind);
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;

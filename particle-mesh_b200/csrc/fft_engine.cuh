@@ -44,6 +44,10 @@ __device__ __forceinline__ C rot64(C d, int k) {
     if (k == 24)
         return DIR < 0 ? cmake<C>((d.y - d.x) * h, -(d.x + d.y) * h) : cmake<C>(-(d.x + d.y) * h, (d.x - d.y) * h);
     const T c = (T)cos64(k), s = (T)(DIR * sin64(k));
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+    if constexpr (sizeof(T) == 4)  // d.x (c, s) + d.y (-s, c) on the f32x2 pipe
+        return __ffma2_rn(make_float2(d.y, d.y), make_float2(-s, c), __fmul2_rn(make_float2(d.x, d.x), make_float2(c, s)));
+#endif
     return cmake<C>(d.x * c - d.y * s, d.x * s + d.y * c);
 }
 
@@ -81,7 +85,7 @@ __device__ __forceinline__ C twiddle(const C* __restrict__ tw, int e) {
     return DIR < 0 ? w : cconj(w);
 }
 
-// Two-pass radix choice for a line of length L = R1 * R2.
+// Two-pass radix choice for a line of length L = R1 * R2, R1 <= R2.
 template <int L> struct Radix;
 template <> struct Radix<4> { static constexpr int R1 = 2, R2 = 2; };
 template <> struct Radix<8> { static constexpr int R1 = 2, R2 = 4; };
@@ -93,8 +97,50 @@ template <> struct Radix<256> { static constexpr int R1 = 16, R2 = 16; };
 template <> struct Radix<512> { static constexpr int R1 = 16, R2 = 32; };
 template <> struct Radix<1024> { static constexpr int R1 = 32, R2 = 32; };
 
-template <int L> constexpr int threads_per_line() {
-    return L / (Radix<L>::R1 < Radix<L>::R2 ? Radix<L>::R1 : Radix<L>::R2);
+// Threads per line: one radix-R2 butterfly each in pass 2; pass 1 has
+// R2 / R1 radix-R1 butterflies per thread.
+template <int L> constexpr int threads_per_line() { return L / Radix<L>::R2; }
+
+// Stockham pass 1 (Ns = 1, radix R1) of a line of L = R1 R2: thread tj owns
+// the butterflies j = tj + it R1 (it < R2/R1).  ld(j, r) returns element
+// j + r R2; st(j, k, v) stores output k of butterfly j, element j R1 + k.
+// The structured indices let each kernel form its (padded) addresses as a
+// per-j base plus compile-time offsets.  With SYNC the block synchronises
+// between all loads and all stores (in-place passes).
+template <int R1, int R2, int DIR, bool SYNC, typename C, typename LD, typename ST>
+__device__ __forceinline__ void stockham_pass1(int tj, const LD& ld, const ST& st) {
+    constexpr int IT = R2 / R1;
+    C v[IT][R1];
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+        const int j = tj + it * R1;
+#pragma unroll
+        for (int r = 0; r < R1; ++r) v[it][r] = ld(j, r);
+        dft<R1, DIR>(v[it]);
+    }
+    if (SYNC) __syncthreads();
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+        const int j = tj + it * R1;
+#pragma unroll
+        for (int k = 0; k < R1; ++k) st(j, k, v[it][brev<R1>(k)]);
+    }
+}
+
+// Stockham pass 2 (Ns = R1, radix R2): thread j < R1 reads ld(j, r) =
+// element j + r R1, multiplies by W_L^{r j} (twf(r j)) and stores output k
+// with st(j, k, v) to element j + k R1.
+template <int R1, int R2, int DIR, bool SYNC, typename C, typename LD, typename ST, typename TW>
+__device__ __forceinline__ void stockham_pass2(int j, const LD& ld, const ST& st, const TW& twf) {
+    C v[R2];
+#pragma unroll
+    for (int r = 0; r < R2; ++r) v[r] = ld(j, r);
+#pragma unroll
+    for (int r = 1; r < R2; ++r) v[r] = cmul(v[r], twf(r * j));
+    dft<R2, DIR>(v);
+    if (SYNC) __syncthreads();
+#pragma unroll
+    for (int k = 0; k < R2; ++k) st(j, k, v[brev<R2>(k)]);
 }
 
 }  // namespace pmb

@@ -31,6 +31,22 @@ template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
 template <typename C> __device__ __forceinline__ C cconj(C a) { return cmake<C>(a.x, -a.y); }
 template <typename C> __device__ __forceinline__ C cscale(C a, decltype(C::x) s) { return cmake<C>(a.x * s, a.y * s); }
 
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+// FP32 complex arithmetic on the paired f32x2 pipe of sm_100 (one
+// instruction per complex add / sub, two per multiply-by-constant).
+template <> __device__ __forceinline__ float2 cadd<float2>(float2 a, float2 b) { return __fadd2_rn(a, b); }
+template <> __device__ __forceinline__ float2 csub<float2>(float2 a, float2 b) {
+    return __ffma2_rn(b, make_float2(-1.f, -1.f), a);
+}
+template <> __device__ __forceinline__ float2 cmul<float2>(float2 a, float2 b) {
+    const float2 t = __fmul2_rn(make_float2(a.x, a.x), b);
+    return __ffma2_rn(make_float2(-a.y, a.y), make_float2(b.y, b.x), t);
+}
+template <> __device__ __forceinline__ float2 cscale<float2>(float2 a, float s) {
+    return __fmul2_rn(a, make_float2(s, s));
+}
+#endif
+
 // ------------------------------------------------------------------- errors
 enum : int { ERRBIT_RANGE = 1 };
 
@@ -78,10 +94,11 @@ struct Plan {
     int device = 0;
     int num_sms = 148;
     // Tables of length ng in the plan's precision:
-    //   tw[k]    = exp(-2 pi i k / ng)          (twiddles, Green cosines)
-    //   lap1d[k] = 2 sin^2(pi k / ng)           (7-point Laplacian, 1D part)
+    //   tw[k]  = exp(-2 pi i k / ng)              (twiddles, Green cosines)
+    //   g1d[k] = 1D part of -(Laplacian symbol): 4 sin^2(pi k / ng) for the
+    //            7-point Laplacian, (2 pi m / ng)^2 (m signed) for spectral
     void* tw = nullptr;
-    void* lap1d = nullptr;
+    void* g1d = nullptr;
     int* d_err = nullptr;           // device error bits
     void* mesh = nullptr;           // workspace mesh [ng][ng][ng+2]
     void* force[3] = {nullptr, nullptr, nullptr};  // FP64 force arrays
