@@ -105,6 +105,28 @@ def bus_id(torch, dev):
         return None
 
 
+# ------------------------------------------------------- ranks and timing
+def reduce_max(v: float, world: int, device=None) -> float:
+    """Max of a per-rank time over all ranks (every rank takes this step)."""
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def throughput(world: int, particles_per_rank: int, steps: int, t_ms: float) -> float:
+    """Whole-job particle-updates/s: every rank advances its own box."""
+    return world * particles_per_rank * steps / (t_ms / 1e3)
+
+
+def rank_seed(rank: int) -> int:
+    """Each rank's box has its own initial conditions."""
+    return SEED + rank
+
+
 # ------------------------------------------------------------- byte model
 def stage_bytes(stage: str, ng: int, np_: int, esz: int) -> float:
     """Algorithmic bytes of one launch of a stage (the minimum it must move).
@@ -253,11 +275,7 @@ def ours(args):
             dist.barrier()
 
     def max_over_ranks(v: float) -> float:
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(v, world, dev)
 
     ng, nrow = args.ng, args.nrow
     np_ = nrow ** 3
@@ -265,7 +283,7 @@ def ours(args):
     cp, ck = pm.unit_box_coefficients(DT)
     stream = torch.cuda.current_stream(dev)
 
-    pos, vel = pm.zeldovich_ic(ng, nrow, N_S, RMS, SEED + rank, device=dev)
+    pos, vel = pm.zeldovich_ic(ng, nrow, N_S, RMS, rank_seed(rank), device=dev)
     p32 = pm.Plan(ng, "fp32", "spectral", 4, stream=stream, device=dev)
     cell, off = p32.split(*pos)
     v32 = [a.float() for a in vel]
@@ -291,7 +309,7 @@ def ours(args):
     t_ms = max_over_ranks(e0.elapsed_time(e1))
     stages = p32.read_timing(reset=True)
     p32.check()
-    value = world * np_ * args.steps / (t_ms / 1e3)
+    value = throughput(world, np_, args.steps, t_ms)
     launches = sum(n for _, n in stages.values())
 
     peak, peak_kind = measured_peaks()
@@ -330,6 +348,8 @@ def ours(args):
         del zero, c0, o0, f32
         for _ in range(args.warmup):
             p64.step(x, y, z, *pv, mass, cp, ck, DT)
+        p64.read_timing(reset=True)
+        p64.set_timing(True)
         barrier()
         torch.cuda.synchronize()
         e0.record(stream)
@@ -339,8 +359,13 @@ def ours(args):
         torch.cuda.synchronize()
         barrier()
         t64 = max_over_ranks(e0.elapsed_time(e1))
-        fp64 = {"value": world * np_ * args.steps / (t64 / 1e3), "unit": UNIT, "ms_per_step": t64 / args.steps,
-                "dtype": "f64"}
+        st64 = p64.read_timing(reset=True)
+        fp64 = {"value": throughput(world, np_, args.steps, t64), "unit": UNIT, "ms_per_step": t64 / args.steps,
+                "dtype": "f64", "path": "plain FP64: separate deposit, 3+3 FFT passes, Green, gradient to 3 force "
+                                        "meshes, interpolate + kick, drift",
+                "stages": {s: {"ms_per_step": ms / args.steps, "launches": n,
+                               "gbs": stage_bytes(s, ng, np_, 8) * n / (ms / 1e3) / 1e9 if ms > 0 else None}
+                           for s, (ms, n) in st64.items()}}
         p64.close()
         del p64, x, y, z, pv
         torch.cuda.empty_cache()
@@ -372,7 +397,7 @@ def ours(args):
         torch.cuda.synchronize()
         barrier()
         te = max_over_ranks(e0.elapsed_time(e1))
-        e2e = {"value": world * np_ * args.steps / (te / 1e3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
+        e2e = {"value": throughput(world, np_, args.steps, te), "unit": UNIT, "h2d_bytes_per_step": nbytes,
                "d2h_bytes_per_step": nbytes, "ms_per_step": te / args.steps,
                "path": "pm_step_f32 through the C ABI; particle state copied from pinned host memory and back "
                        "every step"}

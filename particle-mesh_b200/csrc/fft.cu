@@ -239,19 +239,17 @@ k_fft_x_green(typename Cx<T>::t* __restrict__ data, long long es, long long os, 
         [&](int e) { return twiddle<+1>(tw, e); });
 }
 
-// Separate Green multiply over the spectrum [kx][ky][kz] (the plain path).
+// Separate Green multiply over the spectrum [kx][ky][kz] (the plain path):
+// one block iteration per (kx, ky) row, threads along kz.
 template <typename T>
 __global__ void k_green(typename Cx<T>::t* __restrict__ spec, int n, const typename Cx<T>::t* __restrict__ tw,
                         const T* __restrict__ g1d, double cg, int kind) {
-    using C = typename Cx<T>::t;
-    const int h = n / 2 + 1;
-    const long long total = (long long)n * n * h;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-         i += (long long)gridDim.x * blockDim.x) {
-        const int kz = (int)(i % h);
-        const long long r = i / h;
-        const int ky = (int)(r % n), kx = (int)(r / n);
-        spec[i] = cscale(spec[i], green_value<T>(kx, ky, kz, kind, cg, tw, g1d));
+    const int h = n / 2 + 1, msk = n - 1, sh = __ffs(n) - 1;
+    for (long long row = blockIdx.x; row < (long long)n * n; row += gridDim.x) {
+        const int kx = (int)(row >> sh), ky = (int)(row & msk);
+        typename Cx<T>::t* r = spec + row * h;
+        for (int kz = threadIdx.x; kz < h; kz += blockDim.x)
+            r[kz] = cscale(r[kz], green_value<T>(kx, ky, kz, kind, cg, tw, g1d));
     }
 }
 
@@ -355,9 +353,8 @@ static double green_scale(const Plan& p, double c) {
 
 template <typename T> int green_apply(const Plan& p, T* mesh, double c_poisson) {
     using C = typename Cx<T>::t;
-    const long long total = (long long)p.ng * p.ng * (p.ng / 2 + 1);
     Timed t(p, ST_GREEN);
-    k_green<T><<<grid_for(p, total, 256), 256, 0, p.stream>>>(
+    k_green<T><<<grid_for(p, (long long)p.ng * p.ng, 1), 256, 0, p.stream>>>(
         reinterpret_cast<C*>(mesh), p.ng, static_cast<const C*>(p.tw), static_cast<const T*>(p.g1d),
         green_scale(p, c_poisson), p.green_kind);
     PMB_CUDA_CHECK(cudaGetLastError());

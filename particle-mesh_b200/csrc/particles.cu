@@ -93,26 +93,33 @@ __global__ void k_deposit_f64(const double* __restrict__ x, const double* __rest
     }
 }
 
-// f = -grad phi by centred differences, one thread per cell.
+// f = -grad phi by centred differences.  One block iteration per mesh row
+// (i, j), threads along k, so the ten neighbour rows are addressed once.
 //   order 2: (phi[i-1] - phi[i+1]) / 2          (src/utils/utils.cpp:130-135)
 //   order 4: (8 (phi[i-1] - phi[i+1]) - (phi[i-2] - phi[i+2])) / 12
 template <int ORDER>
 __global__ void k_gradient_f64(const double* __restrict__ phi, double* __restrict__ fx,
                                double* __restrict__ fy, double* __restrict__ fz, int n) {
-    const long long total = (long long)n * n * n, pz = n + 2;
-    const int msk = n - 1;
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < total;
-         c += (long long)gridDim.x * blockDim.x) {
-        const int k = (int)(c & msk), j = (int)((c / n) & msk), i = (int)(c / ((long long)n * n));
-        auto P = [&](int a, int b, int d) { return __ldg(phi + ((long long)(a & msk) * n + (b & msk)) * pz + (d & msk)); };
-        if (ORDER == 4) {
-            fx[c] = (8.0 * (P(i - 1, j, k) - P(i + 1, j, k)) - (P(i - 2, j, k) - P(i + 2, j, k))) / 12.0;
-            fy[c] = (8.0 * (P(i, j - 1, k) - P(i, j + 1, k)) - (P(i, j - 2, k) - P(i, j + 2, k))) / 12.0;
-            fz[c] = (8.0 * (P(i, j, k - 1) - P(i, j, k + 1)) - (P(i, j, k - 2) - P(i, j, k + 2))) / 12.0;
-        } else {
-            fx[c] = (P(i - 1, j, k) - P(i + 1, j, k)) * 0.5;
-            fy[c] = (P(i, j - 1, k) - P(i, j + 1, k)) * 0.5;
-            fz[c] = (P(i, j, k - 1) - P(i, j, k + 1)) * 0.5;
+    const int msk = n - 1, sh = __ffs(n) - 1;
+    const long long pz = n + 2;
+    for (long long row = blockIdx.x; row < (long long)n * n; row += gridDim.x) {
+        const int i = (int)(row >> sh), j = (int)(row & msk);
+        auto R = [&](int a, int b) { return phi + ((long long)(a & msk) * n + (b & msk)) * pz; };
+        const double *c0 = R(i, j), *xm1 = R(i - 1, j), *xp1 = R(i + 1, j), *ym1 = R(i, j - 1), *yp1 = R(i, j + 1);
+        const double *xm2 = R(i - 2, j), *xp2 = R(i + 2, j), *ym2 = R(i, j - 2), *yp2 = R(i, j + 2);
+        const long long o = row * n;
+        for (int k = threadIdx.x; k < n; k += blockDim.x) {
+            const int km1 = (k - 1) & msk, kp1 = (k + 1) & msk;
+            if (ORDER == 4) {
+                const int km2 = (k - 2) & msk, kp2 = (k + 2) & msk;
+                fx[o + k] = (8.0 * (__ldg(xm1 + k) - __ldg(xp1 + k)) - (__ldg(xm2 + k) - __ldg(xp2 + k))) / 12.0;
+                fy[o + k] = (8.0 * (__ldg(ym1 + k) - __ldg(yp1 + k)) - (__ldg(ym2 + k) - __ldg(yp2 + k))) / 12.0;
+                fz[o + k] = (8.0 * (__ldg(c0 + km1) - __ldg(c0 + kp1)) - (__ldg(c0 + km2) - __ldg(c0 + kp2))) / 12.0;
+            } else {
+                fx[o + k] = (__ldg(xm1 + k) - __ldg(xp1 + k)) * 0.5;
+                fy[o + k] = (__ldg(ym1 + k) - __ldg(yp1 + k)) * 0.5;
+                fz[o + k] = (__ldg(c0 + km1) - __ldg(c0 + kp1)) * 0.5;
+            }
         }
     }
 }
@@ -254,55 +261,73 @@ __global__ void k_deposit_f32(const uint32_t* __restrict__ cell, const float* __
 
 // Force at one particle with the gradient fused into the gather: the
 // trilinear weights of cells (i+a, j+b, k+c), a,b,c in {0,1}, applied to the
-// centred difference of phi at those cells (2- or 4-point).
+// centred difference of phi at those cells (2- or 4-point).  The stencils
+// of the three components share their cells: each of the 32 (2-point) or 56
+// (4-point) distinct values is loaded once, from 12 or 20 mesh rows whose
+// offsets fit in 32 bits (ng <= 1024).
 template <int ORDER>
 __device__ __forceinline__ void force_at(const float* __restrict__ phi, int n, int i, int j, int k,
                                          float tx, float ty, float tz, float& gx, float& gy,
                                          float& gz) {
-    const int msk = n - 1;
-    const long long pz = n + 2;
-    auto P = [&](int a, int b, int c) {
-        return __ldg(phi + ((long long)(a & msk) * n + (b & msk)) * pz + (c & msk));
+    constexpr int LO = ORDER == 4 ? -2 : -1, W = ORDER == 4 ? 6 : 4;  // stencil offsets LO..LO+W-1
+    const unsigned msk = (unsigned)n - 1u, pz = (unsigned)n + 2u, plane = (unsigned)n * pz;
+    unsigned xo[W], yo[W], kc[W];
+#pragma unroll
+    for (int d = 0; d < W; ++d) {
+        xo[d] = ((unsigned)(i + LO + d) & msk) * plane;
+        yo[d] = ((unsigned)(j + LO + d) & msk) * pz;
+        kc[d] = (unsigned)(k + LO + d) & msk;
+    }
+    constexpr int C0 = -LO;  // stencil slot of offset 0
+    // core rows (i+a, j+b): the whole z stencil
+    float Z[2][2][W];
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b)
+#pragma unroll
+            for (int c = 0; c < W; ++c) Z[a][b][c] = __ldg(phi + xo[C0 + a] + yo[C0 + b] + kc[c]);
+    // x stencil rows (i+d, j+b) and y stencil rows (i+a, j+d), columns k, k+1
+    float X[W][2][2], Y[2][W][2];
+#pragma unroll
+    for (int d = 0; d < W; ++d)
+#pragma unroll
+        for (int b = 0; b < 2; ++b)
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                if (d == C0 || d == C0 + 1) {
+                    X[d][b][c] = Z[d - C0][b][C0 + c];
+                    Y[b][d][c] = Z[b][d - C0][C0 + c];
+                } else {
+                    X[d][b][c] = __ldg(phi + xo[d] + yo[C0 + b] + kc[C0 + c]);
+                    Y[b][d][c] = __ldg(phi + xo[C0 + b] + yo[d] + kc[C0 + c]);
+                }
+            }
+    const float w0[2] = {1.0f - tx, tx}, w1[2] = {1.0f - ty, ty}, w2[2] = {1.0f - tz, tz};
+    // centred difference at slot s (offset s - C0) of a stencil line v
+    auto D = [](const float* v, int s) {
+        return ORDER == 4 ? (8.0f * (v[s - 1] - v[s + 1]) - (v[s - 2] - v[s + 2])) * (1.0f / 12.0f)
+                          : (v[s - 1] - v[s + 1]) * 0.5f;
     };
-    const float wx[2] = {1.0f - tx, tx}, wy[2] = {1.0f - ty, ty}, wz[2] = {1.0f - tz, tz};
-    auto D = [&](float m2, float m1, float p1, float p2) {
-        return ORDER == 4 ? (8.0f * (m1 - p1) - (m2 - p2)) * (1.0f / 12.0f) : (m1 - p1) * 0.5f;
-    };
-    constexpr int LO = ORDER == 4 ? -2 : -1, HI = ORDER == 4 ? 3 : 2, W = HI - LO + 1;
     gx = gy = gz = 0.0f;
 #pragma unroll
     for (int b = 0; b < 2; ++b)
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
-            float v[W];
+            float lx[W], ly[W];
 #pragma unroll
-            for (int a = 0; a < W; ++a) v[a] = P(i + LO + a, j + b, k + c);
-            const float f0 = ORDER == 4 ? D(v[0], v[1], v[3], v[4]) : D(0.f, v[0], v[2], 0.f);
-            const float f1 = ORDER == 4 ? D(v[1], v[2], v[4], v[5]) : D(0.f, v[1], v[3], 0.f);
-            gx += wy[b] * wz[c] * (wx[0] * f0 + wx[1] * f1);
+            for (int d = 0; d < W; ++d) {
+                lx[d] = X[d][b][c];
+                ly[d] = Y[b][d][c];
+            }
+            gx += w1[b] * w2[c] * (w0[0] * D(lx, C0) + w0[1] * D(lx, C0 + 1));
+            // for y the roles are (a = b here, c): weights w0[a] w2[c]
+            gy += w0[b] * w2[c] * (w1[0] * D(ly, C0) + w1[1] * D(ly, C0 + 1));
         }
 #pragma unroll
     for (int a = 0; a < 2; ++a)
 #pragma unroll
-        for (int c = 0; c < 2; ++c) {
-            float v[W];
-#pragma unroll
-            for (int b = 0; b < W; ++b) v[b] = P(i + a, j + LO + b, k + c);
-            const float f0 = ORDER == 4 ? D(v[0], v[1], v[3], v[4]) : D(0.f, v[0], v[2], 0.f);
-            const float f1 = ORDER == 4 ? D(v[1], v[2], v[4], v[5]) : D(0.f, v[1], v[3], 0.f);
-            gy += wx[a] * wz[c] * (wy[0] * f0 + wy[1] * f1);
-        }
-#pragma unroll
-    for (int a = 0; a < 2; ++a)
-#pragma unroll
-        for (int b = 0; b < 2; ++b) {
-            float v[W];
-#pragma unroll
-            for (int c = 0; c < W; ++c) v[c] = P(i + a, j + b, k + LO + c);
-            const float f0 = ORDER == 4 ? D(v[0], v[1], v[3], v[4]) : D(0.f, v[0], v[2], 0.f);
-            const float f1 = ORDER == 4 ? D(v[1], v[2], v[4], v[5]) : D(0.f, v[1], v[3], 0.f);
-            gz += wx[a] * wy[b] * (wz[0] * f0 + wz[1] * f1);
-        }
+        for (int b = 0; b < 2; ++b) gz += w0[a] * w1[b] * (w2[0] * D(Z[a][b], C0) + w2[1] * D(Z[a][b], C0 + 1));
 }
 
 template <int ORDER>
@@ -378,12 +403,12 @@ int gradient_f64(const Plan& p, const double* phi, double* fx, double* fy, doubl
     if (p.grad_order == 4)
         {
             Timed t(p, ST_GRADIENT);
-            k_gradient_f64<4><<<grid_for(p, total, kThreads), kThreads, 0, p.stream>>>(phi, fx, fy, fz, p.ng);
+            k_gradient_f64<4><<<grid_for(p, (long long)p.ng * p.ng, 1), kThreads, 0, p.stream>>>(phi, fx, fy, fz, p.ng);
         }
     else
         {
             Timed t(p, ST_GRADIENT);
-            k_gradient_f64<2><<<grid_for(p, total, kThreads), kThreads, 0, p.stream>>>(phi, fx, fy, fz, p.ng);
+            k_gradient_f64<2><<<grid_for(p, (long long)p.ng * p.ng, 1), kThreads, 0, p.stream>>>(phi, fx, fy, fz, p.ng);
         }
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;
