@@ -95,7 +95,7 @@ const char* pm_last_error(void);
  * bracketed by CUDA events on the plan's stream.  pm_plan_read_timing waits
  * for the stream and fills ms[PM_STAGE_COUNT] (summed milliseconds) and
  * launches[PM_STAGE_COUNT] (either may be NULL); reset != 0 zeroes both. */
-#define PM_STAGE_COUNT 16
+#define PM_STAGE_COUNT 18
 int pm_plan_set_timing(pm_plan* plan, int on);
 int pm_plan_read_timing(pm_plan* plan, double* ms, int64_t* launches, int reset);
 /* Name of stage i ("mesh_init", "deposit", "fft_z_r2c", ...), "" if out of range. */
@@ -170,9 +170,19 @@ int pm_split_positions(pm_plan* plan, const double* x, const double* y, const do
 int pm_join_positions(pm_plan* plan, const uint32_t* cell, const float* ox, const float* oy,
                       const float* oz, int64_t np, double* x, double* y, double* z);
 
-/* FP32 counterparts of the stages above; mesh is float [ng][ng][ng+2]. */
+/* FP32 counterparts of the stages above; mesh is float [ng][ng][ng+2].
+ * The FP32 deposit bins the particles by 16^3-cell tile every call (counting
+ * sort into plan-owned scratch: 4 bytes per particle plus 3 x 4 bytes per
+ * (tile, face class) bucket) and writes each cell once from its tile's block;
+ * any particle order is accepted. */
 int pm_deposit_f32(pm_plan* plan, const uint32_t* cell, const float* ox, const float* oy,
                    const float* oz, int64_t np, float mass, float* mesh);
+/* Reorders the seven particle arrays in place into Z-order of their 16^3-cell
+ * tiles (counting sort; a temporary copy of the arrays is allocated and freed
+ * on the plan's stream).  Only memory locality changes, never results beyond
+ * rounding: call it after the particles have moved far from sorted order. */
+int pm_sort_f32(pm_plan* plan, uint32_t* cell, float* ox, float* oy, float* oz, float* vx,
+                float* vy, float* vz, int64_t np);
 int pm_fft_r2c_f32(pm_plan* plan, float* mesh);
 int pm_green_f32(pm_plan* plan, float* mesh, double c_poisson);
 int pm_fft_c2r_f32(pm_plan* plan, float* mesh);

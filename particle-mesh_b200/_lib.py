@@ -41,6 +41,7 @@ SIGNATURES = {
     "pm_split_positions": [_V, _V, _V, _V, _L, _V, _V, _V, _V],
     "pm_join_positions": [_V, _V, _V, _V, _V, _L, _V, _V, _V],
     "pm_deposit_f32": [_V, _V, _V, _V, _V, _L, _F, _V],
+    "pm_sort_f32": [_V, _V, _V, _V, _V, _V, _V, _V, _L],
     "pm_fft_r2c_f32": [_V, _V],
     "pm_green_f32": [_V, _V, _D],
     "pm_fft_c2r_f32": [_V, _V],
@@ -71,7 +72,7 @@ def header_symbols() -> list[str]:
     return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(pm_\w+)\s*\(", text, re.M)))
 
 
-STAGE_COUNT = 16
+STAGE_COUNT = 18
 
 
 def load(build_if_missing: bool = True) -> ctypes.CDLL:

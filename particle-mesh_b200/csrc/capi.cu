@@ -28,7 +28,7 @@ int cuda_fail(cudaError_t e, const char* what) {
 static const char* kStageNames[ST_COUNT] = {
     "mesh_init", "deposit", "fft_z_r2c", "fft_y_fwd", "fft_x_fwd", "green", "fft_x_green",
     "fft_x_inv", "fft_y_inv", "fft_z_c2r", "gradient", "interp_kick", "drift", "kick_drift",
-    "interp", "split"};
+    "interp", "split", "bin", "sort"};
 
 const char* stage_name(int st) { return st >= 0 && st < ST_COUNT ? kStageNames[st] : ""; }
 
@@ -90,6 +90,7 @@ void release(Plan& p) {
     p.d_err = nullptr;
     delete p.timers;
     p.timers = nullptr;
+    tile_scratch_release(p);
 }
 
 int ensure_workspace(Plan& p, bool forces) {
@@ -366,7 +367,15 @@ int pm_deposit_f32(pm_plan* plan, const uint32_t* cell, const float* ox, const f
     PM_TRY(check_np(np, {cell, ox, oy, oz}));
     if (!mesh) return fail(PM_ERR_ARG, "mesh is NULL");
     PM_TRY(set_device(plan->p));
-    return deposit_f32(plan->p, cell, ox, oy, oz, np, mass, mesh);
+    return deposit_f32_tiles(plan->p, cell, ox, oy, oz, np, mass, mesh);
+}
+
+int pm_sort_f32(pm_plan* plan, uint32_t* cell, float* ox, float* oy, float* oz, float* vx, float* vy,
+                float* vz, int64_t np) {
+    PM_TRY(check_plan(plan, PM_FP32));
+    PM_TRY(check_np(np, {cell, ox, oy, oz, vx, vy, vz}));
+    PM_TRY(set_device(plan->p));
+    return sort_f32(plan->p, cell, ox, oy, oz, vx, vy, vz, np);
 }
 
 int pm_fft_r2c_f32(pm_plan* plan, float* mesh) {
@@ -425,7 +434,7 @@ int pm_step_f32(pm_plan* plan, uint32_t* cell, float* ox, float* oy, float* oz, 
     Plan& p = plan->p;
     PM_TRY(ensure_workspace(p, false));
     float* m = static_cast<float*>(p.mesh);
-    PM_TRY(deposit_f32(p, cell, ox, oy, oz, np, mass, m));
+    PM_TRY(deposit_f32_tiles(p, cell, ox, oy, oz, np, mass, m));
     PM_TRY(poisson_fused<float>(p, m, c_poisson));
     PM_TRY(kick_drift_f32(p, m, cell, ox, oy, oz, vx, vy, vz, np, c_kick, dt));
     return PM_OK;

@@ -231,34 +231,6 @@ __global__ void k_join(const uint32_t* __restrict__ cell, const float* __restric
 
 // ------------------------------------------------------------------- FP32
 
-__global__ void k_deposit_f32(const uint32_t* __restrict__ cell, const float* __restrict__ ox,
-                              const float* __restrict__ oy, const float* __restrict__ oz,
-                              long long np, float mass, float* __restrict__ mesh, int n) {
-    const long long pz = n + 2;
-    const int msk = n - 1;
-    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np;
-         p += (long long)gridDim.x * blockDim.x) {
-        int i0, j0, k0;
-        unpack_cell(__ldg(cell + p), i0, j0, k0);
-        i0 &= msk; j0 &= msk; k0 &= msk;
-        const int i1 = (i0 + 1) & msk, j1 = (j0 + 1) & msk, k1 = (k0 + 1) & msk;
-        const float tx = __ldg(ox + p), ty = __ldg(oy + p), tz = __ldg(oz + p);
-        const float sx0 = 1.0f - tx, sy0 = 1.0f - ty, sz0 = 1.0f - tz;
-        const float sxy00 = sx0 * sy0, sxy10 = tx * sy0, sxy01 = sx0 * ty, sxy11 = tx * ty;
-        const float m0 = mass * sz0, m1 = mass * tz;
-        const long long r00 = ((long long)i0 * n + j0) * pz, r10 = ((long long)i1 * n + j0) * pz;
-        const long long r01 = ((long long)i0 * n + j1) * pz, r11 = ((long long)i1 * n + j1) * pz;
-        atomicAdd(mesh + r00 + k0, sxy00 * m0);
-        atomicAdd(mesh + r10 + k0, sxy10 * m0);
-        atomicAdd(mesh + r01 + k0, sxy01 * m0);
-        atomicAdd(mesh + r11 + k0, sxy11 * m0);
-        atomicAdd(mesh + r00 + k1, sxy00 * m1);
-        atomicAdd(mesh + r10 + k1, sxy10 * m1);
-        atomicAdd(mesh + r01 + k1, sxy01 * m1);
-        atomicAdd(mesh + r11 + k1, sxy11 * m1);
-    }
-}
-
 // Force at one particle with the gradient fused into the gather: the
 // trilinear weights of cells (i+a, j+b, k+c), a,b,c in {0,1}, applied to the
 // centred difference of phi at those cells (2- or 4-point).  The stencils
@@ -399,7 +371,6 @@ int deposit_f64(const Plan& p, const double* x, const double* y, const double* z
 }
 
 int gradient_f64(const Plan& p, const double* phi, double* fx, double* fy, double* fz) {
-    const long long total = (long long)p.ng * p.ng * p.ng;
     if (p.grad_order == 4)
         {
             Timed t(p, ST_GRADIENT);
@@ -456,20 +427,6 @@ int join_positions(const Plan& p, const uint32_t* cell, const float* ox, const f
         Timed t(p, ST_SPLIT);
         k_join<<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(cell, ox, oy, oz, np, x, y, z);
     }
-    PMB_CUDA_CHECK(cudaGetLastError());
-    return PM_OK;
-}
-
-int deposit_f32(const Plan& p, const uint32_t* cell, const float* ox, const float* oy,
-                const float* oz, int64_t np, float mass, float* mesh) {
-    {
-        Timed t(p, ST_MESH_INIT);
-        k_mesh_init<float><<<grid_for(p, (long long)mesh_elems(p.ng) / 4, kThreads), kThreads, 0, p.stream>>>(mesh, p.ng, -1.0f);
-    }
-    if (np > 0) {
-            Timed t(p, ST_DEPOSIT);
-            k_deposit_f32<<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(cell, ox, oy, oz, np, mass, mesh, p.ng);
-        }
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;
 }

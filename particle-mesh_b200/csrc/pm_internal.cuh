@@ -69,7 +69,7 @@ int cuda_fail(cudaError_t e, const char* what);
 enum Stage : int {
     ST_MESH_INIT, ST_DEPOSIT, ST_FFT_Z_R2C, ST_FFT_Y_FWD, ST_FFT_X_FWD, ST_GREEN, ST_FFT_X_GREEN,
     ST_FFT_X_INV, ST_FFT_Y_INV, ST_FFT_Z_C2R, ST_GRADIENT, ST_INTERP_KICK, ST_DRIFT, ST_KICK_DRIFT,
-    ST_INTERP, ST_SPLIT, ST_COUNT
+    ST_INTERP, ST_SPLIT, ST_BIN, ST_SORT, ST_COUNT
 };
 const char* stage_name(int st);
 
@@ -82,6 +82,15 @@ struct StageTimers {
     long long launches[ST_COUNT] = {};
     cudaEvent_t get();
     ~StageTimers();
+};
+
+// Scratch of the tile-binned deposit and the particle sort (tiles.cu):
+// bucket counters, exclusive offsets (nb + 1), scatter cursors, scan block
+// sums, and the bucket-ordered particle permutation.
+struct TileScratch {
+    uint32_t *count = nullptr, *off = nullptr, *cursor = nullptr, *bsum = nullptr, *perm = nullptr;
+    long long nb = 0;
+    int64_t np_cap = 0;
 };
 
 // ---------------------------------------------------------------- the plan
@@ -104,6 +113,7 @@ struct Plan {
     void* force[3] = {nullptr, nullptr, nullptr};  // FP64 force arrays
     size_t bytes = 0;
     StageTimers* timers = nullptr;  // owned by the C-ABI plan object
+    TileScratch tiles;
 };
 
 // Brackets one kernel launch with the plan's stage timer.
@@ -151,8 +161,14 @@ int split_positions(const Plan& p, const double* x, const double* y, const doubl
                     uint32_t* cell, float* ox, float* oy, float* oz);
 int join_positions(const Plan& p, const uint32_t* cell, const float* ox, const float* oy,
                    const float* oz, int64_t np, double* x, double* y, double* z);
-int deposit_f32(const Plan& p, const uint32_t* cell, const float* ox, const float* oy,
-                const float* oz, int64_t np, float mass, float* mesh);
+// Tile-binned FP32 deposit and spatial sort (tiles.cu); both may grow the
+// plan's tile scratch.
+int deposit_f32_tiles(Plan& p, const uint32_t* cell, const float* ox, const float* oy, const float* oz,
+                      int64_t np, float mass, float* mesh);
+int sort_f32(Plan& p, uint32_t* cell, float* ox, float* oy, float* oz, float* vx, float* vy, float* vz,
+             int64_t np);
+int tile_scratch_ensure(Plan& p, int64_t np);
+void tile_scratch_release(Plan& p);
 int interp_f32(const Plan& p, const float* phi, const uint32_t* cell, const float* ox,
                const float* oy, const float* oz, int64_t np, float* fx, float* fy, float* fz);
 int kick_drift_f32(const Plan& p, const float* phi, uint32_t* cell, float* ox, float* oy, float* oz,

@@ -1,0 +1,407 @@
+// Tile-binned CIC deposit for the FP32 split-position path, and the spatial
+// particle sort that keeps the particle arrays in tile order.
+//
+// The reference deposits into one private mesh per OpenMP thread and sums
+// them (src/utils/utils.cpp:70-113), then folds the +1 ghost planes into
+// their periodic images (src/decomp/slab/reorder_slab.cpp:43-68).  Here each
+// cell is written exactly once by the block that owns its tile:
+//
+//   1. bucket every particle by (tile of its base cell, face class), where a
+//      tile is TS^3 cells and the class has one bit per axis set when the base
+//      cell lies on the tile's upper face (its +1 corner leaves the tile);
+//   2. one block per tile accumulates, in shared memory, the in-tile corners
+//      of its own particles and of the face particles of its seven lower
+//      neighbours (whose +1 corners land in this tile), then stores the tile
+//      with plain coalesced stores (background -1 added, row padding zeroed).
+//
+// No global atomics touch the mesh and no separate initialisation pass is
+// needed.  Counting uses warp-aggregated atomics (__match_any_sync) on the
+// bucket counters; the exclusive scan is a three-kernel block scan.
+#include "pm_internal.cuh"
+
+namespace pmb {
+
+namespace {
+
+constexpr int kScanThreads = 1024, kScanItems = 2;  // 2048 entries per scan block
+
+__device__ __forceinline__ void unpack(uint32_t c, int& i, int& j, int& k) {
+    i = (int)(c >> 20);
+    j = (int)((c >> 10) & 1023u);
+    k = (int)(c & 1023u);
+}
+
+// Bucket of a particle: ((tx * nt + ty) * nt + tz) * 8 + class.  Cell
+// indices are wrapped by the mesh mask, so a cell >= ng (invalid input)
+// lands on its periodic image rather than outside the bucket arrays.
+__device__ __forceinline__ uint32_t bucket_of(uint32_t c, int ts_log, int nt) {
+    int i, j, k;
+    unpack(c, i, j, k);
+    const int mk = (nt << ts_log) - 1;
+    i &= mk;
+    j &= mk;
+    k &= mk;
+    const int m = (1 << ts_log) - 1;
+    const uint32_t tile = ((uint32_t)(i >> ts_log) * nt + (uint32_t)(j >> ts_log)) * nt + (uint32_t)(k >> ts_log);
+    const uint32_t cls = ((i & m) == m ? 1u : 0u) | ((j & m) == m ? 2u : 0u) | ((k & m) == m ? 4u : 0u);
+    return tile * 8u + cls;
+}
+
+// Morton (Z-order) index of a particle's tile, for the spatial sort.
+__device__ __forceinline__ uint32_t spread3(uint32_t v) {  // 10 bits -> every third bit
+    v &= 0x3ffu;
+    v = (v | (v << 16)) & 0x030000ffu;
+    v = (v | (v << 8)) & 0x0300f00fu;
+    v = (v | (v << 4)) & 0x030c30c3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+__device__ __forceinline__ uint32_t morton_tile(uint32_t c, int ts_log, int nt) {
+    int i, j, k;
+    unpack(c, i, j, k);
+    const int mk = (nt << ts_log) - 1;
+    i &= mk;
+    j &= mk;
+    k &= mk;
+    return (spread3((uint32_t)(i >> ts_log)) << 2) | (spread3((uint32_t)(j >> ts_log)) << 1) |
+           spread3((uint32_t)(k >> ts_log));
+}
+
+// count[key(p)] += 1, aggregated over the lanes of a warp that share a key.
+template <bool MORTON>
+__global__ void k_bucket_count(const uint32_t* __restrict__ cell, long long np, int ts_log, int nt,
+                               uint32_t* __restrict__ count) {
+    const int lane = threadIdx.x & 31;
+    const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long base = warp * 32; base < np; base += nwarps * 32) {
+        const long long p = base + lane;
+        const bool valid = p < np;
+        const uint32_t key = valid ? (MORTON ? morton_tile(__ldg(cell + p), ts_log, nt)
+                                             : bucket_of(__ldg(cell + p), ts_log, nt))
+                                   : 0xffffffffu;
+        const unsigned peers = __match_any_sync(0xffffffffu, key);
+        if (valid && lane == __ffs(peers) - 1) atomicAdd(count + key, (uint32_t)__popc(peers));
+    }
+}
+
+// perm[cursor[key(p)]++] = p, aggregated per warp.
+template <bool MORTON>
+__global__ void k_bucket_scatter(const uint32_t* __restrict__ cell, long long np, int ts_log, int nt,
+                                 uint32_t* __restrict__ cursor, uint32_t* __restrict__ perm) {
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long base = warp * 32; base < np; base += nwarps * 32) {
+        const long long p = base + lane;
+        const bool valid = p < np;
+        const uint32_t key = valid ? (MORTON ? morton_tile(__ldg(cell + p), ts_log, nt)
+                                             : bucket_of(__ldg(cell + p), ts_log, nt))
+                                   : 0xffffffffu;
+        const unsigned peers = __match_any_sync(0xffffffffu, key);
+        const int leader = __ffs(peers) - 1;
+        uint32_t at = 0;
+        if (valid && lane == leader) at = atomicAdd(cursor + key, (uint32_t)__popc(peers));
+        at = __shfl_sync(0xffffffffu, at, leader);
+        if (valid) perm[at + __popc(peers & lt)] = (uint32_t)p;
+    }
+}
+
+// Exclusive scan of count[0..nb) into off[0..nb] (off[nb] = total) and
+// cursor[0..nb), in three steps: per-block scan, scan of block sums, add.
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* sh, uint32_t& total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) sh[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        uint32_t s = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += y;
+        }
+        sh[lane] = s;  // inclusive prefix of warp sums
+    }
+    __syncthreads();
+    total = sh[(blockDim.x >> 5) - 1];
+    const uint32_t r = x - v + (w > 0 ? sh[w - 1] : 0u);
+    __syncthreads();
+    return r;
+}
+
+__global__ void k_scan_local(const uint32_t* __restrict__ count, long long nb, uint32_t* __restrict__ off,
+                             uint32_t* __restrict__ bsum) {
+    __shared__ uint32_t sh[32];
+    const long long i0 = (long long)blockIdx.x * kScanThreads * kScanItems + (long long)threadIdx.x * kScanItems;
+    uint32_t v[kScanItems], s = 0;
+#pragma unroll
+    for (int q = 0; q < kScanItems; ++q) {
+        v[q] = i0 + q < nb ? count[i0 + q] : 0u;
+        s += v[q];
+    }
+    uint32_t total;
+    uint32_t e = block_excl_scan(s, sh, total);
+#pragma unroll
+    for (int q = 0; q < kScanItems; ++q) {
+        if (i0 + q < nb) off[i0 + q] = e;
+        e += v[q];
+    }
+    if (threadIdx.x == 0) bsum[blockIdx.x] = total;
+}
+
+__global__ void k_scan_sums(uint32_t* __restrict__ bsum, int nblocks, uint32_t* __restrict__ total_out) {
+    __shared__ uint32_t sh[32];
+    uint32_t carry = 0;
+    for (int b0 = 0; b0 < nblocks; b0 += kScanThreads) {
+        const int b = b0 + threadIdx.x;
+        const uint32_t v = b < nblocks ? bsum[b] : 0u;
+        uint32_t tot;
+        const uint32_t e = block_excl_scan(v, sh, tot);
+        if (b < nblocks) bsum[b] = e + carry;
+        carry += tot;
+    }
+    if (threadIdx.x == 0) *total_out = carry;
+}
+
+__global__ void k_scan_add(uint32_t* __restrict__ off, uint32_t* __restrict__ cursor, long long nb,
+                           const uint32_t* __restrict__ bsum) {
+    const long long i0 = (long long)blockIdx.x * kScanThreads * kScanItems + (long long)threadIdx.x * kScanItems;
+    const uint32_t add = bsum[blockIdx.x];
+#pragma unroll
+    for (int q = 0; q < kScanItems; ++q)
+        if (i0 + q < nb) {
+            const uint32_t o = off[i0 + q] + add;
+            off[i0 + q] = o;
+            cursor[i0 + q] = o;
+        }
+}
+
+// One block per tile: accumulate, store.  Source tiles are the tile itself
+// (all classes) and its 7 lower neighbours, periodic, restricted to the
+// classes whose bits cover the neighbour offset q.  Those classes form the
+// 14 fixed runs [c0, c1) below (q = 0: all 8 classes; q = x: 1, 3, 5, 7; ...).
+constexpr int kRuns = 14;
+__constant__ int kRunQ[kRuns] = {0, 1, 1, 1, 1, 2, 2, 3, 3, 4, 5, 5, 6, 7};
+__constant__ int kRunC0[kRuns] = {0, 1, 3, 5, 7, 2, 6, 3, 7, 4, 5, 7, 6, 7};
+__constant__ int kRunC1[kRuns] = {8, 2, 4, 6, 8, 4, 8, 4, 8, 8, 6, 8, 8, 8};
+template <int TS>
+__global__ void __launch_bounds__(256) k_tile_deposit(const uint32_t* __restrict__ cell, const float* __restrict__ ox,
+                                                      const float* __restrict__ oy, const float* __restrict__ oz,
+                                                      const uint32_t* __restrict__ perm,
+                                                      const uint32_t* __restrict__ off, float mass, float background,
+                                                      float* __restrict__ mesh, int n, int nt) {
+    __shared__ __align__(16) float acc[TS * TS * TS];
+    __shared__ uint32_t rbeg[kRuns], rpre[kRuns + 1];
+    const int tile = blockIdx.x;
+    const int tx = tile / (nt * nt), ty = (tile / nt) % nt, tz = tile % nt;
+    for (int c = threadIdx.x; c < TS * TS * TS / 4; c += blockDim.x)
+        reinterpret_cast<float4*>(acc)[c] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (threadIdx.x < kRuns) {  // one bucket run per thread, loaded in parallel
+        const int q = kRunQ[threadIdx.x];
+        const int sx = (tx - (q & 1) + nt) % nt, sy = (ty - ((q >> 1) & 1) + nt) % nt;
+        const int sz = (tz - ((q >> 2) & 1) + nt) % nt;
+        const uint32_t b = (uint32_t)((sx * nt + sy) * nt + sz) * 8u;
+        const uint32_t beg = __ldg(off + b + kRunC0[threadIdx.x]);
+        rbeg[threadIdx.x] = beg;
+        rpre[threadIdx.x + 1] = __ldg(off + b + kRunC1[threadIdx.x]) - beg;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        rpre[0] = 0;
+        for (int r = 0; r < kRuns; ++r) rpre[r + 1] += rpre[r];
+    }
+    __syncthreads();
+    const uint32_t total = rpre[kRuns];
+    for (uint32_t t = threadIdx.x; t < total; t += blockDim.x) {
+        int r = 0;
+        while (t >= rpre[r + 1]) ++r;
+        const uint32_t p = __ldg(perm + rbeg[r] + (t - rpre[r]));
+        const int q = kRunQ[r];
+        int i, j, k;
+        unpack(__ldg(cell + p), i, j, k);  // (only the low ts_log bits are used below)
+        // base cell in this tile's frame: local coordinate, minus TS for a
+        // source tile one step below (the particle sits on its upper face)
+        const int li = (i & (TS - 1)) - ((q & 1) ? TS : 0);
+        const int lj = (j & (TS - 1)) - ((q & 2) ? TS : 0);
+        const int lk = (k & (TS - 1)) - ((q & 4) ? TS : 0);
+        const float fx = __ldg(ox + p), fy = __ldg(oy + p), fz = __ldg(oz + p);
+        const float wx[2] = {1.0f - fx, fx}, wy[2] = {1.0f - fy, fy}, wz[2] = {mass * (1.0f - fz), mass * fz};
+#pragma unroll
+        for (int a = 0; a < 2; ++a) {
+            const int ci = li + a;
+            if (ci < 0 || ci >= TS) continue;
+#pragma unroll
+            for (int b = 0; b < 2; ++b) {
+                const int cj = lj + b;
+                if (cj < 0 || cj >= TS) continue;
+                const float wab = wx[a] * wy[b];
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    const int ck = lk + c;
+                    if (ck < 0 || ck >= TS) continue;
+                    atomicAdd(&acc[(ci * TS + cj) * TS + ck], wab * wz[c]);
+                }
+            }
+        }
+    }
+    __syncthreads();
+    // store as float2 pairs (mesh rows are 8-byte aligned: n + 2 is even);
+    // consecutive threads take consecutive pairs of a row
+    const long long pz = n + 2;
+    constexpr int PAIRS = TS / 2;
+    for (int c = threadIdx.x; c < TS * TS * PAIRS; c += blockDim.x) {
+        const int r = c / PAIRS, ck = 2 * (c % PAIRS);  // r = ci * TS + cj
+        const long long row = (long long)(tx * TS + r / TS) * n + (ty * TS + r % TS);
+        float2* dst = reinterpret_cast<float2*>(mesh + row * pz + tz * TS + ck);
+        const float2 v = reinterpret_cast<const float2*>(acc)[c];
+        *dst = make_float2(background + v.x, background + v.y);
+        if (tz == nt - 1 && ck == TS - 2) *reinterpret_cast<float2*>(mesh + row * pz + n) = make_float2(0.f, 0.f);
+    }
+}
+
+// out[i] = in[perm[i]] for the seven particle arrays (32-bit words).
+__global__ void k_gather7(const uint32_t* __restrict__ perm, long long np, const uint32_t* const* __restrict__ src,
+                          uint32_t* const* __restrict__ dst) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < np;
+         i += (long long)gridDim.x * blockDim.x) {
+        const uint32_t p = perm[i];
+#pragma unroll
+        for (int a = 0; a < 7; ++a) dst[a][i] = __ldg(src[a] + p);
+    }
+}
+
+int tile_log(int n) { return n >= 16 ? 4 : 3; }  // 16^3 tiles (8^3 for the 8^3 mesh)
+
+// Counting sort of the bucket keys into perm / off (scratch of the plan).
+template <bool MORTON>
+int bucket_sort(const Plan& p, const uint32_t* cell, int64_t np, int ts_log, int nt, long long nb, TileScratch& s) {
+    const long long nscan = (nb + kScanThreads * kScanItems - 1) / (kScanThreads * kScanItems);
+    PMB_CUDA_CHECK(cudaMemsetAsync(s.count, 0, nb * sizeof(uint32_t), p.stream));
+    const unsigned g = grid_for(p, np, 256);
+    {
+        Timed t(p, ST_BIN);
+        if (np > 0) k_bucket_count<MORTON><<<g, 256, 0, p.stream>>>(cell, np, ts_log, nt, s.count);
+        k_scan_local<<<(unsigned)nscan, kScanThreads, 0, p.stream>>>(s.count, nb, s.off, s.bsum);
+        k_scan_sums<<<1, kScanThreads, 0, p.stream>>>(s.bsum, (int)nscan, s.off + nb);
+        k_scan_add<<<(unsigned)nscan, kScanThreads, 0, p.stream>>>(s.off, s.cursor, nb, s.bsum);
+        if (np > 0) k_bucket_scatter<MORTON><<<g, 256, 0, p.stream>>>(cell, np, ts_log, nt, s.cursor, s.perm);
+    }
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+}  // namespace
+
+int tile_scratch_ensure(Plan& p, int64_t np) {
+    const int ts = 1 << tile_log(p.ng), nt = p.ng / ts;
+    const long long nb = (long long)nt * nt * nt * 8;
+    TileScratch& s = p.tiles;
+    if (s.nb < nb) {
+        for (uint32_t** q : {&s.count, &s.off, &s.cursor, &s.bsum}) {
+            if (*q) cudaFree(*q);
+            *q = nullptr;
+        }
+        const long long nscan = (nb + kScanThreads * kScanItems - 1) / (kScanThreads * kScanItems);
+        if (cudaMalloc(&s.count, nb * 4) != cudaSuccess || cudaMalloc(&s.off, (nb + 1) * 4) != cudaSuccess ||
+            cudaMalloc(&s.cursor, nb * 4) != cudaSuccess || cudaMalloc(&s.bsum, nscan * 4) != cudaSuccess) {
+            cudaGetLastError();
+            s.nb = 0;
+            return fail(PM_ERR_NOMEM, "tile scratch allocation failed");
+        }
+        s.nb = nb;
+        p.bytes += (size_t)(nb * 3 + 1 + nscan) * 4;
+    }
+    if (s.np_cap < np) {
+        if (s.perm) cudaFree(s.perm);
+        s.perm = nullptr;
+        if (cudaMalloc(&s.perm, (size_t)np * 4) != cudaSuccess) {
+            cudaGetLastError();
+            s.np_cap = 0;
+            return fail(PM_ERR_NOMEM, "tile scratch allocation failed");
+        }
+        p.bytes += (size_t)(np - s.np_cap) * 4;
+        s.np_cap = np;
+    }
+    return PM_OK;
+}
+
+void tile_scratch_release(Plan& p) {
+    TileScratch& s = p.tiles;
+    for (uint32_t* q : {s.count, s.off, s.cursor, s.bsum, s.perm})
+        if (q) cudaFree(q);
+    s = TileScratch{};
+}
+
+int deposit_f32_tiles(Plan& p, const uint32_t* cell, const float* ox, const float* oy, const float* oz, int64_t np,
+                      float mass, float* mesh) {
+    const int tl = tile_log(p.ng), ts = 1 << tl, nt = p.ng / ts;
+    const long long nb = (long long)nt * nt * nt * 8;
+    int rc = tile_scratch_ensure(p, np > 0 ? np : 1);
+    if (rc != PM_OK) return rc;
+    rc = bucket_sort<false>(p, cell, np, tl, nt, nb, p.tiles);
+    if (rc != PM_OK) return rc;
+    {
+        Timed t(p, ST_DEPOSIT);
+        if (ts == 16)
+            k_tile_deposit<16><<<nt * nt * nt, 256, 0, p.stream>>>(cell, ox, oy, oz, p.tiles.perm, p.tiles.off, mass,
+                                                                  -1.0f, mesh, p.ng, nt);
+        else
+            k_tile_deposit<8><<<nt * nt * nt, 256, 0, p.stream>>>(cell, ox, oy, oz, p.tiles.perm, p.tiles.off, mass,
+                                                                 -1.0f, mesh, p.ng, nt);
+    }
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+int sort_f32(Plan& p, uint32_t* cell, float* ox, float* oy, float* oz, float* vx, float* vy, float* vz, int64_t np) {
+    if (np == 0) return PM_OK;
+    const int tl = tile_log(p.ng), nt = p.ng >> tl;
+    const long long nb = (long long)nt * nt * nt;  // Morton keys cover [0, nt^3) for nt a power of two
+    int rc = tile_scratch_ensure(p, np);
+    if (rc != PM_OK) return rc;
+    rc = bucket_sort<true>(p, cell, np, tl, nt, nb, p.tiles);
+    if (rc != PM_OK) return rc;
+    uint32_t* tmp = nullptr;
+    if (cudaMallocAsync(&tmp, (size_t)np * 7 * 4, p.stream) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(PM_ERR_NOMEM, "sort: temporary allocation failed");
+    }
+    uint32_t* arrays[7] = {cell, reinterpret_cast<uint32_t*>(ox), reinterpret_cast<uint32_t*>(oy),
+                           reinterpret_cast<uint32_t*>(oz), reinterpret_cast<uint32_t*>(vx),
+                           reinterpret_cast<uint32_t*>(vy), reinterpret_cast<uint32_t*>(vz)};
+    uint32_t* outs[7];
+    for (int a = 0; a < 7; ++a) outs[a] = tmp + (size_t)a * np;
+    uint32_t** dptr = nullptr;
+    if (cudaMallocAsync(&dptr, 14 * sizeof(uint32_t*), p.stream) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFreeAsync(tmp, p.stream);
+        return fail(PM_ERR_NOMEM, "sort: temporary allocation failed");
+    }
+    uint32_t* hptr[14];
+    for (int a = 0; a < 7; ++a) {
+        hptr[a] = arrays[a];
+        hptr[7 + a] = outs[a];
+    }
+    cudaMemcpyAsync(dptr, hptr, sizeof(hptr), cudaMemcpyHostToDevice, p.stream);
+    {
+        Timed t(p, ST_SORT);
+        k_gather7<<<grid_for(p, np, 256), 256, 0, p.stream>>>(p.tiles.perm, np, dptr, dptr + 7);
+    }
+    for (int a = 0; a < 7; ++a)
+        cudaMemcpyAsync(arrays[a], outs[a], (size_t)np * 4, cudaMemcpyDeviceToDevice, p.stream);
+    cudaFreeAsync(dptr, p.stream);
+    cudaFreeAsync(tmp, p.stream);
+    // the host copy of the pointer table must outlive the async copy
+    PMB_CUDA_CHECK(cudaStreamSynchronize(p.stream));
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+}  // namespace pmb

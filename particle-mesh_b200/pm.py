@@ -240,6 +240,11 @@ class Plan:
         check(self.lib.pm_deposit_f32(self._h, _vp(cell), *(_vp(t) for t in off), np_, float(mass), _vp(mesh)))
         return mesh
 
+    def sort_split(self, cell, off, vel):
+        """Reorders the particle arrays in place into tile Z-order."""
+        np_ = self._split_args(cell, off, vel)
+        check(self.lib.pm_sort_f32(self._h, _vp(cell), *(_vp(t) for t in off), *(_vp(t) for t in vel), np_))
+
     def interp_split(self, phi, cell, off):
         np_ = self._split_args(cell, off)
         out = [torch.empty(np_, dtype=torch.float32, device=self.device) for _ in range(3)]

@@ -269,6 +269,48 @@ def test_split_forces_within_1e4_of_fp64(pmpkg, O, ng, nrow, kind, order):
     assert err < 1e-4, err
 
 
+@pytest.mark.parametrize("ng,np_,mode", [(8, 300, "uniform"), (16, 4096, "faces"), (32, 40000, "uniform"),
+                                         (64, 0, "uniform"), (128, 300000, "faces")])
+def test_tile_deposit_f32_matches_oracle(pmpkg, O, ng, np_, mode):
+    """Binned owner-computes deposit, including particles on tile faces,
+    edges and the periodic wrap, and an empty particle set."""
+    rng = np.random.default_rng(ng + np_)
+    pos = [rng.uniform(0, ng, np_) for _ in range(3)]
+    if mode == "faces" and np_:
+        ts = 16 if ng >= 16 else 8
+        for a in range(3):  # a third of the particles in the last cell of a tile, some at ng - 1
+            sel = rng.random(np_) < 0.34
+            pos[a][sel] = (rng.integers(0, ng // ts, sel.sum()) * ts + ts - 1) + rng.random(sel.sum())
+    mass = 1.7
+    plan = pmpkg.Plan(ng, "fp32")
+    cell, off = plan.split(*(T(a) for a in pos))
+    got = H(plan.deposit_split(cell, off, mass)).astype(np.float64)
+    x, y, z = (H(a) for a in plan.join(cell, off))
+    ref = O.deposit(ng, x, y, z, mass)
+    assert np.abs(got - ref).max() < 1e-5 * max(1.0, mass * np_ / ng ** 3 * 8)
+    assert np.all(got[:, :, ng:] == 0)
+
+
+def test_sort_preserves_particles_and_step(pmpkg, O):
+    ng, nrow = 64, 32
+    pos, vel = O.zeldovich_ic(ng, nrow, -2.0, 0.5, seed=9)
+    plan = pmpkg.Plan(ng, "fp32", "spectral", 4)
+    cell, off = plan.split(*(T(a) for a in pos))
+    v = [T(a, torch.float32) for a in vel]
+    before = np.stack([H(cell).astype(np.float64)] + [H(a) for a in off] + [H(a) for a in v])
+    m0 = H(plan.deposit_split(cell, off, 1.0))
+    plan.sort_split(cell, off, v)
+    after = np.stack([H(cell).astype(np.float64)] + [H(a) for a in off] + [H(a) for a in v])
+    order_b = np.lexsort(before[::-1])
+    order_a = np.lexsort(after[::-1])
+    assert np.array_equal(before[:, order_b], after[:, order_a])  # same particles
+    assert not np.array_equal(before, after)                      # in a new order
+    tiles = (H(cell) >> 24, (H(cell) >> 14) & 63, (H(cell) >> 4) & 63)
+    assert len(np.unique(np.stack(tiles), axis=1).T) > 1
+    m1 = H(plan.deposit_split(cell, off, 1.0))
+    assert np.abs(m1 - m0).max() < 1e-5
+
+
 def test_split_step_kick_drift(pmpkg, O):
     ng, nrow = 64, 32
     pos, vel = O.zeldovich_ic(ng, nrow, -2.0, 0.5, seed=3)
