@@ -201,6 +201,25 @@ int pm_step_f32(pm_plan* plan, uint32_t* cell, float* ox, float* oy, float* oz, 
                 float* vy, float* vz, int64_t np, float mass, double c_poisson, double c_kick,
                 double dt);
 
+/* Allocation-free FP32 deposit.  No counterpart in the reference.  For
+ * callers that cannot allocate device memory themselves: code under a host
+ * framework whose allocator owns every device allocation, or a per-step path
+ * that must not allocate.  Same result as pm_deposit_f32 (delta into mesh
+ * [ng][ng][ng+2], background -1), but needs no plan and calls no cudaMalloc,
+ * cudaFree or allocating library routine: its scratch is a file-scope device
+ * array of 8.4 MiB (3 * 32768 + 17 bucket words plus 2^21 permutation words)
+ * that every GPU loading the library holds until the process exits.
+ * Limits: ng a power of two in [8, 256], np <= 2097152; larger sizes return
+ * PM_ERR_SIZE.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress) with that device current; make that first
+ * call before any stream capture.  Every call shares the one array, which
+ * keeps the previous call's contents (the counters are cleared on the stream
+ * at the start of each call): calls that overlap on the GPU -- on different
+ * streams, or from different threads -- race and give wrong results.
+ * stream may be NULL. */
+int pm_deposit_f32_noalloc(int ng, const uint32_t* cell, const float* ox, const float* oy,
+                           const float* oz, int64_t np, float mass, float* mesh, void* stream);
+
 /* ---------------------------------------------- initial conditions (new)
  * Zel'dovich particles on an nrow^3 lattice q = (i + 1/2) ng/nrow from a
  * Gaussian random field with P(k) ~ k^n_s, scaled to an rms 3D displacement

@@ -49,6 +49,7 @@ SIGNATURES = {
     "pm_interp_f32": [_V, _V, _V, _V, _V, _V, _L, _V, _V, _V],
     "pm_kick_drift_f32": [_V, _V, _V, _V, _V, _V, _V, _V, _V, _L, _D, _D],
     "pm_step_f32": [_V, _V, _V, _V, _V, _V, _V, _V, _L, _F, _D, _D, _D],
+    "pm_deposit_f32_noalloc": [_I, _V, _V, _V, _V, _L, _F, _V, _V],
     "pm_ic_zeldovich": [_I, _I, _D, _D, _U64, _D, _V, _V, _V, _V, _V, _V, _V],
 }
 

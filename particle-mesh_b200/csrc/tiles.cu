@@ -17,6 +17,8 @@
 // No global atomics touch the mesh and no separate initialisation pass is
 // needed.  Counting uses warp-aggregated atomics (__match_any_sync) on the
 // bucket counters; the exclusive scan is a three-kernel block scan.
+#include <mutex>
+
 #include "pm_internal.cuh"
 
 namespace pmb {
@@ -405,3 +407,100 @@ int sort_f32(Plan& p, uint32_t* cell, float* ox, float* oy, float* oz, float* vx
 }
 
 }  // namespace pmb
+
+// ------------------------------------------------ allocation-free deposit
+// pm_deposit_f32_noalloc: the tile-binned FP32 deposit for callers that
+// cannot allocate device memory themselves -- code running under a host
+// framework whose allocator owns every device allocation, or a per-step
+// path that must not allocate.  Its scratch (bucket counters, offsets,
+// cursors, scan sums, permutation) is this file-scope array: every GPU that
+// loads the library holds it until the process exits.
+namespace pmb {
+namespace {
+
+constexpr int kNoAllocMaxNg = 256;
+constexpr long long kNoAllocMaxNp = 1LL << 21;
+constexpr long long kNoAllocMaxBuckets = (long long)(kNoAllocMaxNg / 16) * (kNoAllocMaxNg / 16) *
+                                         (kNoAllocMaxNg / 16) * 8;
+constexpr long long kNoAllocScanBlocks = (kNoAllocMaxBuckets + kScanThreads * kScanItems - 1) /
+                                         (kScanThreads * kScanItems);
+constexpr size_t kNoAllocWords = (size_t)(3 * kNoAllocMaxBuckets + 1 + kNoAllocScanBlocks + kNoAllocMaxNp);
+
+__device__ __align__(256) uint32_t g_noalloc_scratch[kNoAllocWords];
+
+// The device address of g_noalloc_scratch, looked up once per device with
+// that device current (a host-side use of the symbol's name is not a device
+// address).
+struct NoAllocDevice {
+    uint32_t* scratch = nullptr;
+    int num_sms = 0;
+    bool ready = false;
+};
+constexpr int kNoAllocMaxDevices = 64;
+NoAllocDevice g_noalloc_dev[kNoAllocMaxDevices];
+std::mutex g_noalloc_mu;
+
+int noalloc_device(NoAllocDevice** out) {
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(PM_ERR_ARG, "device index out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    NoAllocDevice& d = g_noalloc_dev[dev];
+    if (!d.ready) {
+        void* ptr = nullptr;
+        e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+        e = cudaDeviceGetAttribute(&d.num_sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute");
+        d.scratch = static_cast<uint32_t*>(ptr);
+        d.ready = true;
+    }
+    *out = &d;
+    return PM_OK;
+}
+
+}  // namespace
+
+}  // namespace pmb
+
+extern "C" int pm_deposit_f32_noalloc(int ng, const uint32_t* cell, const float* ox, const float* oy,
+                                      const float* oz, int64_t np, float mass, float* mesh, void* stream) {
+    using namespace pmb;
+    if (!(ng >= 8 && ng <= kNoAllocMaxNg && (ng & (ng - 1)) == 0))
+        return fail(PM_ERR_SIZE, "pm_deposit_f32_noalloc: ng must be a power of two in [8, 256]");
+    if (np < 0) return fail(PM_ERR_ARG, "pm_deposit_f32_noalloc: negative particle count");
+    if (np > kNoAllocMaxNp)
+        return fail(PM_ERR_SIZE, "pm_deposit_f32_noalloc: at most 2097152 particles (static scratch limit)");
+    if (!mesh || (np > 0 && (!cell || !ox || !oy || !oz)))
+        return fail(PM_ERR_ARG, "pm_deposit_f32_noalloc: NULL array");
+    NoAllocDevice* d = nullptr;
+    int rc = noalloc_device(&d);
+    if (rc != PM_OK) return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int tl = tile_log(ng), ts = 1 << tl, nt = ng / ts;
+    const long long nb = (long long)nt * nt * nt * 8;
+    const long long nscan = (nb + kScanThreads * kScanItems - 1) / (kScanThreads * kScanItems);
+    uint32_t* count = d->scratch;
+    uint32_t* off = count + nb;
+    uint32_t* cursor = off + nb + 1;
+    uint32_t* bsum = cursor + nb;
+    uint32_t* perm = bsum + nscan;
+    // the array keeps the previous call's contents: counters start at zero
+    cudaError_t e = cudaMemsetAsync(count, 0, (size_t)nb * sizeof(uint32_t), s);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
+    long long need = (np + 255) / 256, cap = (long long)d->num_sms * 8;
+    const unsigned g = (unsigned)(need < 1 ? 1 : (need < cap ? need : cap));
+    if (np > 0) k_bucket_count<false><<<g, 256, 0, s>>>(cell, np, tl, nt, count);
+    k_scan_local<<<(unsigned)nscan, kScanThreads, 0, s>>>(count, nb, off, bsum);
+    k_scan_sums<<<1, kScanThreads, 0, s>>>(bsum, (int)nscan, off + nb);
+    k_scan_add<<<(unsigned)nscan, kScanThreads, 0, s>>>(off, cursor, nb, bsum);
+    if (np > 0) k_bucket_scatter<false><<<g, 256, 0, s>>>(cell, np, tl, nt, cursor, perm);
+    if (ts == 16)
+        k_tile_deposit<16><<<nt * nt * nt, 256, 0, s>>>(cell, ox, oy, oz, perm, off, mass, -1.0f, mesh, ng, nt);
+    else
+        k_tile_deposit<8><<<nt * nt * nt, 256, 0, s>>>(cell, ox, oy, oz, perm, off, mass, -1.0f, mesh, ng, nt);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "pm_deposit_f32_noalloc launch");
+    return PM_OK;
+}
