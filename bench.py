@@ -372,6 +372,38 @@ def ours(args):
         del p64, x, y, z, pv
         torch.cuda.empty_cache()
 
+    # ---- adjoint step vs forward step, differentiable-PM configuration
+    adjoint = None
+    if not args.skip_fp64:
+        na = 128
+        pa, va = pm.zeldovich_ic(na, na, -2.0, 0.5, 7 + rank, device=dev)
+        pla = pm.Plan(na, "fp64", "spectral", 4, stream=stream, device=dev)
+        xb = [torch.randn_like(pa[0]) for _ in range(3)]
+        vb = [torch.randn_like(pa[0]) for _ in range(3)]
+        xs = [a.clone() for a in pa]
+        vs = [a.clone() for a in va]
+
+        def timed(fn, reps=20):
+            for _ in range(3):
+                fn()
+            torch.cuda.synchronize()
+            e0.record(stream)
+            for _ in range(reps):
+                fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1) / reps
+
+        t_f = timed(lambda: pla.step(*xs, *vs, 1.0, cp, 0.01, 0.0))
+        t_a = timed(lambda: pla.step_adjoint(*pa, 1.0, cp, 0.01, 0.01, xb, vb))
+        adjoint = {"config": "128^3 particles on 128^3 mesh, FP64, spectral Poisson, 4-point gradient",
+                   "forward_step_ms": t_f, "adjoint_step_ms": t_a, "adjoint_over_forward": t_a / t_f,
+                   "with_recompute_over_forward": (t_a + t_f) / t_f,
+                   "note": "adjoint step = force recomputation at the step's start + transposed pairs; "
+                           "checkpointed backprop also re-runs each forward step once"}
+        pla.close()
+        del pla, pa, va, xb, vb, xs, vs
+
     # ---- end to end through the C ABI with host buffers
     e2e = None
     if not args.skip_e2e:
@@ -432,7 +464,7 @@ def ours(args):
                        "parallelism": f"{world} independent boxes, one per GPU"},
             "fp64": fp64, "force_err": force_err,
             "speedup_fp32_vs_fp64": (value / fp64["value"]) if fp64 else None,
-            "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "stages": per_stage,
+            "e2e": e2e, "adjoint": adjoint, "gpu_launches": launches, "roofline": roofline, "stages": per_stage,
             "cpu_baseline": cpu, "clocks": clocks}
     print(json.dumps(line), flush=True)
     return 0

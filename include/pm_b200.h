@@ -95,7 +95,7 @@ const char* pm_last_error(void);
  * bracketed by CUDA events on the plan's stream.  pm_plan_read_timing waits
  * for the stream and fills ms[PM_STAGE_COUNT] (summed milliseconds) and
  * launches[PM_STAGE_COUNT] (either may be NULL); reset != 0 zeroes both. */
-#define PM_STAGE_COUNT 18
+#define PM_STAGE_COUNT 19
 int pm_plan_set_timing(pm_plan* plan, int on);
 int pm_plan_read_timing(pm_plan* plan, double* ms, int64_t* launches, int reset);
 /* Name of stage i ("mesh_init", "deposit", "fft_z_r2c", ...), "" if out of range. */
@@ -155,6 +155,31 @@ int pm_drift_f64(pm_plan* plan, double* x, double* y, double* z, const double* p
  * src/core/main.cpp:91-138. */
 int pm_step_f64(pm_plan* plan, double* x, double* y, double* z, double* px, double* py,
                 double* pz, int64_t np, double mass, double c_poisson, double c_kick, double dt);
+
+/* ------------------------------------------------- FP64 adjoints (new)
+ * Vector-Jacobian products of the step for reverse-mode differentiation; no
+ * counterpart in the reference.  All add into their output arrays.
+ *
+ * pm_adjoint_deposit_f64: xbar += (d delta / d x)^T dbar, the adjoint of
+ *   pm_deposit_f64 (dbar a mesh [ng][ng][ng+2]; padding ignored): the CIC
+ *   weight-derivative gather mass * grad W(x_p - c) . dbar(c).
+ * pm_adjoint_force_f64: xbar += scale * (dF/dx)^T u, F the particle forces
+ *   of pm_step_f64 at x (deposit, Poisson with c_poisson, gradient,
+ *   interpolation): the direct weight-derivative term u . grad W . f plus the
+ *   mesh term through the transposed pairs (interpolation^T = deposit,
+ *   gradient^T = -gradient, the symmetric Green's multiply, deposit^T =
+ *   weight-derivative gather).  Uses the plan's workspace.
+ * pm_step_adjoint_f64: the adjoint of one pm_step_f64 (v' = v + c_kick F(x);
+ *   x' = x + dt v').  On entry (xbar, vbar) are the adjoints of (x', v'); on
+ *   return those of (x, v).  x is the state the forward step started from. */
+int pm_adjoint_deposit_f64(pm_plan* plan, const double* x, const double* y, const double* z, int64_t np,
+                           double mass, const double* dbar, double* xbar, double* ybar, double* zbar);
+int pm_adjoint_force_f64(pm_plan* plan, const double* x, const double* y, const double* z, int64_t np,
+                         double mass, double c_poisson, const double* ux, const double* uy,
+                         const double* uz, double scale, double* xbar, double* ybar, double* zbar);
+int pm_step_adjoint_f64(pm_plan* plan, const double* x, const double* y, const double* z, int64_t np,
+                        double mass, double c_poisson, double c_kick, double dt, double* xbar,
+                        double* ybar, double* zbar, double* vxbar, double* vybar, double* vzbar);
 
 /* Device pointer to the plan's own mesh [ng][ng][ng+2] (density after the
  * deposit of pm_step_*, potential after it returns). */

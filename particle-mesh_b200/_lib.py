@@ -38,6 +38,9 @@ SIGNATURES = {
     "pm_interp_kick_f64": [_V, _V, _V, _V, _V, _V, _V, _V, _V, _V, _L, _D],
     "pm_drift_f64": [_V, _V, _V, _V, _V, _V, _V, _L, _D],
     "pm_step_f64": [_V, _V, _V, _V, _V, _V, _V, _L, _D, _D, _D, _D],
+    "pm_adjoint_deposit_f64": [_V, _V, _V, _V, _L, _D, _V, _V, _V, _V],
+    "pm_adjoint_force_f64": [_V, _V, _V, _V, _L, _D, _D, _V, _V, _V, _D, _V, _V, _V],
+    "pm_step_adjoint_f64": [_V, _V, _V, _V, _L, _D, _D, _D, _D, _V, _V, _V, _V, _V, _V],
     "pm_split_positions": [_V, _V, _V, _V, _L, _V, _V, _V, _V],
     "pm_join_positions": [_V, _V, _V, _V, _V, _L, _V, _V, _V],
     "pm_deposit_f32": [_V, _V, _V, _V, _V, _L, _F, _V],
@@ -73,7 +76,7 @@ def header_symbols() -> list[str]:
     return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(pm_\w+)\s*\(", text, re.M)))
 
 
-STAGE_COUNT = 18
+STAGE_COUNT = 19
 
 
 def load(build_if_missing: bool = True) -> ctypes.CDLL:

@@ -28,7 +28,7 @@ int cuda_fail(cudaError_t e, const char* what) {
 static const char* kStageNames[ST_COUNT] = {
     "mesh_init", "deposit", "fft_z_r2c", "fft_y_fwd", "fft_x_fwd", "green", "fft_x_green",
     "fft_x_inv", "fft_y_inv", "fft_z_c2r", "gradient", "interp_kick", "drift", "kick_drift",
-    "interp", "split", "bin", "sort"};
+    "interp", "split", "bin", "sort", "adjoint"};
 
 const char* stage_name(int st) { return st >= 0 && st < ST_COUNT ? kStageNames[st] : ""; }
 
@@ -341,6 +341,64 @@ int pm_step_f64(pm_plan* plan, double* x, double* y, double* z, double* px, doub
     PM_TRY(interp_kick_f64(p, x, y, z, f[0], f[1], f[2], px, py, pz, np, c_kick));
     if (dt != 0.0) PM_TRY(drift_f64(p, x, y, z, px, py, pz, np, dt));
     return PM_OK;
+}
+
+// ------------------------------------------------------- FP64 adjoints
+
+int pm_adjoint_deposit_f64(pm_plan* plan, const double* x, const double* y, const double* z, int64_t np,
+                           double mass, const double* dbar, double* xbar, double* ybar, double* zbar) {
+    PM_TRY(check_plan(plan, PM_FP64));
+    PM_TRY(check_np(np, {x, y, z, xbar, ybar, zbar}));
+    if (!dbar) return fail(PM_ERR_ARG, "dbar is NULL");
+    PM_TRY(set_device(plan->p));
+    return adjoint_gather_f64(plan->p, x, y, z, dbar, mass, nullptr, nullptr, 0.0, xbar, ybar, zbar, np);
+}
+
+// Recomputes the force meshes at x on the plan's workspace, adds the direct
+// (weight-derivative) term, then reuses the workspace for the mesh term.
+static int adjoint_force(Plan& p, const double* x, const double* y, const double* z, int64_t np, double mass,
+                         double c_poisson, const double* ux, const double* uy, const double* uz, double scale,
+                         double* xbar, double* ybar, double* zbar) {
+    PM_TRY(ensure_workspace(p, true));
+    double* m = static_cast<double*>(p.mesh);
+    double* f[3] = {static_cast<double*>(p.force[0]), static_cast<double*>(p.force[1]),
+                    static_cast<double*>(p.force[2])};
+    const double* fc[3] = {f[0], f[1], f[2]};
+    const double* u[3] = {ux, uy, uz};
+    PM_TRY(deposit_f64(p, x, y, z, np, mass, m));
+    PM_TRY(fft_r2c<double>(p, m));
+    PM_TRY(green_apply<double>(p, m, c_poisson));
+    PM_TRY(fft_c2r<double>(p, m));
+    PM_TRY(gradient_f64(p, m, f[0], f[1], f[2]));
+    PM_TRY(adjoint_gather_f64(p, x, y, z, nullptr, 0.0, u, fc, scale, xbar, ybar, zbar, np));
+    PM_TRY(adjoint_mesh_source_f64(p, x, y, z, u, np, f, m));
+    PM_TRY(fft_r2c<double>(p, m));
+    PM_TRY(green_apply<double>(p, m, c_poisson));
+    PM_TRY(fft_c2r<double>(p, m));
+    return adjoint_gather_f64(p, x, y, z, m, scale * mass, nullptr, nullptr, 0.0, xbar, ybar, zbar, np);
+}
+
+int pm_adjoint_force_f64(pm_plan* plan, const double* x, const double* y, const double* z, int64_t np,
+                         double mass, double c_poisson, const double* ux, const double* uy, const double* uz,
+                         double scale, double* xbar, double* ybar, double* zbar) {
+    PM_TRY(check_plan(plan, PM_FP64));
+    PM_TRY(check_np(np, {x, y, z, ux, uy, uz, xbar, ybar, zbar}));
+    PM_TRY(set_device(plan->p));
+    return adjoint_force(plan->p, x, y, z, np, mass, c_poisson, ux, uy, uz, scale, xbar, ybar, zbar);
+}
+
+int pm_step_adjoint_f64(pm_plan* plan, const double* x, const double* y, const double* z, int64_t np,
+                        double mass, double c_poisson, double c_kick, double dt, double* xbar, double* ybar,
+                        double* zbar, double* vxbar, double* vybar, double* vzbar) {
+    PM_TRY(check_plan(plan, PM_FP64));
+    PM_TRY(check_np(np, {x, y, z, xbar, ybar, zbar, vxbar, vybar, vzbar}));
+    PM_TRY(set_device(plan->p));
+    Plan& p = plan->p;
+    double* vb[3] = {vxbar, vybar, vzbar};
+    const double* xb[3] = {xbar, ybar, zbar};
+    if (dt != 0.0) PM_TRY(axpy3_f64(p, vb, xb, dt, np));  // x' = x + dt v'  =>  vbar' += dt xbar
+    if (c_kick == 0.0) return PM_OK;
+    return adjoint_force(p, x, y, z, np, mass, c_poisson, vxbar, vybar, vzbar, c_kick, xbar, ybar, zbar);
 }
 
 // ------------------------------------------------------------------ FP32

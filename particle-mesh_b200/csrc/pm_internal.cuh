@@ -69,7 +69,7 @@ int cuda_fail(cudaError_t e, const char* what);
 enum Stage : int {
     ST_MESH_INIT, ST_DEPOSIT, ST_FFT_Z_R2C, ST_FFT_Y_FWD, ST_FFT_X_FWD, ST_GREEN, ST_FFT_X_GREEN,
     ST_FFT_X_INV, ST_FFT_Y_INV, ST_FFT_Z_C2R, ST_GRADIENT, ST_INTERP_KICK, ST_DRIFT, ST_KICK_DRIFT,
-    ST_INTERP, ST_SPLIT, ST_BIN, ST_SORT, ST_COUNT
+    ST_INTERP, ST_SPLIT, ST_BIN, ST_SORT, ST_ADJOINT, ST_COUNT
 };
 const char* stage_name(int st);
 
@@ -173,6 +173,14 @@ int interp_f32(const Plan& p, const float* phi, const uint32_t* cell, const floa
                const float* oy, const float* oz, int64_t np, float* fx, float* fy, float* fz);
 int kick_drift_f32(const Plan& p, const float* phi, uint32_t* cell, float* ox, float* oy, float* oz,
                    float* vx, float* vy, float* vz, int64_t np, double c_kick, double dt);
+
+// Adjoint kernels (adjoint.cu).
+int adjoint_gather_f64(const Plan& p, const double* x, const double* y, const double* z, const double* dbar,
+                       double scale_d, const double* u[3], const double* f[3], double scale_u, double* bx,
+                       double* by, double* bz, int64_t np);
+int adjoint_mesh_source_f64(const Plan& p, const double* x, const double* y, const double* z, const double* u[3],
+                            int64_t np, double* ub[3], double* phibar);
+int axpy3_f64(const Plan& p, double* y[3], const double* x[3], double a, int64_t np);
 
 // Zel'dovich initial conditions (ic.cu); p is an FP64 plan of size nrow.
 int ic_zeldovich(const Plan& p, double n_s, double rms_cells, uint64_t seed, double vel_factor, int ng,

@@ -205,6 +205,35 @@ class Plan:
         check(self.lib.pm_step_f64(self._h, _vp(x), _vp(y), _vp(z), _vp(px), _vp(py), _vp(pz), np_,
                                    float(mass), float(c_poisson), float(c_kick), float(dt)))
 
+    # ----------------------------------------------------------- adjoints
+    def adjoint_deposit(self, x, y, z, mass: float, dbar, xbar):
+        np_ = x.numel()
+        for t, nm in ((x, "x"), (y, "y"), (z, "z")):
+            _need(t, torch.float64, np_, name=nm)
+        for t, nm in zip(xbar, ("xbar", "ybar", "zbar")):
+            _need(t, torch.float64, np_, name=nm)
+        check(self.lib.pm_adjoint_deposit_f64(self._h, _vp(x), _vp(y), _vp(z), np_, float(mass),
+                                              _vp(self._mesh(dbar, "dbar")), *(_vp(t) for t in xbar)))
+
+    def adjoint_force(self, x, y, z, mass: float, c_poisson: float, u, scale: float, xbar):
+        np_ = x.numel()
+        for t, nm in ((x, "x"), (y, "y"), (z, "z")):
+            _need(t, torch.float64, np_, name=nm)
+        for t in (*u, *xbar):
+            _need(t, torch.float64, np_, name="adjoint array")
+        check(self.lib.pm_adjoint_force_f64(self._h, _vp(x), _vp(y), _vp(z), np_, float(mass), float(c_poisson),
+                                            *(_vp(t) for t in u), float(scale), *(_vp(t) for t in xbar)))
+
+    def step_adjoint(self, x, y, z, mass: float, c_poisson: float, c_kick: float, dt: float, xbar, vbar):
+        np_ = x.numel()
+        for t, nm in ((x, "x"), (y, "y"), (z, "z")):
+            _need(t, torch.float64, np_, name=nm)
+        for t in (*xbar, *vbar):
+            _need(t, torch.float64, np_, name="adjoint array")
+        check(self.lib.pm_step_adjoint_f64(self._h, _vp(x), _vp(y), _vp(z), np_, float(mass), float(c_poisson),
+                                           float(c_kick), float(dt), *(_vp(t) for t in xbar),
+                                           *(_vp(t) for t in vbar)))
+
     # ------------------------------------------------- FP32 split positions
     def split(self, x, y, z):
         np_ = x.numel()
