@@ -155,10 +155,18 @@ extern "C" {
 
 const char* pm_last_error(void) { return g_last_error.c_str(); }
 
-int pm_plan_create(int ng, int precision, int green_kind, int grad_order, void* stream, pm_plan** out) {
+}  // extern "C"
+
+// allow_fp64_any: internal FP64 plans (initial conditions) may use the mixed-radix
+// sizes, whose FP64 particle kernels do not exist.
+static int plan_create(int ng, int precision, int green_kind, int grad_order, void* stream, pm_plan** out,
+                       bool allow_fp64_any) {
     if (!out) return fail(PM_ERR_ARG, "output pointer is NULL");
     *out = nullptr;
-    if (!fft_size_supported(ng)) return fail(PM_ERR_SIZE, "ng must be a power of two in [8, 1024]");
+    if (!fft_size_supported(ng))
+        return fail(PM_ERR_SIZE, "ng must be a power of two in [8, 1024], or 48 or 96 (FP32)");
+    if (precision == PM_FP64 && (ng & (ng - 1)) != 0 && !allow_fp64_any)
+        return fail(PM_ERR_SIZE, "FP64 plans need a power-of-two ng");
     if (precision != PM_FP64 && precision != PM_FP32) return fail(PM_ERR_ARG, "unknown precision");
     if (green_kind != PM_GREEN_DISCRETE && green_kind != PM_GREEN_SPECTRAL) return fail(PM_ERR_ARG, "unknown green_kind");
     if (grad_order != 2 && grad_order != 4) return fail(PM_ERR_ARG, "grad_order must be 2 or 4");
@@ -192,6 +200,12 @@ int pm_plan_create(int ng, int precision, int green_kind, int grad_order, void* 
     }
     *out = plan;
     return PM_OK;
+}
+
+extern "C" {
+
+int pm_plan_create(int ng, int precision, int green_kind, int grad_order, void* stream, pm_plan** out) {
+    return plan_create(ng, precision, green_kind, grad_order, stream, out, false);
 }
 
 int pm_plan_destroy(pm_plan* plan) {
@@ -503,12 +517,12 @@ int pm_step_f32(pm_plan* plan, uint32_t* cell, float* ox, float* oy, float* oz, 
 int pm_ic_zeldovich(int ng, int nrow, double n_s, double rms_cells, uint64_t seed,
                     double vel_factor, double* x, double* y, double* z, double* vx, double* vy,
                     double* vz, void* stream) {
-    if (!fft_size_supported(nrow)) return fail(PM_ERR_SIZE, "nrow must be a power of two in [8, 1024]");
+    if (!fft_size_supported(nrow)) return fail(PM_ERR_SIZE, "nrow must be a power of two in [8, 1024], or 48 or 96");
     if (ng < 1) return fail(PM_ERR_ARG, "ng must be positive");
     if (!(rms_cells >= 0.0) || !std::isfinite(n_s)) return fail(PM_ERR_ARG, "bad spectrum parameters");
     PM_TRY(check_np(1, {x, y, z, vx, vy, vz}));
     pm_plan* plan = nullptr;
-    PM_TRY(pm_plan_create(nrow, PM_FP64, PM_GREEN_DISCRETE, 2, stream, &plan));
+    PM_TRY(plan_create(nrow, PM_FP64, PM_GREEN_DISCRETE, 2, stream, &plan, true));
     const int rc = ic_zeldovich(plan->p, n_s, rms_cells, seed, vel_factor, ng, x, y, z, vx, vy, vz);
     pm_plan_destroy(plan);
     return rc;

@@ -13,7 +13,9 @@
 //           global load / store of a warp is a contiguous run of TK complex.
 //   fused x pass: forward x FFT, Green multiply, inverse x FFT in one block,
 //           so the Poisson solve costs 5 passes instead of 7.
-#include "fft_engine.cuh"
+#include <type_traits>
+
+#include "fft_generic.cuh"
 
 namespace pmb {
 
@@ -155,7 +157,7 @@ template <typename T, int N> constexpr int strided_smem_elems() { return (N + N 
 
 template <typename T, int N, int DIR>
 __global__ void __launch_bounds__(strided_threads<T, N>(), 2)
-k_fft_strided(typename Cx<T>::t* __restrict__ data, long long es, long long os, int ncols,
+k_fft_strided(typename Cx<T>::t* __restrict__ data, long long es, long long os, long long bs, int ncols,
               const typename Cx<T>::t* __restrict__ tw) {
     using C = typename Cx<T>::t;
     constexpr int R1 = Radix<N>::R1, R2 = Radix<N>::R2, TK = tk_cols<T, N>();
@@ -164,7 +166,8 @@ k_fft_strided(typename Cx<T>::t* __restrict__ data, long long es, long long os, 
     const int tx = threadIdx.x % TK, ty = threadIdx.x / TK;
     const int col = blockIdx.x * TK + tx;
     const bool active = col < ncols;
-    C* base = data + (long long)blockIdx.y * os + (active ? col : 0);
+    // plane blockIdx.y % N of box blockIdx.y / N (boxes of a batch at stride bs)
+    C* base = data + (long long)(blockIdx.y / N) * bs + (long long)(blockIdx.y % N) * os + (active ? col : 0);
 
     using I = SIdx<R1, R2, TK>;
     const long long es1 = es * R2, es2 = es * R1;
@@ -205,7 +208,7 @@ __device__ __forceinline__ T green_value(int kx, int ky, int kz, int kind, doubl
 // inverse FFT along x, for TK kz columns of one ky plane.
 template <typename T, int N>
 __global__ void __launch_bounds__(strided_threads<T, N>(), 2)
-k_fft_x_green(typename Cx<T>::t* __restrict__ data, long long es, long long os, int ncols,
+k_fft_x_green(typename Cx<T>::t* __restrict__ data, long long es, long long os, long long bs, int ncols,
               const typename Cx<T>::t* __restrict__ tw, const T* __restrict__ g1d, double cg, int kind) {
     using C = typename Cx<T>::t;
     constexpr int R1 = Radix<N>::R1, R2 = Radix<N>::R2, TK = tk_cols<T, N>();
@@ -214,8 +217,8 @@ k_fft_x_green(typename Cx<T>::t* __restrict__ data, long long es, long long os, 
     const int tx = threadIdx.x % TK, ty = threadIdx.x / TK;
     const int col = blockIdx.x * TK + tx;
     const bool active = col < ncols;
-    const int ky = blockIdx.y;
-    C* base = data + (long long)ky * os + (active ? col : 0);
+    const int ky = blockIdx.y % N;
+    C* base = data + (long long)(blockIdx.y / N) * bs + (long long)ky * os + (active ? col : 0);
 
     using I = SIdx<R1, R2, TK>;
     const long long es1 = es * R2, es2 = es * R1;
@@ -244,14 +247,143 @@ k_fft_x_green(typename Cx<T>::t* __restrict__ data, long long es, long long os, 
 template <typename T>
 __global__ void k_green(typename Cx<T>::t* __restrict__ spec, int n, const typename Cx<T>::t* __restrict__ tw,
                         const T* __restrict__ g1d, double cg, int kind) {
-    const int h = n / 2 + 1, msk = n - 1, sh = __ffs(n) - 1;
+    const int h = n / 2 + 1;
     for (long long row = blockIdx.x; row < (long long)n * n; row += gridDim.x) {
-        const int kx = (int)(row >> sh), ky = (int)(row & msk);
+        const int kx = (int)(row / n), ky = (int)(row % n);
         typename Cx<T>::t* r = spec + row * h;
         for (int kz = threadIdx.x; kz < h; kz += blockDim.x)
             r[kz] = cscale(r[kz], green_value<T>(kx, ky, kz, kind, cg, tw, g1d));
     }
 }
+
+// ---------------------------------------------- 48 and 96: generic passes
+template <int N> constexpr int g_z_rows() { return 256 / GRadix<N / 2>::NT; }
+constexpr int kGTK = 16;  // columns per block of the generic strided passes
+
+template <typename T, int N>
+__global__ void __launch_bounds__(256) k_fftg_z_r2c(T* __restrict__ mesh, long long nrows,
+                                                    const typename Cx<T>::t* __restrict__ tw) {
+    using C = typename Cx<T>::t;
+    constexpr int M = N / 2, NT = GRadix<M>::NT, LPB = g_z_rows<N>();
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* A = reinterpret_cast<C*>(smraw) + (threadIdx.x / NT) * 2 * (M + 1);
+    C* B = A + (M + 1);
+    const int tj = threadIdx.x % NT;
+    const long long row = (long long)blockIdx.x * LPB + threadIdx.x / NT;
+    const bool active = row < nrows;
+    C* crow = reinterpret_cast<C*>(mesh + (active ? row : 0) * (long long)(N + 2));
+    for (int k = tj; k < M; k += NT) A[k] = active ? crow[k] : cmake<C>(0, 0);
+    __syncthreads();
+    const C* Z = gfft<M, -1>(A, B, tj, [](int e) { return e; }, tw, 2);
+    if (active) {
+        for (int k = tj; k <= M; k += NT) {
+            const C zk = Z[k == M ? 0 : k];
+            const C zc = cconj(Z[k == 0 ? 0 : M - k]);
+            const C e = cscale(cadd(zk, zc), (T)0.5);
+            const C d = csub(zk, zc);
+            const C o = cmake<C>((T)0.5 * d.y, (T)-0.5 * d.x);
+            crow[k] = cadd(e, cmul(twiddle<-1>(tw, k), o));
+        }
+    }
+}
+
+template <typename T, int N>
+__global__ void __launch_bounds__(256) k_fftg_z_c2r(T* __restrict__ mesh, long long nrows,
+                                                    const typename Cx<T>::t* __restrict__ tw) {
+    using C = typename Cx<T>::t;
+    constexpr int M = N / 2, NT = GRadix<M>::NT, LPB = g_z_rows<N>();
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* A = reinterpret_cast<C*>(smraw) + (threadIdx.x / NT) * 2 * (M + 1);
+    C* B = A + (M + 1);
+    const int tj = threadIdx.x % NT;
+    const long long row = (long long)blockIdx.x * LPB + threadIdx.x / NT;
+    const bool active = row < nrows;
+    C* crow = reinterpret_cast<C*>(mesh + (active ? row : 0) * (long long)(N + 2));
+    for (int k = tj; k <= M; k += NT) {
+        C x = active ? crow[k] : cmake<C>(0, 0);
+        if (k == 0 || k == M) x.y = 0;
+        A[k] = x;
+    }
+    __syncthreads();
+    for (int k = tj; k < M; k += NT) {
+        const C a = A[k], b = cconj(A[M - k]);
+        const C s = cadd(a, b), d = cmul(csub(a, b), twiddle<+1>(tw, k));
+        B[k] = cmake<C>(s.x - d.y, s.y + d.x);
+    }
+    __syncthreads();
+    const C* z = gfft<M, +1>(B, A, tj, [](int e) { return e; }, tw, 2);
+    if (active) {
+        for (int k = tj; k < M; k += NT) crow[k] = z[k];
+        if (tj == 0) crow[M] = cmake<C>(0, 0);
+    }
+}
+
+template <typename T, int N, int DIR, bool GREEN>
+__global__ void __launch_bounds__(kGTK * GRadix<N>::NT)
+k_fftg_strided(typename Cx<T>::t* __restrict__ data, long long es, long long os, long long bs, int ncols,
+               const typename Cx<T>::t* __restrict__ tw, const T* __restrict__ g1d, double cg, int kind) {
+    using C = typename Cx<T>::t;
+    constexpr int NT = GRadix<N>::NT, TK = kGTK;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* A = reinterpret_cast<C*>(smraw);
+    C* B = A + N * TK;
+    const int tx = threadIdx.x % TK, ty = threadIdx.x / TK;
+    const int col = blockIdx.x * TK + tx;
+    const bool active = col < ncols;
+    const int plane = blockIdx.y % N, box = blockIdx.y / N;
+    C* base = data + box * bs + plane * os + (active ? col : 0);
+    auto ix = [&](int e) { return e * TK + tx; };
+    for (int e = ty; e < N; e += NT) A[ix(e)] = active ? base[e * es] : cmake<C>(0, 0);
+    __syncthreads();
+    C* r = gfft<N, DIR>(A, B, ty, ix, tw, 1);
+    if constexpr (GREEN) {
+        for (int e = ty; e < N; e += NT)
+            r[ix(e)] = cscale(r[ix(e)], active ? green_value<T>(e, plane, col, kind, cg, tw, g1d) : (T)0);
+        __syncthreads();
+        r = gfft<N, +1>(r, r == A ? B : A, ty, ix, tw, 1);
+    }
+    if (active)
+        for (int e = ty; e < N; e += NT) base[e * es] = r[ix(e)];
+}
+
+template <typename T, int N> struct LaunchG {
+    using C = typename Cx<T>::t;
+    static constexpr int H = N / 2 + 1;
+    static size_t smem_z() { return (size_t)g_z_rows<N>() * 2 * (N / 2 + 1) * sizeof(C); }
+    static size_t smem_s() { return (size_t)2 * N * kGTK * sizeof(C); }
+    static int prepare() { return PM_OK; }
+    static void z(const Plan& p, T* mesh, bool forward, int nbox = 1) {
+        const long long rows = (long long)nbox * N * N;
+        const unsigned grid = (unsigned)((rows + g_z_rows<N>() - 1) / g_z_rows<N>());
+        const C* tw = static_cast<const C*>(p.tw);
+        Timed t(p, forward ? ST_FFT_Z_R2C : ST_FFT_Z_C2R);
+        if (forward)
+            k_fftg_z_r2c<T, N><<<grid, 256, smem_z(), p.stream>>>(mesh, rows, tw);
+        else
+            k_fftg_z_c2r<T, N><<<grid, 256, smem_z(), p.stream>>>(mesh, rows, tw);
+    }
+    static void strided(const Plan& p, T* mesh, int axis, int dir, int nbox = 1) {
+        C* d = reinterpret_cast<C*>(mesh);
+        const long long es = axis == 1 ? H : (long long)N * H, os = axis == 1 ? (long long)N * H : H;
+        dim3 grid((H + kGTK - 1) / kGTK, N * nbox);
+        const C* tw = static_cast<const C*>(p.tw);
+        const T* g = static_cast<const T*>(p.g1d);
+        Timed t(p, axis == 1 ? (dir < 0 ? ST_FFT_Y_FWD : ST_FFT_Y_INV) : (dir < 0 ? ST_FFT_X_FWD : ST_FFT_X_INV));
+        const long long bs = (long long)N * N * H;
+        if (dir < 0)
+            k_fftg_strided<T, N, -1, false><<<grid, kGTK * GRadix<N>::NT, smem_s(), p.stream>>>(d, es, os, bs, H, tw, g, 0.0, 0);
+        else
+            k_fftg_strided<T, N, +1, false><<<grid, kGTK * GRadix<N>::NT, smem_s(), p.stream>>>(d, es, os, bs, H, tw, g, 0.0, 0);
+    }
+    static void xgreen(const Plan& p, T* mesh, double cg, int nbox = 1) {
+        C* d = reinterpret_cast<C*>(mesh);
+        dim3 grid((H + kGTK - 1) / kGTK, N * nbox);
+        Timed t(p, ST_FFT_X_GREEN);
+        k_fftg_strided<T, N, -1, true><<<grid, kGTK * GRadix<N>::NT, smem_s(), p.stream>>>(
+            d, (long long)N * H, H, (long long)N * N * H, H, static_cast<const C*>(p.tw), static_cast<const T*>(p.g1d),
+            cg, p.green_kind);
+    }
+};
 
 // ------------------------------------------------------------- launchers
 template <typename T, int N> struct Launch {
@@ -267,8 +399,8 @@ template <typename T, int N> struct Launch {
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_x_green<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         return PM_OK;
     }
-    static void z(const Plan& p, T* mesh, bool forward) {
-        const long long rows = (long long)N * N;
+    static void z(const Plan& p, T* mesh, bool forward, int nbox = 1) {
+        const long long rows = (long long)nbox * N * N;
         const unsigned grid = (unsigned)((rows + z_rows_per_block<T, N>() - 1) / z_rows_per_block<T, N>());
         const int thr = z_threads_per_row<N>() * z_rows_per_block<T, N>();
         const C* tw = static_cast<const C*>(p.tw);
@@ -278,24 +410,27 @@ template <typename T, int N> struct Launch {
         else
             k_fft_z_c2r<T, N><<<grid, thr, smem_z(), p.stream>>>(mesh, rows, tw);
     }
-    // axis 1 = y (stride H, planes x), axis 0 = x (stride N H, planes y)
-    static void strided(const Plan& p, T* mesh, int axis, int dir) {
+    // axis 1 = y (stride H, planes x), axis 0 = x (stride N H, planes y); a
+    // batch of nbox meshes lies at a stride of N^2 H complex
+    static void strided(const Plan& p, T* mesh, int axis, int dir, int nbox = 1) {
         C* d = reinterpret_cast<C*>(mesh);
         const long long es = axis == 1 ? H : (long long)N * H, os = axis == 1 ? (long long)N * H : H;
-        dim3 grid((H + tk_cols<T, N>() - 1) / tk_cols<T, N>(), N);
+        const long long bs = (long long)N * N * H;
+        dim3 grid((H + tk_cols<T, N>() - 1) / tk_cols<T, N>(), N * nbox);
         const C* tw = static_cast<const C*>(p.tw);
         Timed t(p, axis == 1 ? (dir < 0 ? ST_FFT_Y_FWD : ST_FFT_Y_INV) : (dir < 0 ? ST_FFT_X_FWD : ST_FFT_X_INV));
         if (dir < 0)
-            k_fft_strided<T, N, -1><<<grid, strided_threads<T, N>(), smem_s(), p.stream>>>(d, es, os, H, tw);
+            k_fft_strided<T, N, -1><<<grid, strided_threads<T, N>(), smem_s(), p.stream>>>(d, es, os, bs, H, tw);
         else
-            k_fft_strided<T, N, +1><<<grid, strided_threads<T, N>(), smem_s(), p.stream>>>(d, es, os, H, tw);
+            k_fft_strided<T, N, +1><<<grid, strided_threads<T, N>(), smem_s(), p.stream>>>(d, es, os, bs, H, tw);
     }
-    static void xgreen(const Plan& p, T* mesh, double cg) {
+    static void xgreen(const Plan& p, T* mesh, double cg, int nbox = 1) {
         C* d = reinterpret_cast<C*>(mesh);
-        dim3 grid((H + tk_cols<T, N>() - 1) / tk_cols<T, N>(), N);
+        dim3 grid((H + tk_cols<T, N>() - 1) / tk_cols<T, N>(), N * nbox);
         Timed t(p, ST_FFT_X_GREEN);
         k_fft_x_green<T, N><<<grid, strided_threads<T, N>(), smem_s(), p.stream>>>(
-            d, (long long)N * H, H, H, static_cast<const C*>(p.tw), static_cast<const T*>(p.g1d), cg, p.green_kind);
+            d, (long long)N * H, H, (long long)N * N * H, H, static_cast<const C*>(p.tw),
+            static_cast<const T*>(p.g1d), cg, p.green_kind);
     }
 };
 
@@ -304,7 +439,9 @@ template <typename T, int N> struct Launch {
         case 8: { constexpr int N_ = 8; __VA_ARGS__; } break;        \
         case 16: { constexpr int N_ = 16; __VA_ARGS__; } break;      \
         case 32: { constexpr int N_ = 32; __VA_ARGS__; } break;      \
+        case 48: { constexpr int N_ = 48; __VA_ARGS__; } break;      \
         case 64: { constexpr int N_ = 64; __VA_ARGS__; } break;      \
+        case 96: { constexpr int N_ = 96; __VA_ARGS__; } break;      \
         case 128: { constexpr int N_ = 128; __VA_ARGS__; } break;    \
         case 256: { constexpr int N_ = 256; __VA_ARGS__; } break;    \
         case 512: { constexpr int N_ = 512; __VA_ARGS__; } break;    \
@@ -313,24 +450,29 @@ template <typename T, int N> struct Launch {
     }
 
 bool fft_size_supported(int ng) {
-    return ng >= 8 && ng <= 1024 && (ng & (ng - 1)) == 0;
+    return (ng >= 8 && ng <= 1024 && (ng & (ng - 1)) == 0) || ng == 48 || ng == 96;
 }
+
+// Launcher of a mesh size: the two-pass power-of-two kernels, or the
+// generic mixed-radix ones for 48 and 96.
+template <typename T, int N>
+using LaunchFor = typename std::conditional<(N & (N - 1)) == 0, Launch<T, N>, LaunchG<T, N>>::type;
 
 int fft_prepare(const Plan& p) {
     int rc = PM_OK;
     if (p.precision == PM_FP64) {
-        PMB_FFT_DISPATCH(p.ng, rc = Launch<double, N_>::prepare());
+        PMB_FFT_DISPATCH(p.ng, rc = LaunchFor<double, N_>::prepare());
     } else {
-        PMB_FFT_DISPATCH(p.ng, rc = Launch<float, N_>::prepare());
+        PMB_FFT_DISPATCH(p.ng, rc = LaunchFor<float, N_>::prepare());
     }
     return rc;
 }
 
 template <typename T> int fft_r2c(const Plan& p, T* mesh) {
     PMB_FFT_DISPATCH(p.ng, {
-        Launch<T, N_>::z(p, mesh, true);
-        Launch<T, N_>::strided(p, mesh, 1, -1);
-        Launch<T, N_>::strided(p, mesh, 0, -1);
+        LaunchFor<T, N_>::z(p, mesh, true);
+        LaunchFor<T, N_>::strided(p, mesh, 1, -1);
+        LaunchFor<T, N_>::strided(p, mesh, 0, -1);
     });
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;
@@ -338,9 +480,9 @@ template <typename T> int fft_r2c(const Plan& p, T* mesh) {
 
 template <typename T> int fft_c2r(const Plan& p, T* mesh) {
     PMB_FFT_DISPATCH(p.ng, {
-        Launch<T, N_>::strided(p, mesh, 0, +1);
-        Launch<T, N_>::strided(p, mesh, 1, +1);
-        Launch<T, N_>::z(p, mesh, false);
+        LaunchFor<T, N_>::strided(p, mesh, 0, +1);
+        LaunchFor<T, N_>::strided(p, mesh, 1, +1);
+        LaunchFor<T, N_>::z(p, mesh, false);
     });
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;
@@ -364,11 +506,11 @@ template <typename T> int green_apply(const Plan& p, T* mesh, double c_poisson) 
 template <typename T> int poisson_fused(const Plan& p, T* mesh, double c_poisson) {
     const double cg = green_scale(p, c_poisson);
     PMB_FFT_DISPATCH(p.ng, {
-        Launch<T, N_>::z(p, mesh, true);
-        Launch<T, N_>::strided(p, mesh, 1, -1);
-        Launch<T, N_>::xgreen(p, mesh, cg);
-        Launch<T, N_>::strided(p, mesh, 1, +1);
-        Launch<T, N_>::z(p, mesh, false);
+        LaunchFor<T, N_>::z(p, mesh, true);
+        LaunchFor<T, N_>::strided(p, mesh, 1, -1);
+        LaunchFor<T, N_>::xgreen(p, mesh, cg);
+        LaunchFor<T, N_>::strided(p, mesh, 1, +1);
+        LaunchFor<T, N_>::z(p, mesh, false);
     });
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;

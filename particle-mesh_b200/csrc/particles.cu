@@ -177,13 +177,13 @@ __global__ void k_drift_f64(double* __restrict__ x, double* __restrict__ y, doub
 
 // ------------------------------------------------------ split positions
 
-__device__ __forceinline__ void split1(double v, int msk, int& cell, float& off) {
+__device__ __forceinline__ void split1(double v, int n, int& cell, float& off) {
     const double f = floor(v);
-    cell = ((int)(long long)f) & msk;
+    cell = wrap_cell((int)(long long)f, n);
     off = (float)(v - f);
     if (off >= 1.0f) {  // rounding to FP32 reached the next cell
         off = 0.0f;
-        cell = (cell + 1) & msk;
+        cell = wrap_cell(cell + 1, n);
     }
 }
 
@@ -201,14 +201,13 @@ __global__ void k_split(const double* __restrict__ x, const double* __restrict__
                         float* __restrict__ ox, float* __restrict__ oy, float* __restrict__ oz, int n,
                         int* err) {
     const double dn = (double)n;
-    const int msk = n - 1;
     for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np;
          p += (long long)gridDim.x * blockDim.x) {
         int i, j, k;
         float a, b, c;
-        split1(sanitize(x[p], dn, err), msk, i, a);
-        split1(sanitize(y[p], dn, err), msk, j, b);
-        split1(sanitize(z[p], dn, err), msk, k, c);
+        split1(sanitize(x[p], dn, err), n, i, a);
+        split1(sanitize(y[p], dn, err), n, j, b);
+        split1(sanitize(z[p], dn, err), n, k, c);
         cell[p] = pack_cell(i, j, k);
         ox[p] = a;
         oy[p] = b;
@@ -242,13 +241,13 @@ __device__ __forceinline__ void force_at(const float* __restrict__ phi, int n, i
                                          float tx, float ty, float tz, float& gx, float& gy,
                                          float& gz) {
     constexpr int LO = ORDER == 4 ? -2 : -1, W = ORDER == 4 ? 6 : 4;  // stencil offsets LO..LO+W-1
-    const unsigned msk = (unsigned)n - 1u, pz = (unsigned)n + 2u, plane = (unsigned)n * pz;
+    const unsigned pz = (unsigned)n + 2u, plane = (unsigned)n * pz;
     unsigned xo[W], yo[W], kc[W];
 #pragma unroll
     for (int d = 0; d < W; ++d) {
-        xo[d] = ((unsigned)(i + LO + d) & msk) * plane;
-        yo[d] = ((unsigned)(j + LO + d) & msk) * pz;
-        kc[d] = (unsigned)(k + LO + d) & msk;
+        xo[d] = (unsigned)wrap_cell(i + LO + d, n) * plane;
+        yo[d] = (unsigned)wrap_cell(j + LO + d, n) * pz;
+        kc[d] = (unsigned)wrap_cell(k + LO + d, n);
     }
     constexpr int C0 = -LO;  // stencil slot of offset 0
     // core rows (i+a, j+b): the whole z stencil
@@ -325,7 +324,6 @@ __global__ void k_kick_drift_f32(const float* __restrict__ phi, uint32_t* __rest
                                  float* __restrict__ ox, float* __restrict__ oy, float* __restrict__ oz,
                                  float* __restrict__ vx, float* __restrict__ vy, float* __restrict__ vz,
                                  long long np, float c_kick, double dt, int n) {
-    const int msk = n - 1;
     for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np;
          p += (long long)gridDim.x * blockDim.x) {
         int i, j, k;
@@ -340,9 +338,9 @@ __global__ void k_kick_drift_f32(const float* __restrict__ phi, uint32_t* __rest
         if (dt != 0.0) {
             int a, b, c;
             float qa, qb, qc;
-            split1((double)i + (double)tx + (double)ux * dt, msk, a, qa);
-            split1((double)j + (double)ty + (double)uy * dt, msk, b, qb);
-            split1((double)k + (double)tz + (double)uz * dt, msk, c, qc);
+            split1((double)i + (double)tx + (double)ux * dt, n, a, qa);
+            split1((double)j + (double)ty + (double)uy * dt, n, b, qb);
+            split1((double)k + (double)tz + (double)uz * dt, n, c, qc);
             cell[p] = pack_cell(a, b, c);
             ox[p] = qa;
             oy[p] = qb;

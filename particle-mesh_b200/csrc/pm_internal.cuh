@@ -47,6 +47,15 @@ template <> __device__ __forceinline__ float2 cscale<float2>(float2 a, float s) 
 }
 #endif
 
+// Periodic wrap of a cell index into [0, n) for any n (the FP32 path also
+// serves meshes of 48 and 96 cells); one compare each way in the common case.
+__host__ __device__ __forceinline__ int wrap_cell(int c, int n) {
+    if (c < 0) c += n;
+    else if (c >= n) c -= n;
+    if (c < 0 || c >= n) c = ((c % n) + n) % n;
+    return c;
+}
+
 // ------------------------------------------------------------------- errors
 enum : int { ERRBIT_RANGE = 1 };
 

@@ -34,15 +34,15 @@ __device__ __forceinline__ void unpack(uint32_t c, int& i, int& j, int& k) {
 }
 
 // Bucket of a particle: ((tx * nt + ty) * nt + tz) * 8 + class.  Cell
-// indices are wrapped by the mesh mask, so a cell >= ng (invalid input)
+// indices are wrapped by the mesh size, so a cell >= ng (invalid input)
 // lands on its periodic image rather than outside the bucket arrays.
 __device__ __forceinline__ uint32_t bucket_of(uint32_t c, int ts_log, int nt) {
     int i, j, k;
     unpack(c, i, j, k);
-    const int mk = (nt << ts_log) - 1;
-    i &= mk;
-    j &= mk;
-    k &= mk;
+    const int n = nt << ts_log;
+    if (i >= n) i %= n;
+    if (j >= n) j %= n;
+    if (k >= n) k %= n;
     const int m = (1 << ts_log) - 1;
     const uint32_t tile = ((uint32_t)(i >> ts_log) * nt + (uint32_t)(j >> ts_log)) * nt + (uint32_t)(k >> ts_log);
     const uint32_t cls = ((i & m) == m ? 1u : 0u) | ((j & m) == m ? 2u : 0u) | ((k & m) == m ? 4u : 0u);
@@ -61,10 +61,10 @@ __device__ __forceinline__ uint32_t spread3(uint32_t v) {  // 10 bits -> every t
 __device__ __forceinline__ uint32_t morton_tile(uint32_t c, int ts_log, int nt) {
     int i, j, k;
     unpack(c, i, j, k);
-    const int mk = (nt << ts_log) - 1;
-    i &= mk;
-    j &= mk;
-    k &= mk;
+    const int n = nt << ts_log;
+    if (i >= n) i %= n;
+    if (j >= n) j %= n;
+    if (k >= n) k %= n;
     return (spread3((uint32_t)(i >> ts_log)) << 2) | (spread3((uint32_t)(j >> ts_log)) << 1) |
            spread3((uint32_t)(k >> ts_log));
 }
@@ -365,7 +365,9 @@ int deposit_f32_tiles(Plan& p, const uint32_t* cell, const float* ox, const floa
 int sort_f32(Plan& p, uint32_t* cell, float* ox, float* oy, float* oz, float* vx, float* vy, float* vz, int64_t np) {
     if (np == 0) return PM_OK;
     const int tl = tile_log(p.ng), nt = p.ng >> tl;
-    const long long nb = (long long)nt * nt * nt;  // Morton keys cover [0, nt^3) for nt a power of two
+    int nt2 = 1;  // Morton keys of nt tiles per axis lie in [0, nt2^3), nt2 the next power of two
+    while (nt2 < nt) nt2 <<= 1;
+    const long long nb = (long long)nt2 * nt2 * nt2;
     int rc = tile_scratch_ensure(p, np);
     if (rc != PM_OK) return rc;
     rc = bucket_sort<true>(p, cell, np, tl, nt, nb, p.tiles);

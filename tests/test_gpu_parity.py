@@ -80,7 +80,7 @@ def test_fft_round_trip_large_f64(pmpkg, ng):
     assert float((d[:, :, :ng] / ng ** 3 - x).norm() / x.norm()) < 1e-13
 
 
-@pytest.mark.parametrize("ng", [16, 64, 1024])
+@pytest.mark.parametrize("ng", [16, 48, 64, 96, 1024])
 def test_fft_f32(pmpkg, ng):
     rng = np.random.default_rng(3)
     m = np.zeros((ng, ng, ng + 2), np.float32)
@@ -88,7 +88,7 @@ def test_fft_f32(pmpkg, ng):
     plan = pmpkg.Plan(ng, "fp32")
     d = T(m, torch.float32)
     plan.fft_r2c(d)
-    if ng <= 64:
+    if ng <= 96:
         assert rel(H(d).view(np.complex64), np.fft.rfftn(m[:, :, :ng].astype(np.float64))) < 2e-6
     plan.fft_c2r(d)
     assert rel(H(d)[:, :, :ng] / ng ** 3, m[:, :, :ng]) < 2e-6
@@ -250,7 +250,8 @@ def test_split_join(pmpkg, O):
 
 
 @pytest.mark.parametrize("ng,nrow,kind,order", [(64, 64, "discrete", 2), (64, 32, "spectral", 4),
-                                                (128, 64, "spectral", 4)])
+                                                (128, 64, "spectral", 4), (48, 48, "spectral", 4),
+                                                (96, 96, "discrete", 2)])
 def test_split_forces_within_1e4_of_fp64(pmpkg, O, ng, nrow, kind, order):
     pos, vel = O.zeldovich_ic(ng, nrow, -2.0, 0.5, seed=ng + nrow)
     mass = ng ** 3 / nrow ** 3
@@ -335,7 +336,7 @@ def test_split_step_kick_drift(pmpkg, O):
 
 # ---------------------------------------------------- initial conditions
 
-@pytest.mark.parametrize("ng,nrow,ns,rms", [(16, 16, -2.0, 0.3), (64, 32, -1.5, 1.0)])
+@pytest.mark.parametrize("ng,nrow,ns,rms", [(16, 16, -2.0, 0.3), (64, 32, -1.5, 1.0), (48, 48, -2.5, 0.7)])
 def test_zeldovich_ic_matches_oracle(pmpkg, O, ng, nrow, ns, rms):
     pos, vel = pmpkg.zeldovich_ic(ng, nrow, ns, rms, seed=42, device=DEV)
     opos, ovel = O.zeldovich_ic(ng, nrow, ns, rms, seed=42)
@@ -383,6 +384,9 @@ def test_errors_are_reported(pmpkg):
     with pytest.raises(pmpkg.PMError) as e:
         pmpkg.Plan(12, "fp64")
     assert e.value.code == 2  # PM_ERR_SIZE
+    with pytest.raises(pmpkg.PMError) as e:
+        pmpkg.Plan(48, "fp64")  # mixed-radix sizes are FP32 only
+    assert e.value.code == 2
     p32 = pmpkg.Plan(16, "fp32")
     with pytest.raises(pmpkg.PMError):
         p32.deposit(x, y, z, 1.0)  # FP64 entry point on an FP32 plan
