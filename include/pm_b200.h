@@ -245,6 +245,37 @@ int pm_step_f32(pm_plan* plan, uint32_t* cell, float* ox, float* oy, float* oz, 
 int pm_deposit_f32_noalloc(int ng, const uint32_t* cell, const float* ox, const float* oy,
                            const float* oz, int64_t np, float mass, float* mesh, void* stream);
 
+/* ------------------------------------------ batched ensemble (FP32, new)
+ * Independent periodic boxes of mixed mesh sizes advanced together; no
+ * counterpart in the reference.  Particles of all boxes share the seven split
+ * arrays, box b owning np[b] consecutive entries in box order (positions in
+ * its own cell units).  Boxes of one mesh size form a class: every kernel of
+ * the step covers the whole class in one launch, classes run concurrently on
+ * their own streams.  mass[b] is box b's particle mass (host array, copied).
+ * autotune != 0 times the strided-FFT column-tile widths of each class with
+ * ng <= 128 at creation and keeps the fastest; tune_cache (may be NULL) is a
+ * text file of earlier choices, read first and rewritten when new ones were
+ * measured.  stream NULL: the ensemble uses its own stream (pm_ensemble_sync
+ * waits for it).  Spectral / discrete Green and gradient order as for plans. */
+typedef struct pm_ensemble pm_ensemble;
+int pm_ensemble_create(int nbox, const int* ng, const int64_t* np, const float* mass, int green_kind,
+                       int grad_order, int autotune, const char* tune_cache, void* stream,
+                       pm_ensemble** ensemble);
+int pm_ensemble_destroy(pm_ensemble* ensemble);
+int pm_ensemble_sync(pm_ensemble* ensemble);
+/* One step of every box: deposit, Poisson, kick by c_kick, drift by dt. */
+int pm_ensemble_step_f32(pm_ensemble* ensemble, uint32_t* cell, float* ox, float* oy, float* oz,
+                         float* vx, float* vy, float* vz, double c_poisson, double c_kick, double dt);
+/* `steps` leapfrog KDK steps of every box (steps + 1 force evaluations, half
+ * kicks merged), as one CUDA graph: captured on the first call and replayed
+ * while the arrays, c_poisson, dt and steps stay the same. */
+int pm_ensemble_run_f32(pm_ensemble* ensemble, uint32_t* cell, float* ox, float* oy, float* oz,
+                        float* vx, float* vy, float* vz, double c_poisson, double dt, int steps);
+/* Classes (mesh size, boxes, chosen tile width), device bytes held and the
+ * node count of the last captured graph; any output may be NULL. */
+int pm_ensemble_info(const pm_ensemble* ensemble, int* nclasses, int* class_ng, int* class_nbox,
+                     int* class_tk, size_t* device_bytes, size_t* graph_nodes);
+
 /* ---------------------------------------------- initial conditions (new)
  * Zel'dovich particles on an nrow^3 lattice q = (i + 1/2) ng/nrow from a
  * Gaussian random field with P(k) ~ k^n_s, scaled to an rms 3D displacement

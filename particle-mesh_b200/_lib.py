@@ -53,6 +53,12 @@ SIGNATURES = {
     "pm_kick_drift_f32": [_V, _V, _V, _V, _V, _V, _V, _V, _V, _L, _D, _D],
     "pm_step_f32": [_V, _V, _V, _V, _V, _V, _V, _V, _L, _F, _D, _D, _D],
     "pm_deposit_f32_noalloc": [_I, _V, _V, _V, _V, _L, _F, _V, _V],
+    "pm_ensemble_create": [_I, _V, _V, _V, _I, _I, _I, ctypes.c_char_p, _V, ctypes.POINTER(_V)],
+    "pm_ensemble_destroy": [_V],
+    "pm_ensemble_sync": [_V],
+    "pm_ensemble_step_f32": [_V, _V, _V, _V, _V, _V, _V, _V, _D, _D, _D],
+    "pm_ensemble_run_f32": [_V, _V, _V, _V, _V, _V, _V, _V, _D, _D, _I],
+    "pm_ensemble_info": [_V, _V, _V, _V, _V, _V, _V],
     "pm_ic_zeldovich": [_I, _I, _D, _D, _U64, _D, _V, _V, _V, _V, _V, _V, _V],
 }
 

@@ -1,0 +1,365 @@
+// Batched ensemble of independent periodic boxes (FP32 split positions).
+//
+// No counterpart in the reference, which advances one box.  Boxes are grouped
+// into size classes (same ng); each class is one batch: its meshes lie back to
+// back and every kernel of the step (binning, tile deposit, the five FFT
+// passes with the Green multiply, gather + kick + drift) covers all boxes of
+// the class in one launch.  Classes run on their own streams; a whole KDK run
+// is captured once into a CUDA graph with one branch per class and replayed.
+// The column-tile width of the strided FFT passes is chosen per class by
+// timing the candidates (autotune), optionally cached in a text file keyed by
+// GPU name and mesh size (the analogue of the reference's FFTW wisdom file,
+// src/fft/fftw/fft.cpp:28-49).
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "pm_internal.cuh"
+
+namespace pmb {
+
+struct EnsembleClass {
+    int ng = 0;
+    std::vector<int> boxes;
+    pm_plan* plan = nullptr;
+    float* mesh = nullptr;
+    long long* d_pbeg = nullptr;
+    long long* d_pend = nullptr;
+    float* d_mass = nullptr;
+    int64_t np = 0;
+    cudaEvent_t done = nullptr;
+};
+
+}  // namespace pmb
+
+struct pm_ensemble {
+    bool own_stream = false;
+    int nbox = 0;
+    int64_t np_total = 0;
+    std::vector<pmb::EnsembleClass> classes;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t fork = nullptr;
+    size_t bytes = 0;
+    // cached graph of a KDK run and the arguments it was captured with
+    cudaGraphExec_t exec = nullptr;
+    std::vector<const void*> key_ptrs;
+    double key_cp = 0, key_dt = 0;
+    int key_steps = -1;
+    size_t graph_nodes = 0;
+};
+
+namespace pmb {
+
+namespace {
+
+void release_ensemble(pm_ensemble* e) {
+    if (e->exec) cudaGraphExecDestroy(e->exec);
+    for (auto& c : e->classes) {
+        if (c.plan) {
+            cudaStream_t s = c.plan->p.stream;
+            pm_plan_destroy(c.plan);
+            if (s) cudaStreamDestroy(s);
+        }
+        if (c.mesh) cudaFree(c.mesh);
+        if (c.d_pbeg) cudaFree(c.d_pbeg);
+        if (c.d_pend) cudaFree(c.d_pend);
+        if (c.d_mass) cudaFree(c.d_mass);
+        if (c.done) cudaEventDestroy(c.done);
+    }
+    if (e->fork) cudaEventDestroy(e->fork);
+    if (e->own_stream && e->stream) cudaStreamDestroy(e->stream);
+    delete e;
+}
+
+std::string gpu_name() {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return "unknown";
+    std::string s = prop.name;
+    for (char& ch : s)
+        if (ch == ' ') ch = '_';
+    return s;
+}
+
+// Tune cache lines: "<gpu> <ng> <green> <order> <tk>".
+std::map<std::string, int> read_cache(const char* path) {
+    std::map<std::string, int> m;
+    if (!path) return m;
+    FILE* f = std::fopen(path, "r");
+    if (!f) return m;
+    char gpu[256];
+    int ng, gk, go, tk;
+    while (std::fscanf(f, "%255s %d %d %d %d", gpu, &ng, &gk, &go, &tk) == 5)
+        m[std::string(gpu) + " " + std::to_string(ng) + " " + std::to_string(gk) + " " + std::to_string(go)] = tk;
+    std::fclose(f);
+    return m;
+}
+
+void write_cache(const char* path, const std::map<std::string, int>& m) {
+    if (!path) return;
+    FILE* f = std::fopen(path, "w");
+    if (!f) return;
+    for (auto& kv : m) std::fprintf(f, "%s %d\n", kv.first.c_str(), kv.second);
+    std::fclose(f);
+}
+
+// Times the class's batched Poisson solve for each column-tile width and
+// keeps the fastest.
+int autotune_class(EnsembleClass& c, std::map<std::string, int>& cache, bool measure) {
+    Plan& p = c.plan->p;
+    const std::string key = gpu_name() + " " + std::to_string(c.ng) + " " + std::to_string(p.green_kind) + " " +
+                            std::to_string(p.grad_order);
+    auto it = cache.find(key);
+    if (it != cache.end() && tk_variant_supported(c.ng, PM_FP32, it->second)) {
+        p.tk = it->second;
+        return PM_OK;
+    }
+    if (!measure || c.ng > 128) return PM_OK;
+    const int nbox = (int)c.boxes.size();
+    PMB_CUDA_CHECK(cudaMemsetAsync(c.mesh, 0, mesh_elems(c.ng) * nbox * sizeof(float), p.stream));
+    cudaEvent_t a, b;
+    PMB_CUDA_CHECK(cudaEventCreate(&a));
+    PMB_CUDA_CHECK(cudaEventCreate(&b));
+    float best = 1e30f;
+    int best_tk = 0;
+    for (int tk : {0, 8, 16, 32}) {
+        if (!tk_variant_supported(c.ng, PM_FP32, tk)) continue;
+        p.tk = tk;
+        int rc = PM_OK;
+        for (int r = 0; r < 2 && rc == PM_OK; ++r) rc = poisson_fused<float>(p, c.mesh, 1.0, nbox);
+        cudaEventRecord(a, p.stream);
+        for (int r = 0; r < 5 && rc == PM_OK; ++r) rc = poisson_fused<float>(p, c.mesh, 1.0, nbox);
+        cudaEventRecord(b, p.stream);
+        if (rc != PM_OK) {
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+            return rc;
+        }
+        cudaEventSynchronize(b);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        if (ms < best) {
+            best = ms;
+            best_tk = tk;
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    p.tk = best_tk;
+    cache[key] = best_tk;
+    return PM_OK;
+}
+
+int enqueue_step(pm_ensemble* e, EnsembleClass& c, uint32_t* cell, float* ox, float* oy, float* oz, float* vx,
+                 float* vy, float* vz, double c_poisson, double c_kick, double dt) {
+    Plan& p = c.plan->p;
+    const int nbox = (int)c.boxes.size();
+    int rc = deposit_f32_tiles_batch(p, cell, ox, oy, oz, c.d_pbeg, c.d_pend, nbox, c.np, c.d_mass, c.mesh);
+    if (rc == PM_OK) rc = poisson_fused<float>(p, c.mesh, c_poisson, nbox);
+    if (rc == PM_OK)
+        rc = kick_drift_f32_batch(p, c.mesh, cell, ox, oy, oz, vx, vy, vz, c.d_pbeg, c.d_pend, nbox, c.np, c_kick,
+                                  dt);
+    (void)e;
+    return rc;
+}
+
+// Fork from the ensemble stream, run `body` on each class stream, join.
+template <typename F>
+int fork_join(pm_ensemble* e, F body) {
+    PMB_CUDA_CHECK(cudaEventRecord(e->fork, e->stream));
+    for (auto& c : e->classes) {
+        PMB_CUDA_CHECK(cudaStreamWaitEvent(c.plan->p.stream, e->fork, 0));
+        const int rc = body(c);
+        if (rc != PM_OK) return rc;
+        PMB_CUDA_CHECK(cudaEventRecord(c.done, c.plan->p.stream));
+        PMB_CUDA_CHECK(cudaStreamWaitEvent(e->stream, c.done, 0));
+    }
+    return PM_OK;
+}
+
+}  // namespace
+}  // namespace pmb
+
+using namespace pmb;
+
+extern "C" {
+
+int pm_ensemble_create(int nbox, const int* ng, const int64_t* np, const float* mass, int green_kind,
+                       int grad_order, int autotune, const char* tune_cache, void* stream, pm_ensemble** out) {
+    if (!out) return fail(PM_ERR_ARG, "output pointer is NULL");
+    *out = nullptr;
+    if (nbox <= 0 || !ng || !np || !mass) return fail(PM_ERR_ARG, "need nbox > 0 and ng, np, mass arrays");
+    for (int b = 0; b < nbox; ++b) {
+        if (!fft_size_supported(ng[b])) return fail(PM_ERR_SIZE, "ensemble box mesh size not supported");
+        if (np[b] < 0) return fail(PM_ERR_ARG, "negative particle count");
+    }
+    pm_ensemble* e = new (std::nothrow) pm_ensemble();
+    if (!e) return fail(PM_ERR_NOMEM, "host allocation failed");
+    e->nbox = nbox;
+    e->stream = static_cast<cudaStream_t>(stream);
+    if (!e->stream) {  // graphs cannot be captured on the legacy default stream
+        if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            delete e;
+            return fail(PM_ERR_CUDA, "stream creation failed");
+        }
+        e->own_stream = true;
+    }
+    std::vector<int64_t> off(nbox + 1, 0);
+    for (int b = 0; b < nbox; ++b) off[b + 1] = off[b] + np[b];
+    e->np_total = off[nbox];
+    std::map<int, std::vector<int>> groups;
+    for (int b = 0; b < nbox; ++b) groups[ng[b]].push_back(b);
+    int rc = PM_OK;
+    if (cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) != cudaSuccess)
+        rc = fail(PM_ERR_CUDA, "event creation failed");
+    for (auto& g : groups) {
+        if (rc != PM_OK) break;
+        EnsembleClass c;
+        c.ng = g.first;
+        c.boxes = g.second;
+        cudaStream_t cs = nullptr;
+        if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) {
+            rc = fail(PM_ERR_CUDA, "stream creation failed");
+            break;
+        }
+        rc = pm_plan_create(c.ng, PM_FP32, green_kind, grad_order, cs, &c.plan);
+        if (rc != PM_OK) {
+            cudaStreamDestroy(cs);
+            break;
+        }
+        const size_t nb = c.boxes.size();
+        std::vector<long long> pb(nb), pe(nb);
+        std::vector<float> m(nb);
+        for (size_t i = 0; i < nb; ++i) {
+            pb[i] = off[c.boxes[i]];
+            pe[i] = off[c.boxes[i] + 1];
+            m[i] = mass[c.boxes[i]];
+            c.np += np[c.boxes[i]];
+        }
+        const size_t mb = mesh_elems(c.ng) * nb * sizeof(float);
+        if (cudaMalloc(&c.mesh, mb) != cudaSuccess || cudaMalloc(&c.d_pbeg, nb * 8) != cudaSuccess ||
+            cudaMalloc(&c.d_pend, nb * 8) != cudaSuccess || cudaMalloc(&c.d_mass, nb * 4) != cudaSuccess ||
+            cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            e->classes.push_back(c);
+            rc = fail(PM_ERR_NOMEM, "ensemble allocation failed");
+            break;
+        }
+        cudaMemcpy(c.d_pbeg, pb.data(), nb * 8, cudaMemcpyHostToDevice);
+        cudaMemcpy(c.d_pend, pe.data(), nb * 8, cudaMemcpyHostToDevice);
+        cudaMemcpy(c.d_mass, m.data(), nb * 4, cudaMemcpyHostToDevice);
+        // scratch for the batched binning, allocated now so that steps (and
+        // graph captures) never allocate
+        rc = tile_scratch_ensure(c.plan->p, c.np > 0 ? c.np : 1, (int)nb);
+        e->bytes += mb + nb * 20 + c.plan->p.bytes;
+        e->classes.push_back(c);
+    }
+    if (rc == PM_OK) {
+        auto cache = read_cache(tune_cache);
+        const size_t before = cache.size();
+        for (auto& c : e->classes) {
+            rc = autotune_class(c, cache, autotune != 0);
+            if (rc != PM_OK) break;
+        }
+        if (rc == PM_OK && cache.size() != before) write_cache(tune_cache, cache);
+        if (rc == PM_OK && cudaDeviceSynchronize() != cudaSuccess) rc = fail(PM_ERR_CUDA, "autotune failed");
+    }
+    if (rc != PM_OK) {
+        release_ensemble(e);
+        return rc;
+    }
+    *out = e;
+    return PM_OK;
+}
+
+int pm_ensemble_destroy(pm_ensemble* e) {
+    if (!e) return PM_OK;
+    cudaStreamSynchronize(e->stream);
+    for (auto& c : e->classes)
+        if (c.plan) cudaStreamSynchronize(c.plan->p.stream);
+    release_ensemble(e);
+    return PM_OK;
+}
+
+int pm_ensemble_sync(pm_ensemble* e) {
+    if (!e) return fail(PM_ERR_ARG, "ensemble is NULL");
+    PMB_CUDA_CHECK(cudaStreamSynchronize(e->stream));
+    return PM_OK;
+}
+
+int pm_ensemble_info(const pm_ensemble* e, int* nclasses, int* class_ng, int* class_nbox, int* class_tk,
+                     size_t* device_bytes, size_t* graph_nodes) {
+    if (!e) return fail(PM_ERR_ARG, "ensemble is NULL");
+    if (nclasses) *nclasses = (int)e->classes.size();
+    for (size_t i = 0; i < e->classes.size(); ++i) {
+        if (class_ng) class_ng[i] = e->classes[i].ng;
+        if (class_nbox) class_nbox[i] = (int)e->classes[i].boxes.size();
+        if (class_tk) class_tk[i] = e->classes[i].plan->p.tk;
+    }
+    if (device_bytes) *device_bytes = e->bytes;
+    if (graph_nodes) *graph_nodes = e->graph_nodes;
+    return PM_OK;
+}
+
+int pm_ensemble_step_f32(pm_ensemble* e, uint32_t* cell, float* ox, float* oy, float* oz, float* vx, float* vy,
+                         float* vz, double c_poisson, double c_kick, double dt) {
+    if (!e) return fail(PM_ERR_ARG, "ensemble is NULL");
+    if (e->np_total > 0 && (!cell || !ox || !oy || !oz || !vx || !vy || !vz))
+        return fail(PM_ERR_ARG, "NULL particle array");
+    return fork_join(e, [&](EnsembleClass& c) {
+        return enqueue_step(e, c, cell, ox, oy, oz, vx, vy, vz, c_poisson, c_kick, dt);
+    });
+}
+
+int pm_ensemble_run_f32(pm_ensemble* e, uint32_t* cell, float* ox, float* oy, float* oz, float* vx, float* vy,
+                        float* vz, double c_poisson, double dt, int steps) {
+    if (!e) return fail(PM_ERR_ARG, "ensemble is NULL");
+    if (steps < 0) return fail(PM_ERR_ARG, "negative step count");
+    if (e->np_total > 0 && (!cell || !ox || !oy || !oz || !vx || !vy || !vz))
+        return fail(PM_ERR_ARG, "NULL particle array");
+    std::vector<const void*> ptrs = {cell, ox, oy, oz, vx, vy, vz};
+    const bool hit = e->exec && e->key_ptrs == ptrs && e->key_cp == c_poisson && e->key_dt == dt &&
+                     e->key_steps == steps;
+    if (!hit) {
+        if (e->exec) cudaGraphExecDestroy(e->exec);
+        e->exec = nullptr;
+        for (auto& c : e->classes) c.plan->p.timers->on = false;  // no timing events inside the graph
+        PMB_CUDA_CHECK(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+        // KDK with merged half kicks: steps + 1 force evaluations
+        int rc = fork_join(e, [&](EnsembleClass& c) {
+            for (int s = 0; s <= steps; ++s) {
+                const double ck = (s == 0 || s == steps) ? 0.5 * dt : dt, dd = s < steps ? dt : 0.0;
+                const int r = enqueue_step(e, c, cell, ox, oy, oz, vx, vy, vz, c_poisson, ck, dd);
+                if (r != PM_OK) return r;
+            }
+            return PM_OK;
+        });
+        cudaGraph_t graph = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(e->stream, &graph);
+        if (rc != PM_OK) {
+            if (graph) cudaGraphDestroy(graph);
+            return rc;
+        }
+        if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture");
+        cudaGraphGetNodes(graph, nullptr, &e->graph_nodes);
+        const cudaError_t ie = cudaGraphInstantiate(&e->exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ie != cudaSuccess) {
+            e->exec = nullptr;
+            return cuda_fail(ie, "cudaGraphInstantiate");
+        }
+        e->key_ptrs = ptrs;
+        e->key_cp = c_poisson;
+        e->key_dt = dt;
+        e->key_steps = steps;
+    }
+    PMB_CUDA_CHECK(cudaGraphLaunch(e->exec, e->stream));
+    return PM_OK;
+}
+
+}  // extern "C"

@@ -152,15 +152,15 @@ k_fft_z_c2r(T* __restrict__ mesh, long long nrows, const typename Cx<T>::t* __re
 // ------------------------------------------------------ strided C2C passes
 // Lines of N complex at element stride `es`; block (bx, by) owns columns
 // [bx*TK, bx*TK+TK) of plane `by` (plane base = by * os).
-template <typename T, int N> constexpr int strided_threads() { return tk_cols<T, N>() * threads_per_line<N>(); }
-template <typename T, int N> constexpr int strided_smem_elems() { return (N + N / Radix<N>::R1) * tk_cols<T, N>(); }
+template <int N, int TK> constexpr int strided_threads() { return TK * threads_per_line<N>(); }
+template <int N, int TK> constexpr int strided_smem_elems() { return (N + N / Radix<N>::R1) * TK; }
 
-template <typename T, int N, int DIR>
-__global__ void __launch_bounds__(strided_threads<T, N>(), 2)
+template <typename T, int N, int DIR, int TK>
+__global__ void __launch_bounds__(strided_threads<N, TK>(), 2)
 k_fft_strided(typename Cx<T>::t* __restrict__ data, long long es, long long os, long long bs, int ncols,
               const typename Cx<T>::t* __restrict__ tw) {
     using C = typename Cx<T>::t;
-    constexpr int R1 = Radix<N>::R1, R2 = Radix<N>::R2, TK = tk_cols<T, N>();
+    constexpr int R1 = Radix<N>::R1, R2 = Radix<N>::R2;
     extern __shared__ __align__(16) unsigned char smraw[];
     C* S = reinterpret_cast<C*>(smraw);
     const int tx = threadIdx.x % TK, ty = threadIdx.x / TK;
@@ -206,12 +206,12 @@ __device__ __forceinline__ T green_value(int kx, int ky, int kz, int kind, doubl
 
 // Fused x pass of the Poisson solve: forward FFT along x, multiply by G,
 // inverse FFT along x, for TK kz columns of one ky plane.
-template <typename T, int N>
-__global__ void __launch_bounds__(strided_threads<T, N>(), 2)
+template <typename T, int N, int TK>
+__global__ void __launch_bounds__(strided_threads<N, TK>(), 2)
 k_fft_x_green(typename Cx<T>::t* __restrict__ data, long long es, long long os, long long bs, int ncols,
               const typename Cx<T>::t* __restrict__ tw, const T* __restrict__ g1d, double cg, int kind) {
     using C = typename Cx<T>::t;
-    constexpr int R1 = Radix<N>::R1, R2 = Radix<N>::R2, TK = tk_cols<T, N>();
+    constexpr int R1 = Radix<N>::R1, R2 = Radix<N>::R2;
     extern __shared__ __align__(16) unsigned char smraw[];
     C* S = reinterpret_cast<C*>(smraw);
     const int tx = threadIdx.x % TK, ty = threadIdx.x / TK;
@@ -318,12 +318,12 @@ __global__ void __launch_bounds__(256) k_fftg_z_c2r(T* __restrict__ mesh, long l
     }
 }
 
-template <typename T, int N, int DIR, bool GREEN>
-__global__ void __launch_bounds__(kGTK * GRadix<N>::NT)
+template <typename T, int N, int DIR, bool GREEN, int TK>
+__global__ void __launch_bounds__(TK * GRadix<N>::NT)
 k_fftg_strided(typename Cx<T>::t* __restrict__ data, long long es, long long os, long long bs, int ncols,
                const typename Cx<T>::t* __restrict__ tw, const T* __restrict__ g1d, double cg, int kind) {
     using C = typename Cx<T>::t;
-    constexpr int NT = GRadix<N>::NT, TK = kGTK;
+    constexpr int NT = GRadix<N>::NT;
     extern __shared__ __align__(16) unsigned char smraw[];
     C* A = reinterpret_cast<C*>(smraw);
     C* B = A + N * TK;
@@ -346,11 +346,11 @@ k_fftg_strided(typename Cx<T>::t* __restrict__ data, long long es, long long os,
         for (int e = ty; e < N; e += NT) base[e * es] = r[ix(e)];
 }
 
-template <typename T, int N> struct LaunchG {
+template <typename T, int N, int TK = kGTK> struct LaunchG {
     using C = typename Cx<T>::t;
     static constexpr int H = N / 2 + 1;
     static size_t smem_z() { return (size_t)g_z_rows<N>() * 2 * (N / 2 + 1) * sizeof(C); }
-    static size_t smem_s() { return (size_t)2 * N * kGTK * sizeof(C); }
+    static size_t smem_s() { return (size_t)2 * N * TK * sizeof(C); }
     static int prepare() { return PM_OK; }
     static void z(const Plan& p, T* mesh, bool forward, int nbox = 1) {
         const long long rows = (long long)nbox * N * N;
@@ -365,38 +365,38 @@ template <typename T, int N> struct LaunchG {
     static void strided(const Plan& p, T* mesh, int axis, int dir, int nbox = 1) {
         C* d = reinterpret_cast<C*>(mesh);
         const long long es = axis == 1 ? H : (long long)N * H, os = axis == 1 ? (long long)N * H : H;
-        dim3 grid((H + kGTK - 1) / kGTK, N * nbox);
+        dim3 grid((H + TK - 1) / TK, N * nbox);
         const C* tw = static_cast<const C*>(p.tw);
         const T* g = static_cast<const T*>(p.g1d);
         Timed t(p, axis == 1 ? (dir < 0 ? ST_FFT_Y_FWD : ST_FFT_Y_INV) : (dir < 0 ? ST_FFT_X_FWD : ST_FFT_X_INV));
         const long long bs = (long long)N * N * H;
         if (dir < 0)
-            k_fftg_strided<T, N, -1, false><<<grid, kGTK * GRadix<N>::NT, smem_s(), p.stream>>>(d, es, os, bs, H, tw, g, 0.0, 0);
+            k_fftg_strided<T, N, -1, false, TK><<<grid, TK * GRadix<N>::NT, smem_s(), p.stream>>>(d, es, os, bs, H, tw, g, 0.0, 0);
         else
-            k_fftg_strided<T, N, +1, false><<<grid, kGTK * GRadix<N>::NT, smem_s(), p.stream>>>(d, es, os, bs, H, tw, g, 0.0, 0);
+            k_fftg_strided<T, N, +1, false, TK><<<grid, TK * GRadix<N>::NT, smem_s(), p.stream>>>(d, es, os, bs, H, tw, g, 0.0, 0);
     }
     static void xgreen(const Plan& p, T* mesh, double cg, int nbox = 1) {
         C* d = reinterpret_cast<C*>(mesh);
-        dim3 grid((H + kGTK - 1) / kGTK, N * nbox);
+        dim3 grid((H + TK - 1) / TK, N * nbox);
         Timed t(p, ST_FFT_X_GREEN);
-        k_fftg_strided<T, N, -1, true><<<grid, kGTK * GRadix<N>::NT, smem_s(), p.stream>>>(
+        k_fftg_strided<T, N, -1, true, TK><<<grid, TK * GRadix<N>::NT, smem_s(), p.stream>>>(
             d, (long long)N * H, H, (long long)N * N * H, H, static_cast<const C*>(p.tw), static_cast<const T*>(p.g1d),
             cg, p.green_kind);
     }
 };
 
 // ------------------------------------------------------------- launchers
-template <typename T, int N> struct Launch {
+template <typename T, int N, int TK = tk_cols<T, N>()> struct Launch {
     using C = typename Cx<T>::t;
     static constexpr int H = N / 2 + 1;
     static size_t smem_z() { return (size_t)z_rows_per_block<T, N>() * z_row_stride<N>() * sizeof(C); }
-    static size_t smem_s() { return (size_t)strided_smem_elems<T, N>() * sizeof(C); }
+    static size_t smem_s() { return (size_t)strided_smem_elems<N, TK>() * sizeof(C); }
     static int prepare() {
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_z_r2c<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_z()));
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_z_c2r<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_z()));
-        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
-        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, +1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
-        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_x_green<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
+        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, -1, TK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
+        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, +1, TK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
+        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_x_green<T, N, TK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         return PM_OK;
     }
     static void z(const Plan& p, T* mesh, bool forward, int nbox = 1) {
@@ -416,19 +416,19 @@ template <typename T, int N> struct Launch {
         C* d = reinterpret_cast<C*>(mesh);
         const long long es = axis == 1 ? H : (long long)N * H, os = axis == 1 ? (long long)N * H : H;
         const long long bs = (long long)N * N * H;
-        dim3 grid((H + tk_cols<T, N>() - 1) / tk_cols<T, N>(), N * nbox);
+        dim3 grid((H + TK - 1) / TK, N * nbox);
         const C* tw = static_cast<const C*>(p.tw);
         Timed t(p, axis == 1 ? (dir < 0 ? ST_FFT_Y_FWD : ST_FFT_Y_INV) : (dir < 0 ? ST_FFT_X_FWD : ST_FFT_X_INV));
         if (dir < 0)
-            k_fft_strided<T, N, -1><<<grid, strided_threads<T, N>(), smem_s(), p.stream>>>(d, es, os, bs, H, tw);
+            k_fft_strided<T, N, -1, TK><<<grid, strided_threads<N, TK>(), smem_s(), p.stream>>>(d, es, os, bs, H, tw);
         else
-            k_fft_strided<T, N, +1><<<grid, strided_threads<T, N>(), smem_s(), p.stream>>>(d, es, os, bs, H, tw);
+            k_fft_strided<T, N, +1, TK><<<grid, strided_threads<N, TK>(), smem_s(), p.stream>>>(d, es, os, bs, H, tw);
     }
     static void xgreen(const Plan& p, T* mesh, double cg, int nbox = 1) {
         C* d = reinterpret_cast<C*>(mesh);
-        dim3 grid((H + tk_cols<T, N>() - 1) / tk_cols<T, N>(), N * nbox);
+        dim3 grid((H + TK - 1) / TK, N * nbox);
         Timed t(p, ST_FFT_X_GREEN);
-        k_fft_x_green<T, N><<<grid, strided_threads<T, N>(), smem_s(), p.stream>>>(
+        k_fft_x_green<T, N, TK><<<grid, strided_threads<N, TK>(), smem_s(), p.stream>>>(
             d, (long long)N * H, H, (long long)N * N * H, H, static_cast<const C*>(p.tw),
             static_cast<const T*>(p.g1d), cg, p.green_kind);
     }
@@ -455,34 +455,60 @@ bool fft_size_supported(int ng) {
 
 // Launcher of a mesh size: the two-pass power-of-two kernels, or the
 // generic mixed-radix ones for 48 and 96.
-template <typename T, int N>
-using LaunchFor = typename std::conditional<(N & (N - 1)) == 0, Launch<T, N>, LaunchG<T, N>>::type;
+template <typename T, int N, int TK = 0>
+using LaunchFor = typename std::conditional<
+    (N & (N - 1)) == 0, Launch<T, N, TK == 0 ? tk_cols<T, N>() : TK>, LaunchG<T, N, TK == 0 ? kGTK : TK>>::type;
+
+// Column-tile widths the autotuner may pick for small FP32 meshes (ng <= 128);
+// Plan::tk == 0 keeps the default width.
+bool tk_variant_supported(int ng, int precision, int tk) {
+    return tk == 0 || (precision == PM_FP32 && ng <= 128 && (tk == 8 || tk == 16 || tk == 32));
+}
+
+// Runs BODY with the launcher L_ of the plan's mesh size and tile width.
+#define PMB_LAUNCH(P, T_, ...)                                                                         \
+    PMB_FFT_DISPATCH((P).ng, {                                                                         \
+        if constexpr (sizeof(T_) == 4 && N_ <= 128) {                                                  \
+            if ((P).tk == 8) { using L_ = LaunchFor<T_, N_, 8>; __VA_ARGS__; break; }                  \
+            if ((P).tk == 16) { using L_ = LaunchFor<T_, N_, 16>; __VA_ARGS__; break; }                \
+            if ((P).tk == 32) { using L_ = LaunchFor<T_, N_, 32>; __VA_ARGS__; break; }                \
+        }                                                                                              \
+        using L_ = LaunchFor<T_, N_>;                                                                  \
+        __VA_ARGS__;                                                                                   \
+    })
 
 int fft_prepare(const Plan& p) {
     int rc = PM_OK;
     if (p.precision == PM_FP64) {
         PMB_FFT_DISPATCH(p.ng, rc = LaunchFor<double, N_>::prepare());
     } else {
-        PMB_FFT_DISPATCH(p.ng, rc = LaunchFor<float, N_>::prepare());
+        PMB_FFT_DISPATCH(p.ng, {
+            rc = LaunchFor<float, N_>::prepare();
+            if constexpr (N_ <= 128) {
+                if (rc == PM_OK) rc = LaunchFor<float, N_, 8>::prepare();
+                if (rc == PM_OK) rc = LaunchFor<float, N_, 16>::prepare();
+                if (rc == PM_OK) rc = LaunchFor<float, N_, 32>::prepare();
+            }
+        });
     }
     return rc;
 }
 
-template <typename T> int fft_r2c(const Plan& p, T* mesh) {
-    PMB_FFT_DISPATCH(p.ng, {
-        LaunchFor<T, N_>::z(p, mesh, true);
-        LaunchFor<T, N_>::strided(p, mesh, 1, -1);
-        LaunchFor<T, N_>::strided(p, mesh, 0, -1);
+template <typename T> int fft_r2c(const Plan& p, T* mesh, int nbox) {
+    PMB_LAUNCH(p, T, {
+        L_::z(p, mesh, true, nbox);
+        L_::strided(p, mesh, 1, -1, nbox);
+        L_::strided(p, mesh, 0, -1, nbox);
     });
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;
 }
 
-template <typename T> int fft_c2r(const Plan& p, T* mesh) {
-    PMB_FFT_DISPATCH(p.ng, {
-        LaunchFor<T, N_>::strided(p, mesh, 0, +1);
-        LaunchFor<T, N_>::strided(p, mesh, 1, +1);
-        LaunchFor<T, N_>::z(p, mesh, false);
+template <typename T> int fft_c2r(const Plan& p, T* mesh, int nbox) {
+    PMB_LAUNCH(p, T, {
+        L_::strided(p, mesh, 0, +1, nbox);
+        L_::strided(p, mesh, 1, +1, nbox);
+        L_::z(p, mesh, false, nbox);
     });
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;
@@ -503,26 +529,26 @@ template <typename T> int green_apply(const Plan& p, T* mesh, double c_poisson) 
     return PM_OK;
 }
 
-template <typename T> int poisson_fused(const Plan& p, T* mesh, double c_poisson) {
+template <typename T> int poisson_fused(const Plan& p, T* mesh, double c_poisson, int nbox) {
     const double cg = green_scale(p, c_poisson);
-    PMB_FFT_DISPATCH(p.ng, {
-        LaunchFor<T, N_>::z(p, mesh, true);
-        LaunchFor<T, N_>::strided(p, mesh, 1, -1);
-        LaunchFor<T, N_>::xgreen(p, mesh, cg);
-        LaunchFor<T, N_>::strided(p, mesh, 1, +1);
-        LaunchFor<T, N_>::z(p, mesh, false);
+    PMB_LAUNCH(p, T, {
+        L_::z(p, mesh, true, nbox);
+        L_::strided(p, mesh, 1, -1, nbox);
+        L_::xgreen(p, mesh, cg, nbox);
+        L_::strided(p, mesh, 1, +1, nbox);
+        L_::z(p, mesh, false, nbox);
     });
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;
 }
 
-template int fft_r2c<float>(const Plan&, float*);
-template int fft_r2c<double>(const Plan&, double*);
-template int fft_c2r<float>(const Plan&, float*);
-template int fft_c2r<double>(const Plan&, double*);
+template int fft_r2c<float>(const Plan&, float*, int);
+template int fft_r2c<double>(const Plan&, double*, int);
+template int fft_c2r<float>(const Plan&, float*, int);
+template int fft_c2r<double>(const Plan&, double*, int);
 template int green_apply<float>(const Plan&, float*, double);
 template int green_apply<double>(const Plan&, double*, double);
-template int poisson_fused<float>(const Plan&, float*, double);
-template int poisson_fused<double>(const Plan&, double*, double);
+template int poisson_fused<float>(const Plan&, float*, double, int);
+template int poisson_fused<double>(const Plan&, double*, double, int);
 
 }  // namespace pmb

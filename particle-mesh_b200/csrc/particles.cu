@@ -319,12 +319,18 @@ __global__ void k_interp_f32(const float* __restrict__ phi, const uint32_t* __re
 }
 
 // v += c_kick * force; x += dt * v accumulated in FP64 and re-split.
+// Batches: with pbeg != null, grid row blockIdx.y advances the particles
+// [pbeg[b], pend[b]) of box b in the mesh phi + b * mesh_stride.
 template <int ORDER>
 __global__ void k_kick_drift_f32(const float* __restrict__ phi, uint32_t* __restrict__ cell,
                                  float* __restrict__ ox, float* __restrict__ oy, float* __restrict__ oz,
                                  float* __restrict__ vx, float* __restrict__ vy, float* __restrict__ vz,
-                                 long long np, float c_kick, double dt, int n) {
-    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np;
+                                 long long np, float c_kick, double dt, int n,
+                                 const long long* __restrict__ pbeg = nullptr,
+                                 const long long* __restrict__ pend = nullptr, long long mesh_stride = 0) {
+    const long long lo = pbeg ? pbeg[blockIdx.y] : 0, hi = pbeg ? pend[blockIdx.y] : np;
+    if (pbeg) phi += blockIdx.y * mesh_stride;
+    for (long long p = lo + blockIdx.x * (long long)blockDim.x + threadIdx.x; p < hi;
          p += (long long)gridDim.x * blockDim.x) {
         int i, j, k;
         unpack_cell(cell[p], i, j, k);
@@ -461,6 +467,30 @@ int kick_drift_f32(const Plan& p, const float* phi, uint32_t* cell, float* ox, f
             k_kick_drift_f32<2><<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz, np,
                                                                                 (float)c_kick, dt, p.ng);
         }
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+}  // namespace pmb
+
+namespace pmb {
+
+int kick_drift_f32_batch(const Plan& p, const float* phi, uint32_t* cell, float* ox, float* oy, float* oz,
+                         float* vx, float* vy, float* vz, const long long* pbeg, const long long* pend, int nbox,
+                         int64_t np_total, double c_kick, double dt) {
+    if (np_total == 0) return PM_OK;
+    const long long per_box = (np_total + nbox - 1) / nbox;
+    dim3 g(grid_for(p, per_box, kThreads, 2), nbox);
+    const long long ms = (long long)mesh_elems(p.ng);
+    {
+        Timed t(p, ST_KICK_DRIFT);
+        if (p.grad_order == 4)
+            k_kick_drift_f32<4><<<g, kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz, np_total,
+                                                            (float)c_kick, dt, p.ng, pbeg, pend, ms);
+        else
+            k_kick_drift_f32<2><<<g, kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz, np_total,
+                                                            (float)c_kick, dt, p.ng, pbeg, pend, ms);
+    }
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;
 }

@@ -123,6 +123,7 @@ struct Plan {
     size_t bytes = 0;
     StageTimers* timers = nullptr;  // owned by the C-ABI plan object
     TileScratch tiles;
+    int tk = 0;  // column-tile width of the strided FFT passes (0: default)
 };
 
 // Brackets one kernel launch with the plan's stage timer.
@@ -150,11 +151,13 @@ struct Timed {
 inline size_t mesh_elems(int ng) { return (size_t)ng * ng * (ng + 2); }
 
 // FFT passes (fft.cu).  Each returns a PM_* status.
-template <typename T> int fft_r2c(const Plan& p, T* mesh);
-template <typename T> int fft_c2r(const Plan& p, T* mesh);
+// nbox > 1: a batch of nbox meshes of the plan's size, back to back.
+template <typename T> int fft_r2c(const Plan& p, T* mesh, int nbox = 1);
+template <typename T> int fft_c2r(const Plan& p, T* mesh, int nbox = 1);
 template <typename T> int green_apply(const Plan& p, T* mesh, double c_poisson);
-template <typename T> int poisson_fused(const Plan& p, T* mesh, double c_poisson);
+template <typename T> int poisson_fused(const Plan& p, T* mesh, double c_poisson, int nbox = 1);
 bool fft_size_supported(int ng);
+bool tk_variant_supported(int ng, int precision, int tk);
 int fft_prepare(const Plan& p);  // one-time kernel attributes (large smem)
 
 // Particle and mesh kernels (particles.cu).
@@ -176,7 +179,13 @@ int deposit_f32_tiles(Plan& p, const uint32_t* cell, const float* ox, const floa
                       int64_t np, float mass, float* mesh);
 int sort_f32(Plan& p, uint32_t* cell, float* ox, float* oy, float* oz, float* vx, float* vy, float* vz,
              int64_t np);
-int tile_scratch_ensure(Plan& p, int64_t np);
+int deposit_f32_tiles_batch(Plan& p, const uint32_t* cell, const float* ox, const float* oy, const float* oz,
+                            const long long* pbeg, const long long* pend, int nbox, int64_t np_total,
+                            const float* box_mass, float* mesh);
+int kick_drift_f32_batch(const Plan& p, const float* phi, uint32_t* cell, float* ox, float* oy, float* oz,
+                         float* vx, float* vy, float* vz, const long long* pbeg, const long long* pend, int nbox,
+                         int64_t np_total, double c_kick, double dt);
+int tile_scratch_ensure(Plan& p, int64_t np, int nbox);
 void tile_scratch_release(Plan& p);
 int interp_f32(const Plan& p, const float* phi, const uint32_t* cell, const float* ox,
                const float* oy, const float* oz, int64_t np, float* fx, float* fy, float* fz);

@@ -70,17 +70,22 @@ __device__ __forceinline__ uint32_t morton_tile(uint32_t c, int ts_log, int nt) 
 }
 
 // count[key(p)] += 1, aggregated over the lanes of a warp that share a key.
+// Batches: with pbeg != null, grid row blockIdx.y handles the particles
+// [pbeg[b], pend[b]) of box b, whose buckets start at b * nb_box.
 template <bool MORTON>
 __global__ void k_bucket_count(const uint32_t* __restrict__ cell, long long np, int ts_log, int nt,
-                               uint32_t* __restrict__ count) {
+                               uint32_t* __restrict__ count, const long long* __restrict__ pbeg = nullptr,
+                               const long long* __restrict__ pend = nullptr, long long nb_box = 0) {
     const int lane = threadIdx.x & 31;
     const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long base = warp * 32; base < np; base += nwarps * 32) {
+    const long long lo = pbeg ? pbeg[blockIdx.y] : 0, hi = pbeg ? pend[blockIdx.y] : np;
+    const uint32_t kb = pbeg ? (uint32_t)(blockIdx.y * nb_box) : 0u;
+    for (long long base = lo + warp * 32; base < hi; base += nwarps * 32) {
         const long long p = base + lane;
-        const bool valid = p < np;
-        const uint32_t key = valid ? (MORTON ? morton_tile(__ldg(cell + p), ts_log, nt)
-                                             : bucket_of(__ldg(cell + p), ts_log, nt))
+        const bool valid = p < hi;
+        const uint32_t key = valid ? kb + (MORTON ? morton_tile(__ldg(cell + p), ts_log, nt)
+                                                  : bucket_of(__ldg(cell + p), ts_log, nt))
                                    : 0xffffffffu;
         const unsigned peers = __match_any_sync(0xffffffffu, key);
         if (valid && lane == __ffs(peers) - 1) atomicAdd(count + key, (uint32_t)__popc(peers));
@@ -90,16 +95,20 @@ __global__ void k_bucket_count(const uint32_t* __restrict__ cell, long long np, 
 // perm[cursor[key(p)]++] = p, aggregated per warp.
 template <bool MORTON>
 __global__ void k_bucket_scatter(const uint32_t* __restrict__ cell, long long np, int ts_log, int nt,
-                                 uint32_t* __restrict__ cursor, uint32_t* __restrict__ perm) {
+                                 uint32_t* __restrict__ cursor, uint32_t* __restrict__ perm,
+                                 const long long* __restrict__ pbeg = nullptr,
+                                 const long long* __restrict__ pend = nullptr, long long nb_box = 0) {
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
     const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long base = warp * 32; base < np; base += nwarps * 32) {
+    const long long lo = pbeg ? pbeg[blockIdx.y] : 0, hi = pbeg ? pend[blockIdx.y] : np;
+    const uint32_t kb = pbeg ? (uint32_t)(blockIdx.y * nb_box) : 0u;
+    for (long long base = lo + warp * 32; base < hi; base += nwarps * 32) {
         const long long p = base + lane;
-        const bool valid = p < np;
-        const uint32_t key = valid ? (MORTON ? morton_tile(__ldg(cell + p), ts_log, nt)
-                                             : bucket_of(__ldg(cell + p), ts_log, nt))
+        const bool valid = p < hi;
+        const uint32_t key = valid ? kb + (MORTON ? morton_tile(__ldg(cell + p), ts_log, nt)
+                                                  : bucket_of(__ldg(cell + p), ts_log, nt))
                                    : 0xffffffffu;
         const unsigned peers = __match_any_sync(0xffffffffu, key);
         const int leader = __ffs(peers) - 1;
@@ -198,11 +207,17 @@ __global__ void __launch_bounds__(256) k_tile_deposit(const uint32_t* __restrict
                                                       const float* __restrict__ oy, const float* __restrict__ oz,
                                                       const uint32_t* __restrict__ perm,
                                                       const uint32_t* __restrict__ off, float mass, float background,
-                                                      float* __restrict__ mesh, int n, int nt) {
+                                                      float* __restrict__ mesh, int n, int nt,
+                                                      long long mesh_stride = 0,
+                                                      const float* __restrict__ box_mass = nullptr) {
     __shared__ __align__(16) float acc[TS * TS * TS];
     __shared__ uint32_t rbeg[kRuns], rpre[kRuns + 1];
-    const int tile = blockIdx.x;
+    // a batch of boxes: blockIdx.x = box * nt^3 + tile, buckets from box * nt^3 * 8
+    const int tpb = nt * nt * nt, box = blockIdx.x / tpb, tile = blockIdx.x % tpb;
     const int tx = tile / (nt * nt), ty = (tile / nt) % nt, tz = tile % nt;
+    mesh += box * mesh_stride;
+    if (box_mass) mass = box_mass[box];
+    off += (size_t)box * tpb * 8;
     for (int c = threadIdx.x; c < TS * TS * TS / 4; c += blockDim.x)
         reinterpret_cast<float4*>(acc)[c] = make_float4(0.f, 0.f, 0.f, 0.f);
     if (threadIdx.x < kRuns) {  // one bucket run per thread, loaded in parallel
@@ -301,9 +316,13 @@ int bucket_sort(const Plan& p, const uint32_t* cell, int64_t np, int ts_log, int
 
 }  // namespace
 
-int tile_scratch_ensure(Plan& p, int64_t np) {
+int tile_scratch_ensure(Plan& p, int64_t np, int nbox) {
     const int ts = 1 << tile_log(p.ng), nt = p.ng / ts;
-    const long long nb = (long long)nt * nt * nt * 8;
+    int nt2 = 1;  // the sort's Morton keys need nt2^3 buckets
+    while (nt2 < nt) nt2 <<= 1;
+    const long long per = (long long)nt * nt * nt * 8 > (long long)nt2 * nt2 * nt2 ? (long long)nt * nt * nt * 8
+                                                                                 : (long long)nt2 * nt2 * nt2;
+    const long long nb = per * nbox;
     TileScratch& s = p.tiles;
     if (s.nb < nb) {
         for (uint32_t** q : {&s.count, &s.off, &s.cursor, &s.bsum}) {
@@ -345,7 +364,7 @@ int deposit_f32_tiles(Plan& p, const uint32_t* cell, const float* ox, const floa
                       float mass, float* mesh) {
     const int tl = tile_log(p.ng), ts = 1 << tl, nt = p.ng / ts;
     const long long nb = (long long)nt * nt * nt * 8;
-    int rc = tile_scratch_ensure(p, np > 0 ? np : 1);
+    int rc = tile_scratch_ensure(p, np > 0 ? np : 1, 1);
     if (rc != PM_OK) return rc;
     rc = bucket_sort<false>(p, cell, np, tl, nt, nb, p.tiles);
     if (rc != PM_OK) return rc;
@@ -362,13 +381,51 @@ int deposit_f32_tiles(Plan& p, const uint32_t* cell, const float* ox, const floa
     return PM_OK;
 }
 
+// A batch of nbox boxes of the plan's size: box b's particles are
+// [pbeg[b], pend[b]) of the shared arrays (device ranges), its mesh is
+// mesh + b * mesh_elems(ng), its particle mass box_mass[b] (device).
+int deposit_f32_tiles_batch(Plan& p, const uint32_t* cell, const float* ox, const float* oy, const float* oz,
+                            const long long* pbeg, const long long* pend, int nbox, int64_t np_total,
+                            const float* box_mass, float* mesh) {
+    const int tl = tile_log(p.ng), ts = 1 << tl, nt = p.ng / ts;
+    const long long nb_box = (long long)nt * nt * nt * 8, nb = nb_box * nbox;
+    int rc = tile_scratch_ensure(p, np_total > 0 ? np_total : 1, nbox);
+    if (rc != PM_OK) return rc;
+    TileScratch& s = p.tiles;
+    const long long nscan = (nb + kScanThreads * kScanItems - 1) / (kScanThreads * kScanItems);
+    PMB_CUDA_CHECK(cudaMemsetAsync(s.count, 0, nb * sizeof(uint32_t), p.stream));
+    const long long per_box = (np_total + nbox - 1) / nbox;
+    dim3 g(grid_for(p, per_box, 256, 2), nbox);
+    {
+        Timed t(p, ST_BIN);
+        k_bucket_count<false><<<g, 256, 0, p.stream>>>(cell, np_total, tl, nt, s.count, pbeg, pend, nb_box);
+        k_scan_local<<<(unsigned)nscan, kScanThreads, 0, p.stream>>>(s.count, nb, s.off, s.bsum);
+        k_scan_sums<<<1, kScanThreads, 0, p.stream>>>(s.bsum, (int)nscan, s.off + nb);
+        k_scan_add<<<(unsigned)nscan, kScanThreads, 0, p.stream>>>(s.off, s.cursor, nb, s.bsum);
+        k_bucket_scatter<false><<<g, 256, 0, p.stream>>>(cell, np_total, tl, nt, s.cursor, s.perm, pbeg, pend, nb_box);
+    }
+    {
+        Timed t(p, ST_DEPOSIT);
+        const unsigned blocks = (unsigned)(nt * nt * nt) * (unsigned)nbox;
+        const long long ms = (long long)mesh_elems(p.ng);
+        if (ts == 16)
+            k_tile_deposit<16><<<blocks, 256, 0, p.stream>>>(cell, ox, oy, oz, s.perm, s.off, 0.0f, -1.0f, mesh,
+                                                            p.ng, nt, ms, box_mass);
+        else
+            k_tile_deposit<8><<<blocks, 256, 0, p.stream>>>(cell, ox, oy, oz, s.perm, s.off, 0.0f, -1.0f, mesh,
+                                                           p.ng, nt, ms, box_mass);
+    }
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
 int sort_f32(Plan& p, uint32_t* cell, float* ox, float* oy, float* oz, float* vx, float* vy, float* vz, int64_t np) {
     if (np == 0) return PM_OK;
     const int tl = tile_log(p.ng), nt = p.ng >> tl;
     int nt2 = 1;  // Morton keys of nt tiles per axis lie in [0, nt2^3), nt2 the next power of two
     while (nt2 < nt) nt2 <<= 1;
     const long long nb = (long long)nt2 * nt2 * nt2;
-    int rc = tile_scratch_ensure(p, np);
+    int rc = tile_scratch_ensure(p, np, 1);
     if (rc != PM_OK) return rc;
     rc = bucket_sort<true>(p, cell, np, tl, nt, nb, p.tiles);
     if (rc != PM_OK) return rc;

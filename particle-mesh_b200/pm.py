@@ -318,6 +318,67 @@ def zeldovich_ic(ng: int, nrow: int, n_s: float, rms_cells: float, seed: int, ve
     return pos, vel
 
 
+class Ensemble:
+    """Independent boxes of mixed mesh sizes advanced together (FP32 split).
+
+    Particles of all boxes live in one set of split arrays, box b owning
+    np[b] consecutive entries."""
+
+    def __init__(self, ng, np, mass, green: str = "spectral", grad_order: int = 4, autotune: bool = True,
+                 tune_cache: str | None = None, stream: torch.cuda.Stream | None = None):
+        self.lib = L.load()
+        n = len(ng)
+        self.ng, self.np = list(ng), list(np)
+        a_ng = (ctypes.c_int * n)(*ng)
+        a_np = (ctypes.c_int64 * n)(*np)
+        a_m = (ctypes.c_float * n)(*mass)
+        # a stream of its own (graphs are not captured on the legacy stream),
+        # ordered against the caller's current stream around every call
+        self.stream = stream if stream is not None else torch.cuda.Stream()
+        h = ctypes.c_void_p()
+        check(self.lib.pm_ensemble_create(n, a_ng, a_np, a_m, _GREEN[green], grad_order, 1 if autotune else 0,
+                                          tune_cache.encode() if tune_cache else None,
+                                          ctypes.c_void_p(self.stream.cuda_stream), ctypes.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self.lib.pm_ensemble_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001
+            pass
+
+    def info(self) -> dict:
+        nc = ctypes.c_int()
+        ng = (ctypes.c_int * 64)()
+        nb = (ctypes.c_int * 64)()
+        tk = (ctypes.c_int * 64)()
+        by = ctypes.c_size_t()
+        nodes = ctypes.c_size_t()
+        check(self.lib.pm_ensemble_info(self._h, ctypes.byref(nc), ng, nb, tk, ctypes.byref(by), ctypes.byref(nodes)))
+        return {"classes": [{"ng": ng[i], "boxes": nb[i], "tile_cols": tk[i]} for i in range(nc.value)],
+                "device_bytes": by.value, "graph_nodes": nodes.value}
+
+    def step(self, cell, off, vel, c_poisson: float, c_kick: float, dt: float):
+        cur = torch.cuda.current_stream()
+        self.stream.wait_stream(cur)
+        check(self.lib.pm_ensemble_step_f32(self._h, _vp(cell), *(_vp(t) for t in off), *(_vp(t) for t in vel),
+                                            float(c_poisson), float(c_kick), float(dt)))
+        cur.wait_stream(self.stream)
+
+    def run(self, cell, off, vel, c_poisson: float, dt: float, steps: int):
+        """`steps` KDK steps as one CUDA graph (captured on first use)."""
+        cur = torch.cuda.current_stream()
+        self.stream.wait_stream(cur)
+        check(self.lib.pm_ensemble_run_f32(self._h, _vp(cell), *(_vp(t) for t in off), *(_vp(t) for t in vel),
+                                           float(c_poisson), float(dt), int(steps)))
+        cur.wait_stream(self.stream)
+
+
 # ------------------------------------------------ reference-named mirrors
 _plans: dict = {}
 
