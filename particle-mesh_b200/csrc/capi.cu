@@ -86,6 +86,8 @@ void release(Plan& p) {
     if (p.mesh) cudaFree(p.mesh);
     for (void*& f : p.force)
         if (f) cudaFree(f), f = nullptr;
+    for (void*& f : p.adj)
+        if (f) cudaFree(f), f = nullptr;
     p.tw = p.g1d = p.mesh = nullptr;
     p.d_err = nullptr;
     delete p.timers;
@@ -93,7 +95,7 @@ void release(Plan& p) {
     tile_scratch_release(p);
 }
 
-int ensure_workspace(Plan& p, bool forces) {
+int ensure_workspace(Plan& p, bool forces, bool adjoint = false) {
     const size_t esz = p.precision == PM_FP64 ? sizeof(double) : sizeof(float);
     if (!p.mesh) {
         if (cudaMalloc(&p.mesh, mesh_elems(p.ng) * esz) != cudaSuccess) {
@@ -110,6 +112,17 @@ int ensure_workspace(Plan& p, bool forces) {
                 cudaGetLastError();
                 f = nullptr;
                 return fail(PM_ERR_NOMEM, "workspace force allocation failed");
+            }
+            p.bytes += b;
+        }
+    }
+    if (adjoint && !p.adj[0]) {
+        const size_t b = (size_t)p.ng * p.ng * p.ng * sizeof(double);
+        for (void*& f : p.adj) {
+            if (cudaMalloc(&f, b) != cudaSuccess) {
+                cudaGetLastError();
+                f = nullptr;
+                return fail(PM_ERR_NOMEM, "adjoint workspace allocation failed");
             }
             p.bytes += b;
         }
@@ -368,28 +381,27 @@ int pm_adjoint_deposit_f64(pm_plan* plan, const double* x, const double* y, cons
     return adjoint_gather_f64(plan->p, x, y, z, dbar, mass, nullptr, nullptr, 0.0, xbar, ybar, zbar, np);
 }
 
-// Recomputes the force meshes at x on the plan's workspace, adds the direct
-// (weight-derivative) term, then reuses the workspace for the mesh term.
+// Recomputes the force meshes at x (fused Poisson solve), builds the mesh
+// source -sum_a G_a D_a(u) in the same padded mesh once phi is no longer
+// needed, solves it with the same (symmetric) Green's operator, and adds the
+// direct and mesh terms in one gather.
 static int adjoint_force(Plan& p, const double* x, const double* y, const double* z, int64_t np, double mass,
                          double c_poisson, const double* ux, const double* uy, const double* uz, double scale,
                          double* xbar, double* ybar, double* zbar) {
-    PM_TRY(ensure_workspace(p, true));
+    PM_TRY(ensure_workspace(p, true, true));
     double* m = static_cast<double*>(p.mesh);
     double* f[3] = {static_cast<double*>(p.force[0]), static_cast<double*>(p.force[1]),
                     static_cast<double*>(p.force[2])};
+    double* ub[3] = {static_cast<double*>(p.adj[0]), static_cast<double*>(p.adj[1]),
+                     static_cast<double*>(p.adj[2])};
     const double* fc[3] = {f[0], f[1], f[2]};
     const double* u[3] = {ux, uy, uz};
     PM_TRY(deposit_f64(p, x, y, z, np, mass, m));
-    PM_TRY(fft_r2c<double>(p, m));
-    PM_TRY(green_apply<double>(p, m, c_poisson));
-    PM_TRY(fft_c2r<double>(p, m));
+    PM_TRY(poisson_fused<double>(p, m, c_poisson));
     PM_TRY(gradient_f64(p, m, f[0], f[1], f[2]));
-    PM_TRY(adjoint_gather_f64(p, x, y, z, nullptr, 0.0, u, fc, scale, xbar, ybar, zbar, np));
-    PM_TRY(adjoint_mesh_source_f64(p, x, y, z, u, np, f, m));
-    PM_TRY(fft_r2c<double>(p, m));
-    PM_TRY(green_apply<double>(p, m, c_poisson));
-    PM_TRY(fft_c2r<double>(p, m));
-    return adjoint_gather_f64(p, x, y, z, m, scale * mass, nullptr, nullptr, 0.0, xbar, ybar, zbar, np);
+    PM_TRY(adjoint_mesh_source_f64(p, x, y, z, u, np, ub, m));
+    PM_TRY(poisson_fused<double>(p, m, c_poisson));
+    return adjoint_gather_f64(p, x, y, z, m, scale * mass, u, fc, scale, xbar, ybar, zbar, np);
 }
 
 int pm_adjoint_force_f64(pm_plan* plan, const double* x, const double* y, const double* z, int64_t np,

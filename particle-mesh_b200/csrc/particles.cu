@@ -236,7 +236,15 @@ __global__ void k_join(const uint32_t* __restrict__ cell, const float* __restric
 // of the three components share their cells: each of the 32 (2-point) or 56
 // (4-point) distinct values is loaded once, from 12 or 20 mesh rows whose
 // offsets fit in 32 bits (ng <= 1024).
-template <int ORDER>
+// Stencil neighbour i + d (|d| <= 3) wrapped into [0, n): a mask for
+// power-of-two meshes, one conditional otherwise.
+template <bool POW2>
+__device__ __forceinline__ int wrap_near(int c, int n) {
+    if (POW2) return c & (n - 1);
+    return c < 0 ? c + n : (c >= n ? c - n : c);
+}
+
+template <int ORDER, bool POW2>
 __device__ __forceinline__ void force_at(const float* __restrict__ phi, int n, int i, int j, int k,
                                          float tx, float ty, float tz, float& gx, float& gy,
                                          float& gz) {
@@ -245,9 +253,9 @@ __device__ __forceinline__ void force_at(const float* __restrict__ phi, int n, i
     unsigned xo[W], yo[W], kc[W];
 #pragma unroll
     for (int d = 0; d < W; ++d) {
-        xo[d] = (unsigned)wrap_cell(i + LO + d, n) * plane;
-        yo[d] = (unsigned)wrap_cell(j + LO + d, n) * pz;
-        kc[d] = (unsigned)wrap_cell(k + LO + d, n);
+        xo[d] = (unsigned)wrap_near<POW2>(i + LO + d, n) * plane;
+        yo[d] = (unsigned)wrap_near<POW2>(j + LO + d, n) * pz;
+        kc[d] = (unsigned)wrap_near<POW2>(k + LO + d, n);
     }
     constexpr int C0 = -LO;  // stencil slot of offset 0
     // core rows (i+a, j+b): the whole z stencil
@@ -301,8 +309,8 @@ __device__ __forceinline__ void force_at(const float* __restrict__ phi, int n, i
         for (int b = 0; b < 2; ++b) gz += w0[a] * w1[b] * (w2[0] * D(Z[a][b], C0) + w2[1] * D(Z[a][b], C0 + 1));
 }
 
-template <int ORDER>
-__global__ void k_interp_f32(const float* __restrict__ phi, const uint32_t* __restrict__ cell,
+template <int ORDER, bool POW2>
+__global__ void __launch_bounds__(256, 4) k_interp_f32(const float* __restrict__ phi, const uint32_t* __restrict__ cell,
                              const float* __restrict__ ox, const float* __restrict__ oy,
                              const float* __restrict__ oz, long long np, float* __restrict__ fx,
                              float* __restrict__ fy, float* __restrict__ fz, int n) {
@@ -311,7 +319,7 @@ __global__ void k_interp_f32(const float* __restrict__ phi, const uint32_t* __re
         int i, j, k;
         unpack_cell(__ldg(cell + p), i, j, k);
         float gx, gy, gz;
-        force_at<ORDER>(phi, n, i, j, k, __ldg(ox + p), __ldg(oy + p), __ldg(oz + p), gx, gy, gz);
+        force_at<ORDER, POW2>(phi, n, i, j, k, __ldg(ox + p), __ldg(oy + p), __ldg(oz + p), gx, gy, gz);
         fx[p] = gx;
         fy[p] = gy;
         fz[p] = gz;
@@ -321,8 +329,10 @@ __global__ void k_interp_f32(const float* __restrict__ phi, const uint32_t* __re
 // v += c_kick * force; x += dt * v accumulated in FP64 and re-split.
 // Batches: with pbeg != null, grid row blockIdx.y advances the particles
 // [pbeg[b], pend[b]) of box b in the mesh phi + b * mesh_stride.
-template <int ORDER>
-__global__ void k_kick_drift_f32(const float* __restrict__ phi, uint32_t* __restrict__ cell,
+// (at most 64 registers: four 256-thread blocks per SM keep enough warps in
+// flight for the ~60 outstanding gathers per particle)
+template <int ORDER, bool POW2>
+__global__ void __launch_bounds__(256, 4) k_kick_drift_f32(const float* __restrict__ phi, uint32_t* __restrict__ cell,
                                  float* __restrict__ ox, float* __restrict__ oy, float* __restrict__ oz,
                                  float* __restrict__ vx, float* __restrict__ vy, float* __restrict__ vz,
                                  long long np, float c_kick, double dt, int n,
@@ -336,7 +346,7 @@ __global__ void k_kick_drift_f32(const float* __restrict__ phi, uint32_t* __rest
         unpack_cell(cell[p], i, j, k);
         const float tx = ox[p], ty = oy[p], tz = oz[p];
         float gx, gy, gz;
-        force_at<ORDER>(phi, n, i, j, k, tx, ty, tz, gx, gy, gz);
+        force_at<ORDER, POW2>(phi, n, i, j, k, tx, ty, tz, gx, gy, gz);
         const float ux = vx[p] + gx * c_kick, uy = vy[p] + gy * c_kick, uz = vz[p] + gz * c_kick;
         vx[p] = ux;
         vy[p] = uy;
@@ -438,16 +448,19 @@ int join_positions(const Plan& p, const uint32_t* cell, const float* ox, const f
 int interp_f32(const Plan& p, const float* phi, const uint32_t* cell, const float* ox,
                const float* oy, const float* oz, int64_t np, float* fx, float* fy, float* fz) {
     if (np == 0) return PM_OK;
-    if (p.grad_order == 4)
-        {
-            Timed t(p, ST_INTERP);
-            k_interp_f32<4><<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, np, fx, fy, fz, p.ng);
-        }
-    else
-        {
-            Timed t(p, ST_INTERP);
-            k_interp_f32<2><<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, np, fx, fy, fz, p.ng);
-        }
+    {
+        Timed t(p, ST_INTERP);
+        const unsigned g = grid_for(p, np, kThreads);
+        const bool pow2 = (p.ng & (p.ng - 1)) == 0;
+        if (p.grad_order == 4 && pow2)
+            k_interp_f32<4, true><<<g, kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, np, fx, fy, fz, p.ng);
+        else if (p.grad_order == 4)
+            k_interp_f32<4, false><<<g, kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, np, fx, fy, fz, p.ng);
+        else if (pow2)
+            k_interp_f32<2, true><<<g, kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, np, fx, fy, fz, p.ng);
+        else
+            k_interp_f32<2, false><<<g, kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, np, fx, fy, fz, p.ng);
+    }
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;
 }
@@ -455,18 +468,20 @@ int interp_f32(const Plan& p, const float* phi, const uint32_t* cell, const floa
 int kick_drift_f32(const Plan& p, const float* phi, uint32_t* cell, float* ox, float* oy, float* oz,
                    float* vx, float* vy, float* vz, int64_t np, double c_kick, double dt) {
     if (np == 0) return PM_OK;
-    if (p.grad_order == 4)
-        {
-            Timed t(p, ST_KICK_DRIFT);
-            k_kick_drift_f32<4><<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz, np,
-                                                                                (float)c_kick, dt, p.ng);
-        }
-    else
-        {
-            Timed t(p, ST_KICK_DRIFT);
-            k_kick_drift_f32<2><<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz, np,
-                                                                                (float)c_kick, dt, p.ng);
-        }
+    {
+        Timed t(p, ST_KICK_DRIFT);
+        const unsigned g = grid_for(p, np, kThreads);
+        const bool pow2 = (p.ng & (p.ng - 1)) == 0;
+        const float ck = (float)c_kick;
+        if (p.grad_order == 4 && pow2)
+            k_kick_drift_f32<4, true><<<g, kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz, np, ck, dt, p.ng);
+        else if (p.grad_order == 4)
+            k_kick_drift_f32<4, false><<<g, kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz, np, ck, dt, p.ng);
+        else if (pow2)
+            k_kick_drift_f32<2, true><<<g, kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz, np, ck, dt, p.ng);
+        else
+            k_kick_drift_f32<2, false><<<g, kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz, np, ck, dt, p.ng);
+    }
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;
 }
@@ -484,12 +499,20 @@ int kick_drift_f32_batch(const Plan& p, const float* phi, uint32_t* cell, float*
     const long long ms = (long long)mesh_elems(p.ng);
     {
         Timed t(p, ST_KICK_DRIFT);
-        if (p.grad_order == 4)
-            k_kick_drift_f32<4><<<g, kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz, np_total,
-                                                            (float)c_kick, dt, p.ng, pbeg, pend, ms);
+        const bool pow2 = (p.ng & (p.ng - 1)) == 0;
+        const float ck = (float)c_kick;
+        if (p.grad_order == 4 && pow2)
+            k_kick_drift_f32<4, true><<<g, kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz, np_total, ck,
+                                                                  dt, p.ng, pbeg, pend, ms);
+        else if (p.grad_order == 4)
+            k_kick_drift_f32<4, false><<<g, kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz, np_total, ck,
+                                                                   dt, p.ng, pbeg, pend, ms);
+        else if (pow2)
+            k_kick_drift_f32<2, true><<<g, kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz, np_total, ck,
+                                                                  dt, p.ng, pbeg, pend, ms);
         else
-            k_kick_drift_f32<2><<<g, kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz, np_total,
-                                                            (float)c_kick, dt, p.ng, pbeg, pend, ms);
+            k_kick_drift_f32<2, false><<<g, kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz, np_total, ck,
+                                                                   dt, p.ng, pbeg, pend, ms);
     }
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;

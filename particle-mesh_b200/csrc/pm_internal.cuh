@@ -120,6 +120,7 @@ struct Plan {
     int* d_err = nullptr;           // device error bits
     void* mesh = nullptr;           // workspace mesh [ng][ng][ng+2]
     void* force[3] = {nullptr, nullptr, nullptr};  // FP64 force arrays
+    void* adj[3] = {nullptr, nullptr, nullptr};    // FP64 adjoint source arrays (deposited u)
     size_t bytes = 0;
     StageTimers* timers = nullptr;  // owned by the C-ABI plan object
     TileScratch tiles;
