@@ -201,6 +201,7 @@ static int plan_create(int ng, int precision, int green_kind, int grad_order, vo
             rc = fail(PM_ERR_NOMEM, "error word allocation failed");
     }
     if (rc == PM_OK) rc = fft_prepare(p);
+    if (rc == PM_OK && precision == PM_FP32) rc = deposit_zr2c_prepare(p);
     if (rc == PM_OK) {
         p.timers = new (std::nothrow) StageTimers();
         if (!p.timers) rc = fail(PM_ERR_NOMEM, "host allocation failed");
@@ -518,8 +519,13 @@ int pm_step_f32(pm_plan* plan, uint32_t* cell, float* ox, float* oy, float* oz, 
     Plan& p = plan->p;
     PM_TRY(ensure_workspace(p, false));
     float* m = static_cast<float*>(p.mesh);
-    PM_TRY(deposit_f32_tiles(p, cell, ox, oy, oz, np, mass, m));
-    PM_TRY(poisson_fused<float>(p, m, c_poisson));
+    if (zcol_supported(p.ng)) {  // deposit fused with the z FFT pass
+        PM_TRY(deposit_zr2c_f32(p, cell, ox, oy, oz, np, mass, m));
+        PM_TRY(poisson_after_z_f32(p, m, c_poisson));
+    } else {
+        PM_TRY(deposit_f32_tiles(p, cell, ox, oy, oz, np, mass, m));
+        PM_TRY(poisson_fused<float>(p, m, c_poisson));
+    }
     PM_TRY(kick_drift_f32(p, m, cell, ox, oy, oz, vx, vy, vz, np, c_kick, dt));
     return PM_OK;
 }

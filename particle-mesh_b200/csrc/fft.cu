@@ -31,7 +31,6 @@ template <typename T, int N> constexpr int tk_cols() {
 // entries, so the pass-1 writes j*R1 + k of consecutive j hit distinct
 // banks.  Strided passes: TK pad entries after every R1 rows, so the rows
 // j*R1 + k of the neighbouring j that share a warp phase differ in bank.
-template <int R1> __device__ __forceinline__ int zpad(int i) { return i + i / R1; }
 template <int R1, int TK> __device__ __forceinline__ int spad(int row, int tx) {
     return row * TK + tx + TK * (row / R1);
 }
@@ -39,11 +38,6 @@ template <int R1, int TK> __device__ __forceinline__ int spad(int row, int tx) {
 // three access patterns of the two-pass schedule (L = R1 R2, R2 % R1 == 0):
 //   pass-1 input  j + r R2      pass-1 output  j R1 + k
 //   pass-2 input  j + r R1      pass-2 output  j + k R1       (j < R1)
-template <int R1, int R2> struct ZIdx {  // z passes, unit stride, pad 1 per R1
-    static __device__ __forceinline__ int in1(int j, int r) { return j + j / R1 + r * (R2 + R2 / R1); }
-    static __device__ __forceinline__ int out1(int j, int k) { return j * (R1 + 1) + k; }
-    static __device__ __forceinline__ int p2(int j, int r) { return j + r * (R1 + 1); }
-};
 template <int R1, int R2, int TK> struct SIdx {  // strided passes, row stride TK, pad TK per R1 rows
     static __device__ __forceinline__ int in1(int j, int r, int tx) {
         return (j + j / R1) * TK + tx + r * (R2 + R2 / R1) * TK;
@@ -61,7 +55,6 @@ template <typename T, int N> constexpr int z_rows_per_block() {
     return l < 1 ? 1 : (l > 64 ? 64 : l);
 }
 template <typename T, int N> constexpr int z_threads() { return z_threads_per_row<N>() * z_rows_per_block<T, N>(); }
-template <int N> constexpr int z_row_stride() { return (N / 2 + 1) + (N / 2 + 1) / Radix<N / 2>::R1 + 1; }
 
 // R2C along z: complex FFT of the M packed pairs (x[2n], x[2n+1]), then
 // X[k] = E[k] + W_N^k O[k], E = (Z[k] + conj Z[M-k]) / 2, O = -i (Z[k] - conj Z[M-k]) / 2.
@@ -537,6 +530,18 @@ template <typename T> int poisson_fused(const Plan& p, T* mesh, double c_poisson
         L_::xgreen(p, mesh, cg, nbox);
         L_::strided(p, mesh, 1, +1, nbox);
         L_::z(p, mesh, false, nbox);
+    });
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+int poisson_after_z_f32(const Plan& p, float* mesh, double c_poisson) {
+    const double cg = green_scale(p, c_poisson);
+    PMB_LAUNCH(p, float, {
+        L_::strided(p, mesh, 1, -1, 1);
+        L_::xgreen(p, mesh, cg, 1);
+        L_::strided(p, mesh, 1, +1, 1);
+        L_::z(p, mesh, false, 1);
     });
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;

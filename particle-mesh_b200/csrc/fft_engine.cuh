@@ -143,4 +143,18 @@ __device__ __forceinline__ void stockham_pass2(int j, const LD& ld, const ST& st
     for (int k = 0; k < R2; ++k) st(j, k, v[brev<R2>(k)]);
 }
 
+// Padded shared-memory index of the z passes: one pad entry after every R1
+// entries, so the pass-1 writes j*R1 + k of consecutive j hit distinct banks.
+template <int R1> __device__ __forceinline__ int zpad(int i) { return i + i / R1; }
+// The same positions as base + compile-time offset for the two-pass schedule
+// (L = R1 R2, R2 % R1 == 0): pass-1 input j + r R2, pass-1 output j R1 + k,
+// pass-2 input / output j + r R1 (j < R1).
+template <int R1, int R2> struct ZIdx {  // z passes, unit stride, pad 1 per R1
+    static __device__ __forceinline__ int in1(int j, int r) { return j + j / R1 + r * (R2 + R2 / R1); }
+    static __device__ __forceinline__ int out1(int j, int k) { return j * (R1 + 1) + k; }
+    static __device__ __forceinline__ int p2(int j, int r) { return j + r * (R1 + 1); }
+};
+// Complex entries per padded z row (M + 1 values of the half spectrum).
+template <int N> constexpr int z_row_stride() { return (N / 2 + 1) + (N / 2 + 1) / Radix<N / 2>::R1 + 1; }
+
 }  // namespace pmb

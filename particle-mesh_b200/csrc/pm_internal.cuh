@@ -187,6 +187,13 @@ int kick_drift_f32_batch(const Plan& p, const float* phi, uint32_t* cell, float*
                          float* vx, float* vy, float* vz, const long long* pbeg, const long long* pend, int nbox,
                          int64_t np_total, double c_kick, double dt);
 int tile_scratch_ensure(Plan& p, int64_t np, int nbox);
+// Fused deposit + z R2C (tiles.cu) and the rest of the fused Poisson solve
+// after it (fft.cu): y forward, x forward + Green + x inverse, y inverse, z C2R.
+bool zcol_supported(int ng);
+int deposit_zr2c_prepare(const Plan& p);
+int deposit_zr2c_f32(Plan& p, const uint32_t* cell, const float* ox, const float* oy, const float* oz, int64_t np,
+                     float mass, float* mesh);
+int poisson_after_z_f32(const Plan& p, float* mesh, double c_poisson);
 void tile_scratch_release(Plan& p);
 int interp_f32(const Plan& p, const float* phi, const uint32_t* cell, const float* ox,
                const float* oy, const float* oz, int64_t np, float* fx, float* fy, float* fz);

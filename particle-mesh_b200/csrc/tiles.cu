@@ -17,9 +17,10 @@
 // No global atomics touch the mesh and no separate initialisation pass is
 // needed.  Counting uses warp-aggregated atomics (__match_any_sync) on the
 // bucket counters; the exclusive scan is a three-kernel block scan.
+#include <algorithm>
 #include <mutex>
 
-#include "pm_internal.cuh"
+#include "fft_engine.cuh"
 
 namespace pmb {
 
@@ -49,6 +50,22 @@ __device__ __forceinline__ uint32_t bucket_of(uint32_t c, int ts_log, int nt) {
     return tile * 8u + cls;
 }
 
+// Bucket of a particle for the column tiles of the fused deposit + z FFT:
+// CT x CT cells in (x, y) and the whole z extent; class bits x-face (1),
+// y-face (2).  ts_log = log2 CT, nt = tiles per axis.
+__device__ __forceinline__ uint32_t column_bucket_of(uint32_t c, int ts_log, int nt) {
+    int i, j, k;
+    unpack(c, i, j, k);
+    const int n = nt << ts_log;
+    if (i >= n) i %= n;
+    if (j >= n) j %= n;
+    const int m = (1 << ts_log) - 1;
+    const uint32_t tile = (uint32_t)(i >> ts_log) * nt + (uint32_t)(j >> ts_log);
+    return tile * 4u + ((i & m) == m ? 1u : 0u) + ((j & m) == m ? 2u : 0u);
+}
+
+enum : int { KEY_TILE3 = 0, KEY_MORTON = 1, KEY_COLUMN = 2 };
+
 // Morton (Z-order) index of a particle's tile, for the spatial sort.
 __device__ __forceinline__ uint32_t spread3(uint32_t v) {  // 10 bits -> every third bit
     v &= 0x3ffu;
@@ -72,7 +89,7 @@ __device__ __forceinline__ uint32_t morton_tile(uint32_t c, int ts_log, int nt) 
 // count[key(p)] += 1, aggregated over the lanes of a warp that share a key.
 // Batches: with pbeg != null, grid row blockIdx.y handles the particles
 // [pbeg[b], pend[b]) of box b, whose buckets start at b * nb_box.
-template <bool MORTON>
+template <int KEY>
 __global__ void k_bucket_count(const uint32_t* __restrict__ cell, long long np, int ts_log, int nt,
                                uint32_t* __restrict__ count, const long long* __restrict__ pbeg = nullptr,
                                const long long* __restrict__ pend = nullptr, long long nb_box = 0) {
@@ -84,16 +101,19 @@ __global__ void k_bucket_count(const uint32_t* __restrict__ cell, long long np, 
     for (long long base = lo + warp * 32; base < hi; base += nwarps * 32) {
         const long long p = base + lane;
         const bool valid = p < hi;
-        const uint32_t key = valid ? kb + (MORTON ? morton_tile(__ldg(cell + p), ts_log, nt)
-                                                  : bucket_of(__ldg(cell + p), ts_log, nt))
-                                   : 0xffffffffu;
+        uint32_t key = 0xffffffffu;
+        if (valid) {
+            const uint32_t c = __ldg(cell + p);
+            key = kb + (KEY == KEY_MORTON ? morton_tile(c, ts_log, nt)
+                                          : (KEY == KEY_COLUMN ? column_bucket_of(c, ts_log, nt) : bucket_of(c, ts_log, nt)));
+        }
         const unsigned peers = __match_any_sync(0xffffffffu, key);
         if (valid && lane == __ffs(peers) - 1) atomicAdd(count + key, (uint32_t)__popc(peers));
     }
 }
 
 // perm[cursor[key(p)]++] = p, aggregated per warp.
-template <bool MORTON>
+template <int KEY>
 __global__ void k_bucket_scatter(const uint32_t* __restrict__ cell, long long np, int ts_log, int nt,
                                  uint32_t* __restrict__ cursor, uint32_t* __restrict__ perm,
                                  const long long* __restrict__ pbeg = nullptr,
@@ -107,9 +127,12 @@ __global__ void k_bucket_scatter(const uint32_t* __restrict__ cell, long long np
     for (long long base = lo + warp * 32; base < hi; base += nwarps * 32) {
         const long long p = base + lane;
         const bool valid = p < hi;
-        const uint32_t key = valid ? kb + (MORTON ? morton_tile(__ldg(cell + p), ts_log, nt)
-                                                  : bucket_of(__ldg(cell + p), ts_log, nt))
-                                   : 0xffffffffu;
+        uint32_t key = 0xffffffffu;
+        if (valid) {
+            const uint32_t c = __ldg(cell + p);
+            key = kb + (KEY == KEY_MORTON ? morton_tile(c, ts_log, nt)
+                                          : (KEY == KEY_COLUMN ? column_bucket_of(c, ts_log, nt) : bucket_of(c, ts_log, nt)));
+        }
         const unsigned peers = __match_any_sync(0xffffffffu, key);
         const int leader = __ffs(peers) - 1;
         uint32_t at = 0;
@@ -283,6 +306,131 @@ __global__ void __launch_bounds__(256) k_tile_deposit(const uint32_t* __restrict
     }
 }
 
+// Fused deposit + z R2C.  One block per column tile of CT x CT (x, y) cells
+// and the whole z extent (16 rows of N reals): the in-tile CIC corners of the
+// tile's own particles and of the x / y face particles of its three lower
+// neighbours are accumulated straight into the padded complex layout of the
+// z FFT, then each row (minus the -1 background) is transformed in shared
+// memory and written as its N/2+1 spectrum entries.  The density mesh itself
+// is never stored: one write of the mesh instead of a write and a read.
+constexpr int kCT = 4, kCTRows = kCT * kCT;
+constexpr int kColRuns = 5;  // (q, class range): own [0,4); x-1 {1},{3}; y-1 [2,4); x-1,y-1 {3}
+__constant__ int kColQ[kColRuns] = {0, 1, 1, 2, 3};
+__constant__ int kColC0[kColRuns] = {0, 1, 3, 2, 3};
+__constant__ int kColC1[kColRuns] = {4, 2, 4, 4, 4};
+
+template <int N> constexpr int zcol_threads() { return kCTRows * (N / 2) / Radix<N / 2>::R2; }
+
+template <int N>
+__global__ void __launch_bounds__(zcol_threads<N>(), 2)
+k_deposit_zr2c(const uint32_t* __restrict__ cell, const float* __restrict__ ox, const float* __restrict__ oy,
+               const float* __restrict__ oz, const uint32_t* __restrict__ perm, const uint32_t* __restrict__ off,
+               float mass, float* __restrict__ mesh, const float2* __restrict__ tw, int nt) {
+    constexpr int M = N / 2, R1 = Radix<M>::R1, R2 = Radix<M>::R2, NT = M / R2, RS = z_row_stride<N>();
+    constexpr int NTH = zcol_threads<N>();
+    using I = ZIdx<R1, R2>;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    float2* S = reinterpret_cast<float2*>(smraw);
+    float* Sf = reinterpret_cast<float*>(smraw);
+    __shared__ uint32_t rbeg[kColRuns], rpre[kColRuns + 1];
+    const int tile = blockIdx.x, tx = tile / nt, ty = tile % nt;
+    for (int c = threadIdx.x; c < kCTRows * RS; c += NTH) S[c] = make_float2(0.f, 0.f);
+    if (threadIdx.x < kColRuns) {
+        const int q = kColQ[threadIdx.x];
+        const int sx = (tx - (q & 1) + nt) % nt, sy = (ty - ((q >> 1) & 1) + nt) % nt;
+        const uint32_t b = (uint32_t)(sx * nt + sy) * 4u;
+        const uint32_t beg = __ldg(off + b + kColC0[threadIdx.x]);
+        rbeg[threadIdx.x] = beg;
+        rpre[threadIdx.x + 1] = __ldg(off + b + kColC1[threadIdx.x]) - beg;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        rpre[0] = 0;
+        for (int r = 0; r < kColRuns; ++r) rpre[r + 1] += rpre[r];
+    }
+    __syncthreads();
+    const uint32_t total = rpre[kColRuns];
+    // four particles per thread per round, their loads issued together
+    constexpr int U = 4;
+    for (uint32_t t0 = threadIdx.x; t0 < total; t0 += U * NTH) {
+        uint32_t pidx[U];
+        int qq[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const uint32_t t = t0 + u * NTH;
+            qq[u] = -1;
+            pidx[u] = 0;
+            if (t < total) {
+                int r = 0;
+                while (t >= rpre[r + 1]) ++r;
+                pidx[u] = __ldg(perm + rbeg[r] + (t - rpre[r]));
+                qq[u] = kColQ[r];
+            }
+        }
+        uint32_t cc[U];
+        float fx[U], fy[U], fz[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (qq[u] < 0) continue;
+            cc[u] = __ldg(cell + pidx[u]);
+            fx[u] = __ldg(ox + pidx[u]);
+            fy[u] = __ldg(oy + pidx[u]);
+            fz[u] = __ldg(oz + pidx[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int q = qq[u];
+            if (q < 0) continue;
+            int i, j, k;
+            unpack(cc[u], i, j, k);
+            if (k >= N) k %= N;
+            const int li = (i & (kCT - 1)) - ((q & 1) ? kCT : 0), lj = (j & (kCT - 1)) - ((q & 2) ? kCT : 0);
+            const float wx[2] = {1.0f - fx[u], fx[u]}, wy[2] = {1.0f - fy[u], fy[u]};
+            const float wz[2] = {mass * (1.0f - fz[u]), mass * fz[u]};
+            const int kz[2] = {k, (k + 1) & (N - 1)};
+            int zo[2];
+#pragma unroll
+            for (int c = 0; c < 2; ++c) zo[c] = 2 * zpad<R1>(kz[c] >> 1) + (kz[c] & 1);
+#pragma unroll
+            for (int a = 0; a < 2; ++a) {
+                const int ci = li + a;
+                if (ci < 0 || ci >= kCT) continue;
+#pragma unroll
+                for (int b = 0; b < 2; ++b) {
+                    const int cj = lj + b;
+                    if (cj < 0 || cj >= kCT) continue;
+                    float* row = Sf + (ci * kCT + cj) * (2 * RS);
+                    const float wab = wx[a] * wy[b];
+#pragma unroll
+                    for (int c = 0; c < 2; ++c) atomicAdd(row + zo[c], wab * wz[c]);
+                }
+            }
+        }
+    }
+    __syncthreads();
+    // z R2C of the 16 rows (the z pass of the FFT, input already in shared memory)
+    const int rrow = threadIdx.x / NT, tj = threadIdx.x % NT;
+    float2* R = S + rrow * RS;
+    stockham_pass1<R1, R2, -1, true, float2>(
+        tj, [&](int j, int r) { const float2 v = R[I::in1(j, r)]; return make_float2(v.x - 1.0f, v.y - 1.0f); },
+        [&](int j, int k, float2 v) { R[I::out1(j, k)] = v; });
+    __syncthreads();
+    stockham_pass2<R1, R2, -1, true, float2>(
+        tj, [&](int j, int r) { return R[I::p2(j, r)]; }, [&](int j, int k, float2 v) { R[I::p2(j, k)] = v; },
+        [&](int e) { return twiddle<-1>(tw, 2 * e); });
+    __syncthreads();
+    const int ci = rrow / kCT, cj = rrow % kCT;
+    float2* crow = reinterpret_cast<float2*>(mesh + ((long long)(tx * kCT + ci) * N + (ty * kCT + cj)) * (N + 2));
+    for (int k = tj; k <= M; k += NT) {
+        const float2 zk = R[zpad<R1>(k == M ? 0 : k)];
+        const float2 zc = cconj(R[zpad<R1>(k == 0 ? 0 : M - k)]);
+        const float2 e = cscale(cadd(zk, zc), 0.5f);
+        const float2 d = csub(zk, zc);
+        const float2 o = make_float2(0.5f * d.y, -0.5f * d.x);
+        crow[k] = cadd(e, cmul(twiddle<-1>(tw, k), o));
+    }
+}
+
 // out[i] = in[perm[i]] for the seven particle arrays (32-bit words).
 __global__ void k_gather7(const uint32_t* __restrict__ perm, long long np, const uint32_t* const* __restrict__ src,
                           uint32_t* const* __restrict__ dst) {
@@ -297,18 +445,18 @@ __global__ void k_gather7(const uint32_t* __restrict__ perm, long long np, const
 int tile_log(int n) { return n >= 16 ? 4 : 3; }  // 16^3 tiles (8^3 for the 8^3 mesh)
 
 // Counting sort of the bucket keys into perm / off (scratch of the plan).
-template <bool MORTON>
+template <int KEY>
 int bucket_sort(const Plan& p, const uint32_t* cell, int64_t np, int ts_log, int nt, long long nb, TileScratch& s) {
     const long long nscan = (nb + kScanThreads * kScanItems - 1) / (kScanThreads * kScanItems);
     PMB_CUDA_CHECK(cudaMemsetAsync(s.count, 0, nb * sizeof(uint32_t), p.stream));
     const unsigned g = grid_for(p, np, 256);
     {
         Timed t(p, ST_BIN);
-        if (np > 0) k_bucket_count<MORTON><<<g, 256, 0, p.stream>>>(cell, np, ts_log, nt, s.count);
+        if (np > 0) k_bucket_count<KEY><<<g, 256, 0, p.stream>>>(cell, np, ts_log, nt, s.count);
         k_scan_local<<<(unsigned)nscan, kScanThreads, 0, p.stream>>>(s.count, nb, s.off, s.bsum);
         k_scan_sums<<<1, kScanThreads, 0, p.stream>>>(s.bsum, (int)nscan, s.off + nb);
         k_scan_add<<<(unsigned)nscan, kScanThreads, 0, p.stream>>>(s.off, s.cursor, nb, s.bsum);
-        if (np > 0) k_bucket_scatter<MORTON><<<g, 256, 0, p.stream>>>(cell, np, ts_log, nt, s.cursor, s.perm);
+        if (np > 0) k_bucket_scatter<KEY><<<g, 256, 0, p.stream>>>(cell, np, ts_log, nt, s.cursor, s.perm);
     }
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;
@@ -320,8 +468,10 @@ int tile_scratch_ensure(Plan& p, int64_t np, int nbox) {
     const int ts = 1 << tile_log(p.ng), nt = p.ng / ts;
     int nt2 = 1;  // the sort's Morton keys need nt2^3 buckets
     while (nt2 < nt) nt2 <<= 1;
-    const long long per = (long long)nt * nt * nt * 8 > (long long)nt2 * nt2 * nt2 ? (long long)nt * nt * nt * 8
-                                                                                 : (long long)nt2 * nt2 * nt2;
+    // the largest bucket layout: 3D tiles x 8 classes, Morton keys, or the
+    // fused deposit's column tiles x 4 classes
+    const long long col = (long long)(p.ng / 4) * (p.ng / 4) * 4;
+    const long long per = std::max(std::max((long long)nt * nt * nt * 8, (long long)nt2 * nt2 * nt2), col);
     const long long nb = per * nbox;
     TileScratch& s = p.tiles;
     if (s.nb < nb) {
@@ -366,7 +516,7 @@ int deposit_f32_tiles(Plan& p, const uint32_t* cell, const float* ox, const floa
     const long long nb = (long long)nt * nt * nt * 8;
     int rc = tile_scratch_ensure(p, np > 0 ? np : 1, 1);
     if (rc != PM_OK) return rc;
-    rc = bucket_sort<false>(p, cell, np, tl, nt, nb, p.tiles);
+    rc = bucket_sort<KEY_TILE3>(p, cell, np, tl, nt, nb, p.tiles);
     if (rc != PM_OK) return rc;
     {
         Timed t(p, ST_DEPOSIT);
@@ -398,11 +548,11 @@ int deposit_f32_tiles_batch(Plan& p, const uint32_t* cell, const float* ox, cons
     dim3 g(grid_for(p, per_box, 256, 2), nbox);
     {
         Timed t(p, ST_BIN);
-        k_bucket_count<false><<<g, 256, 0, p.stream>>>(cell, np_total, tl, nt, s.count, pbeg, pend, nb_box);
+        k_bucket_count<KEY_TILE3><<<g, 256, 0, p.stream>>>(cell, np_total, tl, nt, s.count, pbeg, pend, nb_box);
         k_scan_local<<<(unsigned)nscan, kScanThreads, 0, p.stream>>>(s.count, nb, s.off, s.bsum);
         k_scan_sums<<<1, kScanThreads, 0, p.stream>>>(s.bsum, (int)nscan, s.off + nb);
         k_scan_add<<<(unsigned)nscan, kScanThreads, 0, p.stream>>>(s.off, s.cursor, nb, s.bsum);
-        k_bucket_scatter<false><<<g, 256, 0, p.stream>>>(cell, np_total, tl, nt, s.cursor, s.perm, pbeg, pend, nb_box);
+        k_bucket_scatter<KEY_TILE3><<<g, 256, 0, p.stream>>>(cell, np_total, tl, nt, s.cursor, s.perm, pbeg, pend, nb_box);
     }
     {
         Timed t(p, ST_DEPOSIT);
@@ -419,6 +569,56 @@ int deposit_f32_tiles_batch(Plan& p, const uint32_t* cell, const float* ox, cons
     return PM_OK;
 }
 
+bool zcol_supported(int ng) { return ng >= 32 && ng <= 1024 && (ng & (ng - 1)) == 0; }
+
+template <int N> static int zcol_prepare() {
+    const int smem = kCTRows * z_row_stride<N>() * (int)sizeof(float2);
+    PMB_CUDA_CHECK(cudaFuncSetAttribute(k_deposit_zr2c<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    return PM_OK;
+}
+
+int deposit_zr2c_prepare(const Plan& p) {
+    switch (p.ng) {
+        case 32: return zcol_prepare<32>();
+        case 64: return zcol_prepare<64>();
+        case 128: return zcol_prepare<128>();
+        case 256: return zcol_prepare<256>();
+        case 512: return zcol_prepare<512>();
+        case 1024: return zcol_prepare<1024>();
+        default: return PM_OK;
+    }
+}
+
+// Deposit + z R2C in one pass over the mesh (FP32, power-of-two ng >= 32):
+// mesh receives the z-transformed density contrast, ready for the y pass.
+int deposit_zr2c_f32(Plan& p, const uint32_t* cell, const float* ox, const float* oy, const float* oz, int64_t np,
+                     float mass, float* mesh) {
+    const int nt = p.ng / kCT, cl = 2;  // log2 kCT
+    const long long nb = (long long)nt * nt * 4;
+    int rc = tile_scratch_ensure(p, np > 0 ? np : 1, 1);
+    if (rc != PM_OK) return rc;
+    rc = bucket_sort<KEY_COLUMN>(p, cell, np, cl, nt, nb, p.tiles);
+    if (rc != PM_OK) return rc;
+    const float2* tw = static_cast<const float2*>(p.tw);
+    {
+        Timed t(p, ST_DEPOSIT);
+        const unsigned blocks = (unsigned)(nt * nt);
+#define PMB_ZCOL(NN)                                                                                         case NN:                                                                                                     k_deposit_zr2c<NN><<<blocks, zcol_threads<NN>(), kCTRows * z_row_stride<NN>() * sizeof(float2),                              p.stream>>>(cell, ox, oy, oz, p.tiles.perm, p.tiles.off, mass, mesh, tw, nt);         break;
+        switch (p.ng) {
+            PMB_ZCOL(32)
+            PMB_ZCOL(64)
+            PMB_ZCOL(128)
+            PMB_ZCOL(256)
+            PMB_ZCOL(512)
+            PMB_ZCOL(1024)
+            default: return fail(PM_ERR_SIZE, "fused deposit needs a power-of-two ng >= 32");
+        }
+#undef PMB_ZCOL
+    }
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
 int sort_f32(Plan& p, uint32_t* cell, float* ox, float* oy, float* oz, float* vx, float* vy, float* vz, int64_t np) {
     if (np == 0) return PM_OK;
     const int tl = tile_log(p.ng), nt = p.ng >> tl;
@@ -427,7 +627,7 @@ int sort_f32(Plan& p, uint32_t* cell, float* ox, float* oy, float* oz, float* vx
     const long long nb = (long long)nt2 * nt2 * nt2;
     int rc = tile_scratch_ensure(p, np, 1);
     if (rc != PM_OK) return rc;
-    rc = bucket_sort<true>(p, cell, np, tl, nt, nb, p.tiles);
+    rc = bucket_sort<KEY_MORTON>(p, cell, np, tl, nt, nb, p.tiles);
     if (rc != PM_OK) return rc;
     uint32_t* tmp = nullptr;
     if (cudaMallocAsync(&tmp, (size_t)np * 7 * 4, p.stream) != cudaSuccess) {
@@ -550,11 +750,11 @@ extern "C" int pm_deposit_f32_noalloc(int ng, const uint32_t* cell, const float*
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
     long long need = (np + 255) / 256, cap = (long long)d->num_sms * 8;
     const unsigned g = (unsigned)(need < 1 ? 1 : (need < cap ? need : cap));
-    if (np > 0) k_bucket_count<false><<<g, 256, 0, s>>>(cell, np, tl, nt, count);
+    if (np > 0) k_bucket_count<KEY_TILE3><<<g, 256, 0, s>>>(cell, np, tl, nt, count);
     k_scan_local<<<(unsigned)nscan, kScanThreads, 0, s>>>(count, nb, off, bsum);
     k_scan_sums<<<1, kScanThreads, 0, s>>>(bsum, (int)nscan, off + nb);
     k_scan_add<<<(unsigned)nscan, kScanThreads, 0, s>>>(off, cursor, nb, bsum);
-    if (np > 0) k_bucket_scatter<false><<<g, 256, 0, s>>>(cell, np, tl, nt, cursor, perm);
+    if (np > 0) k_bucket_scatter<KEY_TILE3><<<g, 256, 0, s>>>(cell, np, tl, nt, cursor, perm);
     if (ts == 16)
         k_tile_deposit<16><<<nt * nt * nt, 256, 0, s>>>(cell, ox, oy, oz, perm, off, mass, -1.0f, mesh, ng, nt);
     else
