@@ -321,8 +321,10 @@ __constant__ int kColC1[kColRuns] = {4, 2, 4, 4, 4};
 
 template <int N> constexpr int zcol_threads() { return kCTRows * (N / 2) / Radix<N / 2>::R2; }
 
+// Three blocks per SM (80 registers; 3 x 67.6 KB of rows at N = 1024): the
+// particle phase of one block overlaps the FFT and store phases of another.
 template <int N>
-__global__ void __launch_bounds__(zcol_threads<N>(), 2)
+__global__ void __launch_bounds__(zcol_threads<N>(), 3)
 k_deposit_zr2c(const uint32_t* __restrict__ cell, const float* __restrict__ ox, const float* __restrict__ oy,
                const float* __restrict__ oz, const uint32_t* __restrict__ perm, const uint32_t* __restrict__ off,
                float mass, float* __restrict__ mesh, const float2* __restrict__ tw, int nt) {

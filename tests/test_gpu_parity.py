@@ -95,6 +95,31 @@ def test_fft_f32(pmpkg, ng):
 
 
 @pytest.mark.parametrize("kind", ["discrete", "spectral"])
+@pytest.mark.parametrize("ng", [512, 1024])
+def test_fft_and_poisson_f32_large_match_f64(pmpkg, ng, kind):
+    """Meshes larger than L2 (the pipelined persistent strided passes): the
+    FP32 spectrum and the FP32 fused Poisson solve against the FP64 plan."""
+    g = torch.Generator(device=DEV).manual_seed(ng + 7)
+    x = torch.randn((ng, ng, ng), generator=g, device=DEV, dtype=torch.float64)
+    p64, p32 = pmpkg.Plan(ng, "fp64", kind), pmpkg.Plan(ng, "fp32", kind)
+    d64, d32 = p64.new_mesh(), p32.new_mesh()
+    d64[:, :, :ng] = x
+    d32[:, :, :ng] = x.float()
+    p64.fft_r2c(d64)
+    p32.fft_r2c(d32)
+    err = float((d32.double() - d64).norm() / d64.norm())
+    assert err < 2e-6, err
+    d64[:, :, :ng], d32[:, :, :ng] = x, x.float()
+    d64[:, :, ng:], d32[:, :, ng:] = 0, 0
+    p64.poisson(d64, 2.5)
+    p32.poisson(d32, 2.5)
+    err = float((d32[:, :, :ng].double() - d64[:, :, :ng]).norm() / d64[:, :, :ng].norm())
+    assert err < 2e-6, err
+    del d64, d32, x
+    torch.cuda.empty_cache()
+
+
+@pytest.mark.parametrize("kind", ["discrete", "spectral"])
 @pytest.mark.parametrize("prec", ["fp64", "fp32"])
 def test_green_and_fused_poisson(pmpkg, O, kind, prec):
     ng = 32
@@ -312,7 +337,7 @@ def test_sort_preserves_particles_and_step(pmpkg, O):
     assert np.abs(m1 - m0).max() < 1e-5
 
 
-@pytest.mark.parametrize("ng,nrow", [(32, 32), (128, 64), (256, 128)])
+@pytest.mark.parametrize("ng,nrow", [(32, 32), (128, 64), (256, 128), (512, 64)])
 def test_fused_step_matches_stagewise(pmpkg, O, ng, nrow):
     """pm_step_f32 (deposit fused with the z FFT pass) equals the separate
     stages deposit -> Poisson -> kick + drift on the same state."""
