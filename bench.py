@@ -16,6 +16,8 @@ over every particle; particle-updates/s = particles x steps / time.
   roofline   dominant kernel, algorithmic bytes / CUDA-event time, vs the
              measured HBM copy bandwidth
   cpu_baseline the reference's CPU code on a bounded sample (rank 0, N = 1)
+  adjoint    adjoint step vs forward step at 128^3 (FP32 split path; FP64 check
+             path under "fp64")
 
 Multi-GPU (torchrun): every rank advances its own box (seed + rank) with no
 collective on the data path; the timing is the max over ranks (weak scaling).
@@ -55,6 +57,7 @@ def parse():
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-ensemble", action="store_true")
+    ap.add_argument("--skip-adjoint", action="store_true")
     ap.add_argument("--ensemble-boxes", type=int, default=256)
     return ap.parse_args()
 
@@ -375,15 +378,12 @@ def ours(args):
         torch.cuda.empty_cache()
 
     # ---- adjoint step vs forward step, differentiable-PM configuration
+    # (128^3 on 128^3; the FP32 split path is the configuration's own, FP64
+    # its check path)
     adjoint = None
-    if not args.skip_fp64:
+    if not args.skip_adjoint:
         na = 128
         pa, va = pm.zeldovich_ic(na, na, -2.0, 0.5, 7 + rank, device=dev)
-        pla = pm.Plan(na, "fp64", "spectral", 4, stream=stream, device=dev)
-        xb = [torch.randn_like(pa[0]) for _ in range(3)]
-        vb = [torch.randn_like(pa[0]) for _ in range(3)]
-        xs = [a.clone() for a in pa]
-        vs = [a.clone() for a in va]
 
         def timed(fn, reps=20):
             for _ in range(3):
@@ -396,15 +396,36 @@ def ours(args):
             torch.cuda.synchronize()
             return e0.elapsed_time(e1) / reps
 
-        t_f = timed(lambda: pla.step(*xs, *vs, 1.0, cp, 0.01, 0.0))
-        t_a = timed(lambda: pla.step_adjoint(*pa, 1.0, cp, 0.01, 0.01, xb, vb))
-        adjoint = {"config": "128^3 particles on 128^3 mesh, FP64, spectral Poisson, 4-point gradient",
-                   "forward_step_ms": t_f, "adjoint_step_ms": t_a, "adjoint_over_forward": t_a / t_f,
-                   "with_recompute_over_forward": (t_a + t_f) / t_f,
-                   "note": "adjoint step = force recomputation at the step's start + transposed pairs; "
-                           "checkpointed backprop also re-runs each forward step once"}
-        pla.close()
-        del pla, pa, va, xb, vb, xs, vs
+        def leg(t_f, t_a, prec):
+            return {"config": f"128^3 particles on 128^3 mesh, {prec}, spectral Poisson, 4-point gradient",
+                    "forward_step_ms": t_f, "adjoint_step_ms": t_a, "adjoint_over_forward": t_a / t_f,
+                    "with_recompute_over_forward": (t_a + t_f) / t_f}
+
+        p32a = pm.Plan(na, "fp32", "spectral", 4, stream=stream, device=dev)
+        cell, off = p32a.split(*pa)
+        v32 = [a.float().contiguous() for a in va]
+        cs, os_, vs32 = cell.clone(), [a.clone() for a in off], [a.clone() for a in v32]
+        xb32 = [torch.randn_like(off[0]) for _ in range(3)]
+        vb32 = [torch.randn_like(off[0]) for _ in range(3)]
+        t_f32 = timed(lambda: p32a.step_split(cs, os_, vs32, 1.0, cp, 0.01, 0.01))
+        t_a32 = timed(lambda: p32a.step_adjoint_split(cell, off, 1.0, cp, 0.01, 0.01, xb32, vb32))
+        adjoint = leg(t_f32, t_a32, "FP32 split positions")
+        adjoint["note"] = ("adjoint step = force recomputation at the step's start + transposed pairs; "
+                           "checkpointed backprop also re-runs each forward step once")
+        p32a.close()
+        del p32a, cell, off, v32, cs, os_, vs32, xb32, vb32
+        if not args.skip_fp64:
+            pla = pm.Plan(na, "fp64", "spectral", 4, stream=stream, device=dev)
+            xb = [torch.randn_like(pa[0]) for _ in range(3)]
+            vb = [torch.randn_like(pa[0]) for _ in range(3)]
+            xs = [a.clone() for a in pa]
+            vs = [a.clone() for a in va]
+            t_f = timed(lambda: pla.step(*xs, *vs, 1.0, cp, 0.01, 0.01))
+            t_a = timed(lambda: pla.step_adjoint(*pa, 1.0, cp, 0.01, 0.01, xb, vb))
+            adjoint["fp64"] = leg(t_f, t_a, "FP64")
+            pla.close()
+            del pla, xb, vb, xs, vs
+        del pa, va
 
     # ---- batched ensemble: 256 boxes of mixed mesh sizes, 20 KDK steps per graph
     ensemble = None

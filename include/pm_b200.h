@@ -181,6 +181,24 @@ int pm_step_adjoint_f64(pm_plan* plan, const double* x, const double* y, const d
                         double mass, double c_poisson, double c_kick, double dt, double* xbar,
                         double* ybar, double* zbar, double* vxbar, double* vybar, double* vzbar);
 
+/* ------------------------------------------------- FP32 adjoints (new)
+ * The same vector-Jacobian products for the FP32 split-position step
+ * (pm_step_f32): positions are cell + offset, the adjoint arrays are FP32
+ * per particle, dbar is an FP32 mesh [ng][ng][ng+2].  No counterpart in the
+ * reference.  The force Jacobian is formed from phi at the particle (no
+ * force meshes); the mesh term uses a second FP32 mesh of the plan.
+ * pm_step_adjoint_f32 takes the split state the forward step started from. */
+int pm_adjoint_deposit_f32(pm_plan* plan, const uint32_t* cell, const float* ox, const float* oy,
+                           const float* oz, int64_t np, float mass, const float* dbar, float* xbar,
+                           float* ybar, float* zbar);
+int pm_adjoint_force_f32(pm_plan* plan, const uint32_t* cell, const float* ox, const float* oy,
+                         const float* oz, int64_t np, float mass, double c_poisson, const float* ux,
+                         const float* uy, const float* uz, double scale, float* xbar, float* ybar,
+                         float* zbar);
+int pm_step_adjoint_f32(pm_plan* plan, const uint32_t* cell, const float* ox, const float* oy,
+                        const float* oz, int64_t np, float mass, double c_poisson, double c_kick, double dt,
+                        float* xbar, float* ybar, float* zbar, float* vxbar, float* vybar, float* vzbar);
+
 /* Device pointer to the plan's own mesh [ng][ng][ng+2] (density after the
  * deposit of pm_step_*, potential after it returns). */
 int pm_plan_mesh(pm_plan* plan, void** mesh);

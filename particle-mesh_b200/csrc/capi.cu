@@ -88,7 +88,8 @@ void release(Plan& p) {
         if (f) cudaFree(f), f = nullptr;
     for (void*& f : p.adj)
         if (f) cudaFree(f), f = nullptr;
-    p.tw = p.g1d = p.mesh = nullptr;
+    if (p.adjm) cudaFree(p.adjm);
+    p.tw = p.g1d = p.mesh = p.adjm = nullptr;
     p.d_err = nullptr;
     delete p.timers;
     p.timers = nullptr;
@@ -117,7 +118,7 @@ int ensure_workspace(Plan& p, bool forces, bool adjoint = false) {
         }
     }
     if (adjoint && !p.adj[0]) {
-        const size_t b = (size_t)p.ng * p.ng * p.ng * sizeof(double);
+        const size_t b = (size_t)p.ng * p.ng * p.ng * esz;
         for (void*& f : p.adj) {
             if (cudaMalloc(&f, b) != cudaSuccess) {
                 cudaGetLastError();
@@ -126,6 +127,16 @@ int ensure_workspace(Plan& p, bool forces, bool adjoint = false) {
             }
             p.bytes += b;
         }
+    }
+    // FP32 keeps phi for the direct term, so the adjoint potential needs a
+    // padded mesh of its own (FP64 reuses the plan mesh after the gradient)
+    if (adjoint && p.precision == PM_FP32 && !p.adjm) {
+        if (cudaMalloc(&p.adjm, mesh_elems(p.ng) * esz) != cudaSuccess) {
+            cudaGetLastError();
+            p.adjm = nullptr;
+            return fail(PM_ERR_NOMEM, "adjoint workspace allocation failed");
+        }
+        p.bytes += mesh_elems(p.ng) * esz;
     }
     return PM_OK;
 }
@@ -528,6 +539,69 @@ int pm_step_f32(pm_plan* plan, uint32_t* cell, float* ox, float* oy, float* oz, 
     }
     PM_TRY(kick_drift_f32(p, m, cell, ox, oy, oz, vx, vy, vz, np, c_kick, dt));
     return PM_OK;
+}
+
+// ------------------------------------------------------- FP32 adjoints
+
+int pm_adjoint_deposit_f32(pm_plan* plan, const uint32_t* cell, const float* ox, const float* oy,
+                           const float* oz, int64_t np, float mass, const float* dbar, float* xbar,
+                           float* ybar, float* zbar) {
+    PM_TRY(check_plan(plan, PM_FP32));
+    PM_TRY(check_np(np, {cell, ox, oy, oz, xbar, ybar, zbar}));
+    if (!dbar) return fail(PM_ERR_ARG, "dbar is NULL");
+    PM_TRY(set_device(plan->p));
+    float* xb[3] = {xbar, ybar, zbar};
+    return adjoint_gather_f32(plan->p, cell, ox, oy, oz, np, dbar, mass, nullptr, nullptr, 0.0, xb);
+}
+
+// phi at the split positions (the step's own deposit + Poisson path), the
+// mesh source -sum_a G_a D_a(u) solved with the same symmetric Green's
+// operator into the second mesh, then one gather for both terms.
+static int adjoint_force_f32(Plan& p, const uint32_t* cell, const float* ox, const float* oy, const float* oz,
+                             int64_t np, float mass, double c_poisson, const float* u[3], double scale,
+                             float* xbar[3]) {
+    PM_TRY(ensure_workspace(p, false, true));
+    float* m = static_cast<float*>(p.mesh);
+    float* psi = static_cast<float*>(p.adjm);
+    float* ub[3] = {static_cast<float*>(p.adj[0]), static_cast<float*>(p.adj[1]), static_cast<float*>(p.adj[2])};
+    if (zcol_supported(p.ng)) {
+        PM_TRY(deposit_zr2c_f32(p, cell, ox, oy, oz, np, mass, m));
+        PM_TRY(poisson_after_z_f32(p, m, c_poisson));
+    } else {
+        PM_TRY(deposit_f32_tiles(p, cell, ox, oy, oz, np, mass, m));
+        PM_TRY(poisson_fused<float>(p, m, c_poisson));
+    }
+    PM_TRY(adjoint_mesh_source_f32(p, cell, ox, oy, oz, u, np, ub, psi));
+    PM_TRY(poisson_fused<float>(p, psi, c_poisson));
+    return adjoint_gather_f32(p, cell, ox, oy, oz, np, psi, scale * mass, m, u, scale, xbar);
+}
+
+int pm_adjoint_force_f32(pm_plan* plan, const uint32_t* cell, const float* ox, const float* oy,
+                         const float* oz, int64_t np, float mass, double c_poisson, const float* ux,
+                         const float* uy, const float* uz, double scale, float* xbar, float* ybar,
+                         float* zbar) {
+    PM_TRY(check_plan(plan, PM_FP32));
+    PM_TRY(check_np(np, {cell, ox, oy, oz, ux, uy, uz, xbar, ybar, zbar}));
+    PM_TRY(set_device(plan->p));
+    const float* u[3] = {ux, uy, uz};
+    float* xb[3] = {xbar, ybar, zbar};
+    return adjoint_force_f32(plan->p, cell, ox, oy, oz, np, mass, c_poisson, u, scale, xb);
+}
+
+int pm_step_adjoint_f32(pm_plan* plan, const uint32_t* cell, const float* ox, const float* oy,
+                        const float* oz, int64_t np, float mass, double c_poisson, double c_kick, double dt,
+                        float* xbar, float* ybar, float* zbar, float* vxbar, float* vybar, float* vzbar) {
+    PM_TRY(check_plan(plan, PM_FP32));
+    PM_TRY(check_np(np, {cell, ox, oy, oz, xbar, ybar, zbar, vxbar, vybar, vzbar}));
+    PM_TRY(set_device(plan->p));
+    Plan& p = plan->p;
+    float* vb[3] = {vxbar, vybar, vzbar};
+    float* xb[3] = {xbar, ybar, zbar};
+    const float* xbc[3] = {xbar, ybar, zbar};
+    const float* vbc[3] = {vxbar, vybar, vzbar};
+    if (dt != 0.0) PM_TRY(axpy3_f32(p, vb, xbc, dt, np));  // x' = x + dt v'  =>  vbar' += dt xbar
+    if (c_kick == 0.0) return PM_OK;
+    return adjoint_force_f32(p, cell, ox, oy, oz, np, mass, c_poisson, vbc, c_kick, xb);
 }
 
 // ------------------------------------------------------------------- ICs

@@ -244,50 +244,71 @@ __device__ __forceinline__ int wrap_near(int c, int n) {
     return c < 0 ? c + n : (c >= n ? c - n : c);
 }
 
+// The potential values the 2- or 4-point centred differences need at the 8
+// CIC corners (i+a, j+b, k+c), each loaded once: the core rows (i+a, j+b)
+// over the whole z stencil, and the x and y stencil rows at columns k, k+1.
+template <int ORDER, bool POW2> struct Stencil {
+    static constexpr int LO = ORDER == 4 ? -2 : -1, W = ORDER == 4 ? 6 : 4;  // offsets LO..LO+W-1
+    static constexpr int C0 = -LO;                                            // slot of offset 0
+    float Z[2][2][W], X[W][2][2], Y[2][W][2];
+
+    __device__ __forceinline__ Stencil(const float* __restrict__ phi, int n, int i, int j, int k) {
+        const unsigned pz = (unsigned)n + 2u, plane = (unsigned)n * pz;
+        unsigned xo[W], yo[W], kc[W];
+#pragma unroll
+        for (int d = 0; d < W; ++d) {
+            xo[d] = (unsigned)wrap_near<POW2>(i + LO + d, n) * plane;
+            yo[d] = (unsigned)wrap_near<POW2>(j + LO + d, n) * pz;
+            kc[d] = (unsigned)wrap_near<POW2>(k + LO + d, n);
+        }
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+            for (int b = 0; b < 2; ++b)
+#pragma unroll
+                for (int c = 0; c < W; ++c) Z[a][b][c] = __ldg(phi + xo[C0 + a] + yo[C0 + b] + kc[c]);
+#pragma unroll
+        for (int d = 0; d < W; ++d)
+#pragma unroll
+            for (int b = 0; b < 2; ++b)
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    if (d == C0 || d == C0 + 1) {
+                        X[d][b][c] = Z[d - C0][b][C0 + c];
+                        Y[b][d][c] = Z[b][d - C0][C0 + c];
+                    } else {
+                        X[d][b][c] = __ldg(phi + xo[d] + yo[C0 + b] + kc[C0 + c]);
+                        Y[b][d][c] = __ldg(phi + xo[C0 + b] + yo[d] + kc[C0 + c]);
+                    }
+                }
+    }
+    // centred difference (minus the gradient) at slot s of a stencil line v
+    static __device__ __forceinline__ float D(const float* v, int s) {
+        return ORDER == 4 ? (8.0f * (v[s - 1] - v[s + 1]) - (v[s - 2] - v[s + 2])) * (1.0f / 12.0f)
+                          : (v[s - 1] - v[s + 1]) * 0.5f;
+    }
+    // the three components of -grad phi at corner (a, b, c)
+    __device__ __forceinline__ void corner(int a, int b, int c, float& fx, float& fy, float& fz) const {
+        float lx[W], ly[W];
+#pragma unroll
+        for (int d = 0; d < W; ++d) {
+            lx[d] = X[d][b][c];
+            ly[d] = Y[a][d][c];
+        }
+        fx = D(lx, C0 + a);
+        fy = D(ly, C0 + b);
+        fz = D(Z[a][b], C0 + c);
+    }
+};
+
 template <int ORDER, bool POW2>
 __device__ __forceinline__ void force_at(const float* __restrict__ phi, int n, int i, int j, int k,
                                          float tx, float ty, float tz, float& gx, float& gy,
                                          float& gz) {
-    constexpr int LO = ORDER == 4 ? -2 : -1, W = ORDER == 4 ? 6 : 4;  // stencil offsets LO..LO+W-1
-    const unsigned pz = (unsigned)n + 2u, plane = (unsigned)n * pz;
-    unsigned xo[W], yo[W], kc[W];
-#pragma unroll
-    for (int d = 0; d < W; ++d) {
-        xo[d] = (unsigned)wrap_near<POW2>(i + LO + d, n) * plane;
-        yo[d] = (unsigned)wrap_near<POW2>(j + LO + d, n) * pz;
-        kc[d] = (unsigned)wrap_near<POW2>(k + LO + d, n);
-    }
-    constexpr int C0 = -LO;  // stencil slot of offset 0
-    // core rows (i+a, j+b): the whole z stencil
-    float Z[2][2][W];
-#pragma unroll
-    for (int a = 0; a < 2; ++a)
-#pragma unroll
-        for (int b = 0; b < 2; ++b)
-#pragma unroll
-            for (int c = 0; c < W; ++c) Z[a][b][c] = __ldg(phi + xo[C0 + a] + yo[C0 + b] + kc[c]);
-    // x stencil rows (i+d, j+b) and y stencil rows (i+a, j+d), columns k, k+1
-    float X[W][2][2], Y[2][W][2];
-#pragma unroll
-    for (int d = 0; d < W; ++d)
-#pragma unroll
-        for (int b = 0; b < 2; ++b)
-#pragma unroll
-            for (int c = 0; c < 2; ++c) {
-                if (d == C0 || d == C0 + 1) {
-                    X[d][b][c] = Z[d - C0][b][C0 + c];
-                    Y[b][d][c] = Z[b][d - C0][C0 + c];
-                } else {
-                    X[d][b][c] = __ldg(phi + xo[d] + yo[C0 + b] + kc[C0 + c]);
-                    Y[b][d][c] = __ldg(phi + xo[C0 + b] + yo[d] + kc[C0 + c]);
-                }
-            }
+    using St = Stencil<ORDER, POW2>;
+    constexpr int W = St::W, C0 = St::C0;
+    const St s(phi, n, i, j, k);
     const float w0[2] = {1.0f - tx, tx}, w1[2] = {1.0f - ty, ty}, w2[2] = {1.0f - tz, tz};
-    // centred difference at slot s (offset s - C0) of a stencil line v
-    auto D = [](const float* v, int s) {
-        return ORDER == 4 ? (8.0f * (v[s - 1] - v[s + 1]) - (v[s - 2] - v[s + 2])) * (1.0f / 12.0f)
-                          : (v[s - 1] - v[s + 1]) * 0.5f;
-    };
     gx = gy = gz = 0.0f;
 #pragma unroll
     for (int b = 0; b < 2; ++b)
@@ -296,17 +317,18 @@ __device__ __forceinline__ void force_at(const float* __restrict__ phi, int n, i
             float lx[W], ly[W];
 #pragma unroll
             for (int d = 0; d < W; ++d) {
-                lx[d] = X[d][b][c];
-                ly[d] = Y[b][d][c];
+                lx[d] = s.X[d][b][c];
+                ly[d] = s.Y[b][d][c];
             }
-            gx += w1[b] * w2[c] * (w0[0] * D(lx, C0) + w0[1] * D(lx, C0 + 1));
+            gx += w1[b] * w2[c] * (w0[0] * St::D(lx, C0) + w0[1] * St::D(lx, C0 + 1));
             // for y the roles are (a = b here, c): weights w0[a] w2[c]
-            gy += w0[b] * w2[c] * (w1[0] * D(ly, C0) + w1[1] * D(ly, C0 + 1));
+            gy += w0[b] * w2[c] * (w1[0] * St::D(ly, C0) + w1[1] * St::D(ly, C0 + 1));
         }
 #pragma unroll
     for (int a = 0; a < 2; ++a)
 #pragma unroll
-        for (int b = 0; b < 2; ++b) gz += w0[a] * w1[b] * (w2[0] * D(Z[a][b], C0) + w2[1] * D(Z[a][b], C0 + 1));
+        for (int b = 0; b < 2; ++b)
+            gz += w0[a] * w1[b] * (w2[0] * St::D(s.Z[a][b], C0) + w2[1] * St::D(s.Z[a][b], C0 + 1));
 }
 
 template <int ORDER, bool POW2>
@@ -362,6 +384,147 @@ __global__ void __launch_bounds__(256, 4) k_kick_drift_f32(const float* __restri
             oy[p] = qb;
             oz[p] = qc;
         }
+    }
+}
+
+// ----------------------------------------------------- FP32 adjoints
+// The FP32 split-position counterparts of csrc/adjoint.cu (same algebra; no
+// counterpart in the reference).  With U(c) = scale_d dbar(c) +
+// scale_u sum_a u_pa f_a(c), f_a = -G_a phi computed from phi at the corner
+// as in force_at, the particle adjoint is xbar_p += sum_c grad W(x_p - c) U(c);
+// grad W replaces one factor of the CIC weight by its derivative (-1, +1).
+template <int ORDER, bool POW2>
+__global__ void __launch_bounds__(256) k_adjoint_gather_f32(
+    const uint32_t* __restrict__ cell, const float* __restrict__ ox, const float* __restrict__ oy,
+    const float* __restrict__ oz, long long np, const float* __restrict__ dbar, float scale_d,
+    const float* __restrict__ phi, const float* __restrict__ ux, const float* __restrict__ uy,
+    const float* __restrict__ uz, float scale_u, float* __restrict__ bx, float* __restrict__ by,
+    float* __restrict__ bz, int n) {
+    const unsigned pz = (unsigned)n + 2u, plane = (unsigned)n * pz;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np;
+         p += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        unpack_cell(__ldg(cell + p), i, j, k);
+        const float tx = __ldg(ox + p), ty = __ldg(oy + p), tz = __ldg(oz + p);
+        float U[2][2][2] = {};
+        if (dbar) {
+            const unsigned x0 = (unsigned)i * plane, x1 = (unsigned)wrap_near<POW2>(i + 1, n) * plane;
+            const unsigned y0 = (unsigned)j * pz, y1 = (unsigned)wrap_near<POW2>(j + 1, n) * pz;
+            const unsigned z0 = (unsigned)k, z1 = (unsigned)wrap_near<POW2>(k + 1, n);
+            const unsigned xs[2] = {x0, x1}, ys[2] = {y0, y1}, zs[2] = {z0, z1};
+#pragma unroll
+            for (int a = 0; a < 2; ++a)
+#pragma unroll
+                for (int b = 0; b < 2; ++b)
+#pragma unroll
+                    for (int c = 0; c < 2; ++c) U[a][b][c] = scale_d * __ldg(dbar + xs[a] + ys[b] + zs[c]);
+        }
+        if (phi) {
+            const float u0 = scale_u * __ldg(ux + p), u1 = scale_u * __ldg(uy + p), u2 = scale_u * __ldg(uz + p);
+            const Stencil<ORDER, POW2> st(phi, n, i, j, k);
+#pragma unroll
+            for (int a = 0; a < 2; ++a)
+#pragma unroll
+                for (int b = 0; b < 2; ++b)
+#pragma unroll
+                    for (int c = 0; c < 2; ++c) {
+                        float fx, fy, fz;
+                        st.corner(a, b, c, fx, fy, fz);
+                        U[a][b][c] += u0 * fx + u1 * fy + u2 * fz;
+                    }
+        }
+        const float w0[2] = {1.0f - tx, tx}, w1[2] = {1.0f - ty, ty}, w2[2] = {1.0f - tz, tz};
+        const float dw[2] = {-1.0f, 1.0f};
+        float gx = 0.0f, gy = 0.0f, gz = 0.0f;
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+            for (int b = 0; b < 2; ++b)
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    gx += dw[a] * w1[b] * w2[c] * U[a][b][c];
+                    gy += w0[a] * dw[b] * w2[c] * U[a][b][c];
+                    gz += w0[a] * w1[b] * dw[c] * U[a][b][c];
+                }
+        bx[p] += gx;
+        by[p] += gy;
+        bz[p] += gz;
+    }
+}
+
+// ub_a(c) += sum_p u_pa W(x_p - c) into three unpadded [n][n][n] meshes.
+template <bool POW2>
+__global__ void k_deposit3_f32(const uint32_t* __restrict__ cell, const float* __restrict__ ox,
+                               const float* __restrict__ oy, const float* __restrict__ oz,
+                               const float* __restrict__ ux, const float* __restrict__ uy,
+                               const float* __restrict__ uz, long long np, float* __restrict__ o0,
+                               float* __restrict__ o1, float* __restrict__ o2, int n) {
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np;
+         p += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        unpack_cell(__ldg(cell + p), i, j, k);
+        const float tx = __ldg(ox + p), ty = __ldg(oy + p), tz = __ldg(oz + p);
+        const float w0[2] = {1.0f - tx, tx}, w1[2] = {1.0f - ty, ty}, w2[2] = {1.0f - tz, tz};
+        const float u[3] = {__ldg(ux + p), __ldg(uy + p), __ldg(uz + p)};
+        const unsigned xs[2] = {(unsigned)i * n * n, (unsigned)wrap_near<POW2>(i + 1, n) * n * n};
+        const unsigned ys[2] = {(unsigned)j * n, (unsigned)wrap_near<POW2>(j + 1, n) * n};
+        const unsigned zs[2] = {(unsigned)k, (unsigned)wrap_near<POW2>(k + 1, n)};
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+            for (int b = 0; b < 2; ++b)
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    const unsigned o = xs[a] + ys[b] + zs[c];
+                    const float w = w0[a] * w1[b] * w2[c];
+                    atomicAdd(o0 + o, w * u[0]);
+                    atomicAdd(o1 + o, w * u[1]);
+                    atomicAdd(o2 + o, w * u[2]);
+                }
+    }
+}
+
+// phibar = -sum_a G_a ub_a on the padded mesh (padding zeroed); G_a the
+// 2- or 4-point centred difference of the forward gradient.
+template <int ORDER, bool POW2>
+__global__ void k_neg_divergence_f32(const float* __restrict__ u0, const float* __restrict__ u1,
+                                     const float* __restrict__ u2, float* __restrict__ out, int n) {
+    for (long long row = blockIdx.x; row < (long long)n * n; row += gridDim.x) {
+        const int i = (int)(row / n), j = (int)(row % n);
+        auto R = [&](const float* g, int a, int b) {
+            return g + ((long long)wrap_near<POW2>(a, n) * n + wrap_near<POW2>(b, n)) * n;
+        };
+        const float *xm1 = R(u0, i - 1, j), *xp1 = R(u0, i + 1, j), *xm2 = R(u0, i - 2, j), *xp2 = R(u0, i + 2, j);
+        const float *ym1 = R(u1, i, j - 1), *yp1 = R(u1, i, j + 1), *ym2 = R(u1, i, j - 2), *yp2 = R(u1, i, j + 2);
+        const float* zc = R(u2, i, j);
+        float* o = out + row * (n + 2);
+        for (int k = threadIdx.x; k < n + 2; k += blockDim.x) {
+            if (k >= n) {
+                o[k] = 0.0f;
+                continue;
+            }
+            const int km1 = wrap_near<POW2>(k - 1, n), kp1 = wrap_near<POW2>(k + 1, n);
+            const int km2 = wrap_near<POW2>(k - 2, n), kp2 = wrap_near<POW2>(k + 2, n);
+            float g;
+            if (ORDER == 4)
+                g = (8.0f * (xm1[k] - xp1[k]) - (xm2[k] - xp2[k])) * (1.0f / 12.0f) +
+                    (8.0f * (ym1[k] - yp1[k]) - (ym2[k] - yp2[k])) * (1.0f / 12.0f) +
+                    (8.0f * (zc[km1] - zc[kp1]) - (zc[km2] - zc[kp2])) * (1.0f / 12.0f);
+            else
+                g = (xm1[k] - xp1[k]) * 0.5f + (ym1[k] - yp1[k]) * 0.5f + (zc[km1] - zc[kp1]) * 0.5f;
+            o[k] = -g;
+        }
+    }
+}
+
+__global__ void k_axpy3_f32(float* __restrict__ y0, float* __restrict__ y1, float* __restrict__ y2,
+                            const float* __restrict__ x0, const float* __restrict__ x1,
+                            const float* __restrict__ x2, float a, long long np) {
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np;
+         p += (long long)gridDim.x * blockDim.x) {
+        y0[p] += a * x0[p];
+        y1[p] += a * x1[p];
+        y2[p] += a * x2[p];
     }
 }
 
@@ -482,6 +645,70 @@ int kick_drift_f32(const Plan& p, const float* phi, uint32_t* cell, float* ox, f
         else
             k_kick_drift_f32<2, false><<<g, kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz, np, ck, dt, p.ng);
     }
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+// ------------------------------------------------------- FP32 adjoints
+int adjoint_gather_f32(const Plan& p, const uint32_t* cell, const float* ox, const float* oy, const float* oz,
+                       int64_t np, const float* dbar, double scale_d, const float* phi, const float* u[3],
+                       double scale_u, float* xbar[3]) {
+    if (np == 0) return PM_OK;
+    {
+        Timed t(p, ST_ADJOINT);
+        const unsigned g = grid_for(p, np, kThreads);
+        const bool pow2 = (p.ng & (p.ng - 1)) == 0;
+        const float* u0 = u ? u[0] : nullptr;
+        const float* u1 = u ? u[1] : nullptr;
+        const float* u2 = u ? u[2] : nullptr;
+#define PMB_ADJ_G(O, P2)                                                                                   \
+    k_adjoint_gather_f32<O, P2><<<g, kThreads, 0, p.stream>>>(cell, ox, oy, oz, np, dbar, (float)scale_d, phi, \
+                                                              u0, u1, u2, (float)scale_u, xbar[0], xbar[1],  \
+                                                              xbar[2], p.ng)
+        if (p.grad_order == 4 && pow2) PMB_ADJ_G(4, true);
+        else if (p.grad_order == 4) PMB_ADJ_G(4, false);
+        else if (pow2) PMB_ADJ_G(2, true);
+        else PMB_ADJ_G(2, false);
+#undef PMB_ADJ_G
+    }
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+int adjoint_mesh_source_f32(const Plan& p, const uint32_t* cell, const float* ox, const float* oy,
+                            const float* oz, const float* u[3], int64_t np, float* ub[3], float* phibar) {
+    const size_t cells = (size_t)p.ng * p.ng * p.ng;
+    for (int a = 0; a < 3; ++a) PMB_CUDA_CHECK(cudaMemsetAsync(ub[a], 0, cells * sizeof(float), p.stream));
+    {
+        Timed t(p, ST_ADJOINT, 2);
+        const bool pow2 = (p.ng & (p.ng - 1)) == 0;
+        if (np > 0) {
+            const unsigned g = grid_for(p, np, kThreads);
+            if (pow2)
+                k_deposit3_f32<true><<<g, kThreads, 0, p.stream>>>(cell, ox, oy, oz, u[0], u[1], u[2], np, ub[0],
+                                                                    ub[1], ub[2], p.ng);
+            else
+                k_deposit3_f32<false><<<g, kThreads, 0, p.stream>>>(cell, ox, oy, oz, u[0], u[1], u[2], np, ub[0],
+                                                                     ub[1], ub[2], p.ng);
+        }
+        const unsigned gr = grid_for(p, (long long)p.ng * p.ng, 1);
+        if (p.grad_order == 4 && pow2)
+            k_neg_divergence_f32<4, true><<<gr, kThreads, 0, p.stream>>>(ub[0], ub[1], ub[2], phibar, p.ng);
+        else if (p.grad_order == 4)
+            k_neg_divergence_f32<4, false><<<gr, kThreads, 0, p.stream>>>(ub[0], ub[1], ub[2], phibar, p.ng);
+        else if (pow2)
+            k_neg_divergence_f32<2, true><<<gr, kThreads, 0, p.stream>>>(ub[0], ub[1], ub[2], phibar, p.ng);
+        else
+            k_neg_divergence_f32<2, false><<<gr, kThreads, 0, p.stream>>>(ub[0], ub[1], ub[2], phibar, p.ng);
+    }
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+int axpy3_f32(const Plan& p, float* y[3], const float* x[3], double a, int64_t np) {
+    if (np == 0) return PM_OK;
+    k_axpy3_f32<<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(y[0], y[1], y[2], x[0], x[1], x[2], (float)a,
+                                                                       np);
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;
 }

@@ -120,7 +120,8 @@ struct Plan {
     int* d_err = nullptr;           // device error bits
     void* mesh = nullptr;           // workspace mesh [ng][ng][ng+2]
     void* force[3] = {nullptr, nullptr, nullptr};  // FP64 force arrays
-    void* adj[3] = {nullptr, nullptr, nullptr};    // FP64 adjoint source arrays (deposited u)
+    void* adj[3] = {nullptr, nullptr, nullptr};    // adjoint source arrays (deposited u), plan precision
+    void* adjm = nullptr;                          // FP32 adjoint: the second padded mesh (psi)
     size_t bytes = 0;
     StageTimers* timers = nullptr;  // owned by the C-ABI plan object
     TileScratch tiles;
@@ -132,9 +133,9 @@ struct Timed {
     const Plan& p;
     int st;
     cudaEvent_t a = nullptr;
-    Timed(const Plan& plan, int stage) : p(plan), st(stage) {
+    Timed(const Plan& plan, int stage, int nlaunch = 1) : p(plan), st(stage) {
         if (!p.timers) return;
-        p.timers->launches[st]++;
+        p.timers->launches[st] += nlaunch;
         if (p.timers->on) {
             a = p.timers->get();
             cudaEventRecord(a, p.stream);
@@ -207,6 +208,12 @@ int adjoint_gather_f64(const Plan& p, const double* x, const double* y, const do
 int adjoint_mesh_source_f64(const Plan& p, const double* x, const double* y, const double* z, const double* u[3],
                             int64_t np, double* ub[3], double* phibar);
 int axpy3_f64(const Plan& p, double* y[3], const double* x[3], double a, int64_t np);
+int adjoint_gather_f32(const Plan& p, const uint32_t* cell, const float* ox, const float* oy, const float* oz,
+                       int64_t np, const float* dbar, double scale_d, const float* phi, const float* u[3],
+                       double scale_u, float* xbar[3]);
+int adjoint_mesh_source_f32(const Plan& p, const uint32_t* cell, const float* ox, const float* oy,
+                            const float* oz, const float* u[3], int64_t np, float* ub[3], float* phibar);
+int axpy3_f32(const Plan& p, float* y[3], const float* x[3], double a, int64_t np);
 
 // Zel'dovich initial conditions (ic.cu); p is an FP64 plan of size nrow.
 int ic_zeldovich(const Plan& p, double n_s, double rms_cells, uint64_t seed, double vel_factor, int ng,

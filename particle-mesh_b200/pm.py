@@ -291,6 +291,34 @@ class Plan:
         check(self.lib.pm_step_f32(self._h, _vp(cell), *(_vp(t) for t in off), *(_vp(t) for t in vel), np_,
                                    float(mass), float(c_poisson), float(c_kick), float(dt)))
 
+    # ------------------------------------------- FP32 split-position adjoints
+    def _adj_arrays(self, arrays, np_):
+        for t in arrays:
+            _need(t, torch.float32, np_, name="adjoint array")
+
+    def adjoint_deposit_split(self, cell, off, mass: float, dbar, xbar):
+        """xbar += (d delta / d x)^T dbar at the split positions (FP32)."""
+        np_ = self._split_args(cell, off)
+        self._adj_arrays(xbar, np_)
+        check(self.lib.pm_adjoint_deposit_f32(self._h, _vp(cell), *(_vp(t) for t in off), np_, float(mass),
+                                              _vp(self._mesh(dbar, "dbar")), *(_vp(t) for t in xbar)))
+
+    def adjoint_force_split(self, cell, off, mass: float, c_poisson: float, u, scale: float, xbar):
+        """xbar += scale (dF/dx)^T u, F the FP32 step's forces at the split positions."""
+        np_ = self._split_args(cell, off)
+        self._adj_arrays((*u, *xbar), np_)
+        check(self.lib.pm_adjoint_force_f32(self._h, _vp(cell), *(_vp(t) for t in off), np_, float(mass),
+                                            float(c_poisson), *(_vp(t) for t in u), float(scale),
+                                            *(_vp(t) for t in xbar)))
+
+    def step_adjoint_split(self, cell, off, mass: float, c_poisson: float, c_kick: float, dt: float, xbar, vbar):
+        """The adjoint of one step_split started from (cell, off): (xbar, vbar) in/out."""
+        np_ = self._split_args(cell, off)
+        self._adj_arrays((*xbar, *vbar), np_)
+        check(self.lib.pm_step_adjoint_f32(self._h, _vp(cell), *(_vp(t) for t in off), np_, float(mass),
+                                           float(c_poisson), float(c_kick), float(dt), *(_vp(t) for t in xbar),
+                                           *(_vp(t) for t in vbar)))
+
 
 def _wrap_device_ptr(ptr: int, shape, dtype, device, nbytes: int) -> torch.Tensor:
     """A tensor view of device memory owned by a plan (valid while it lives)."""

@@ -1,4 +1,5 @@
-"""torch.autograd.Function over the C ABI's FP64 step and its adjoints.
+"""torch.autograd.Function over the C ABI's steps and their adjoints (FP64,
+and FP32 with split positions).
 
 Differentiable PM run: particles on the lattice q are displaced by psi (one
 3-vector per particle, cell units) with velocities vel_factor * psi, advanced
@@ -70,3 +71,57 @@ class PMLoss(torch.autograd.Function):
 
 def loss_fn(psi, q, plan, ng, mass, c_poisson, dt, steps, target, vel_factor=1.0, ckpt=8):
     return PMLoss.apply(psi, q, plan, ng, mass, c_poisson, dt, steps, target, vel_factor, ckpt)
+
+
+class PMLossSplit(torch.autograd.Function):
+    """The same differentiable run on the FP32 split-position path
+    (pm_step_f32, pm_adjoint_deposit_f32, pm_step_adjoint_f32).  psi, q and
+    the target are FP64 tensors; the state, the mesh and the adjoint arrays
+    are FP32, the loss and the returned gradient FP64."""
+
+    @staticmethod
+    def forward(ctx, psi, q, plan, ng, mass, c_poisson, dt, steps, target, vel_factor, ckpt):
+        sched = kdk_schedule(steps, dt)
+        cell, off = plan.split(*[wrap(q[a] + psi[a], ng).contiguous() for a in range(3)])
+        v = [(vel_factor * psi[a]).float().contiguous() for a in range(3)]
+        ckpts = {}
+        for s, (ck, dd) in enumerate(sched[:-1]):
+            if s % ckpt == 0:
+                ckpts[s] = (cell.clone(), [t.clone() for t in off], [t.clone() for t in v])
+            plan.step_split(cell, off, v, mass, c_poisson, ck, dd)
+        delta = plan.deposit_split(cell, off, mass)
+        diff = delta[:, :, :ng].double() - target
+        loss = (diff * diff).mean()
+        ctx.save_for_backward(psi)
+        ctx.plan, ctx.ng, ctx.mass, ctx.cp, ctx.sched, ctx.ckpts = plan, ng, mass, c_poisson, sched, ckpts
+        ctx.final, ctx.diff, ctx.vel_factor, ctx.ckpt = (cell, off), diff, vel_factor, ckpt
+        return loss
+
+    @staticmethod
+    def backward(ctx, gloss):
+        plan, n, mass, cp, sched = ctx.plan, ctx.ng, ctx.mass, ctx.cp, ctx.sched
+        cell, off = ctx.final
+        dbar = torch.zeros((n, n, n + 2), dtype=torch.float32, device=gloss.device)
+        dbar[:, :, :n] = (ctx.diff * (2.0 / n ** 3) * gloss).float()
+        xb = [torch.zeros_like(off[0]) for _ in range(3)]
+        vb = [torch.zeros_like(off[0]) for _ in range(3)]
+        plan.adjoint_deposit_split(cell, off, mass, dbar, xb)
+        nsteps = len(sched) - 1
+        for a in reversed(sorted(ctx.ckpts)):
+            b = min(a + ctx.ckpt, nsteps)
+            c0, o0, v0 = ctx.ckpts[a]
+            c, o, v = c0.clone(), [t.clone() for t in o0], [t.clone() for t in v0]
+            states = []
+            for s in range(a, b):
+                states.append((c.clone(), [t.clone() for t in o]))
+                ck, dd = sched[s]
+                plan.step_split(c, o, v, mass, cp, ck, dd)
+            for s in reversed(range(a, b)):
+                ck, dd = sched[s]
+                plan.step_adjoint_split(*states[s - a], mass, cp, ck, dd, xb, vb)
+        grad = torch.stack([xb[a].double() + ctx.vel_factor * vb[a].double() for a in range(3)])
+        return grad, None, None, None, None, None, None, None, None, None, None
+
+
+def loss_fn_split(psi, q, plan, ng, mass, c_poisson, dt, steps, target, vel_factor=1.0, ckpt=8):
+    return PMLossSplit.apply(psi, q, plan, ng, mass, c_poisson, dt, steps, target, vel_factor, ckpt)

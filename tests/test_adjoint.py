@@ -1,9 +1,11 @@
-"""Hand-written adjoints of the FP64 step, checked against central finite
-differences: dot-product tests of each vector-Jacobian product, and the full
-gradient of a differentiable PM run (loss = MSE between the final CIC density
-and a target density from a second seed) with respect to the initial
+"""Hand-written adjoints of the step, checked against central finite
+differences: dot-product tests of each FP64 vector-Jacobian product, and the
+full gradient of a differentiable PM run (loss = MSE between the final CIC
+density and a target density from a second seed) with respect to the initial
 displacement field, through the checkpointed torch.autograd.Function of
-tests/pm_autograd.py."""
+tests/pm_autograd.py.  The FP32 split-position adjoints are checked against
+the FP64 ones (per product and for the whole run) and against the same finite
+differences."""
 import numpy as np
 import pytest
 
@@ -116,3 +118,85 @@ def test_run_gradient_matches_finite_differences(pmpkg, O, ng, nrow, steps, dt, 
     fd, ad = np.array(fd), np.array(ad)
     err = np.linalg.norm(fd - ad) / np.linalg.norm(fd)
     assert err < 1e-4, (err, fd[:5], ad[:5])
+
+
+# ---------------------------------------------------- FP32 split positions
+@pytest.mark.parametrize("ng,kind,order", [(32, "discrete", 2), (64, "spectral", 4)])
+def test_adjoint_f32_products_match_f64(pmpkg, ng, kind, order):
+    """pm_adjoint_deposit_f32 / pm_adjoint_force_f32 against the FP64
+    products at the same positions (FP32 arithmetic: relative L2 < 1e-4)."""
+    np_ = 4 * ng ** 3 // 8
+    rng = np.random.default_rng(ng)
+    x = [T(rng.uniform(0, ng, np_)) for _ in range(3)]
+    u = [T(rng.standard_normal(np_)) for _ in range(3)]
+    p64, p32 = pmpkg.Plan(ng, "fp64", kind, order), pmpkg.Plan(ng, "fp32", kind, order)
+    cell, off = p32.split(*x)
+    x = p32.join(cell, off)  # the FP64 side at exactly the FP32 positions
+    mass, cp = ng ** 3 / np_, 4 * np.pi
+    dbar = torch.zeros((ng, ng, ng + 2), dtype=torch.float64, device=DEV)
+    dbar[:, :, :ng] = torch.randn((ng, ng, ng), dtype=torch.float64, device=DEV)
+
+    def rel(a, b):
+        a, b = torch.stack(a).double(), torch.stack(b)
+        return float((a - b).norm() / b.norm())
+
+    b64 = [torch.zeros_like(x[0]) for _ in range(3)]
+    b32 = [torch.zeros(np_, dtype=torch.float32, device=DEV) for _ in range(3)]
+    p64.adjoint_deposit(*x, mass, dbar, b64)
+    p32.adjoint_deposit_split(cell, off, mass, dbar.float(), b32)
+    assert rel(b32, b64) < 1e-5
+    b64 = [torch.zeros_like(x[0]) for _ in range(3)]
+    b32 = [torch.zeros(np_, dtype=torch.float32, device=DEV) for _ in range(3)]
+    p64.adjoint_force(*x, mass, cp, u, 0.7, b64)
+    p32.adjoint_force_split(cell, off, mass, cp, [t.float() for t in u], 0.7, b32)
+    assert rel(b32, b64) < 1e-4
+
+
+def test_run_gradient_f32_matches_f64_and_finite_differences(pmpkg, O):
+    """The differentiable-PM configuration on the FP32 path (128^3 on 128^3,
+    32 KDK steps at dt = 0.01, checkpoint every 8): the FP32 gradient against
+    the FP64 adjoint gradient of the same run (relative L2 < 1e-3) and
+    against central differences of the FP64 loss on 64 random components
+    (relative L2 < 1e-3)."""
+    from pm_autograd import kdk_schedule, loss_fn, loss_fn_split
+
+    ng = nrow = 128
+    steps, dt, ckpt = 32, 0.01, 8
+    psi0 = O.zeldovich_displacement(nrow, -2.0, seed=11)
+    rms = np.sqrt(np.mean(np.sum(psi0 * psi0, axis=0)))
+    psi_np = (psi0 * (0.5 / rms)).reshape(3, -1)
+    q = lattice(ng, nrow)
+    mass, cp = ng ** 3 / nrow ** 3, 4 * np.pi
+    p64 = pmpkg.Plan(ng, "fp64", "spectral", 4)
+    p32 = pmpkg.Plan(ng, "fp32", "spectral", 4)
+    tpos, tvel = O.zeldovich_ic(ng, nrow, -2.0, 0.5, seed=12)
+    tx, tv = [T(a) for a in tpos], [T(a) for a in tvel]
+    for ck, dd in kdk_schedule(steps, dt)[:-1]:
+        p64.step(*tx, *tv, mass, cp, ck, dd)
+    target = p64.deposit(*tx, mass)[:, :, :ng].clone()
+
+    psi64 = T(psi_np).requires_grad_(True)
+    loss_fn(psi64, q, p64, ng, mass, cp, dt, steps, target, 1.0, ckpt).backward()
+    psi32 = T(psi_np).requires_grad_(True)
+    l32 = loss_fn_split(psi32, q, p32, ng, mass, cp, dt, steps, target, 1.0, ckpt)
+    l32.backward()
+    g64, g32 = psi64.grad.detach(), psi32.grad.detach()
+    assert torch.isfinite(g32).all()
+    e_adj = float((g32 - g64).norm() / g64.norm())
+    assert e_adj < 1e-3, e_adj
+
+    rng = np.random.default_rng(13)
+    comps = [(int(rng.integers(3)), int(rng.integers(nrow ** 3))) for _ in range(64)]
+    eps, fd, ad = 1e-5, [], []
+    with torch.no_grad():
+        for a, p in comps:
+            base = psi64.detach().clone()
+            base[a, p] += eps
+            lp = float(loss_fn(base, q, p64, ng, mass, cp, dt, steps, target, 1.0, ckpt))
+            base[a, p] -= 2 * eps
+            lm = float(loss_fn(base, q, p64, ng, mass, cp, dt, steps, target, 1.0, ckpt))
+            fd.append((lp - lm) / (2 * eps))
+            ad.append(float(g32[a, p]))
+    fd, ad = np.array(fd), np.array(ad)
+    e_fd = np.linalg.norm(fd - ad) / np.linalg.norm(fd)
+    assert e_fd < 1e-3, (e_fd, fd[:5], ad[:5])
