@@ -16,6 +16,8 @@ over every particle; particle-updates/s = particles x steps / time.
   roofline   dominant kernel, algorithmic bytes / CUDA-event time, vs the
              measured HBM copy bandwidth
   cpu_baseline the reference's CPU code on a bounded sample (rank 0, N = 1)
+  accuracy   FP32 vs FP64 after the configuration's 50 KDK steps (positions,
+             velocities, density) and FP64-summed mass / momentum drift
   adjoint    adjoint step vs forward step at 128^3 (FP32 split path; FP64 check
              path under "fp64")
 
@@ -43,6 +45,7 @@ METRIC = "PM particle-updates/s, 512^3 on 1024^3 mesh: FP32 vs FP64 at force err
 UNIT = "particle-updates/s"
 N_S, RMS, DT, SEED = -1.5, 1.0, 0.005, 1000
 CPU_SAMPLE = (256, 128)  # (mesh, particles per side): 1/64 of the workload
+ACC_STEPS = 50  # the mixed-precision configuration's run length
 
 
 def parse():
@@ -58,20 +61,21 @@ def parse():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-ensemble", action="store_true")
     ap.add_argument("--skip-adjoint", action="store_true")
+    ap.add_argument("--skip-accuracy", action="store_true")
     ap.add_argument("--ensemble-boxes", type=int, default=256)
     return ap.parse_args()
 
 
 # ---------------------------------------------------------------- clocks
 class ClockSampler:
-    """nvidia-smi samples every 200 ms while the timed region runs."""
+    """nvidia-smi samples every 100 ms while the timed region runs."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, bus_id=None):
-        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"]
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100"]
         if bus_id:
             cmd += ["-i", bus_id]
         try:
@@ -377,6 +381,58 @@ def ours(args):
         del p64, x, y, z, pv
         torch.cuda.empty_cache()
 
+    # ---- accuracy of the FP32 split path against the FP64 path over the
+    # configuration's own run: 50 leapfrog KDK steps at dt = 0.005 from the
+    # same initial state (half kicks merged; 51 force evaluations)
+    accuracy = None
+    if not args.skip_fp64 and not args.skip_accuracy:
+        nsteps = ACC_STEPS
+        sched = [(0.5 * DT if s in (0, nsteps) else DT, DT if s < nsteps else 0.0) for s in range(nsteps + 1)]
+        c32, o32 = p32.split(*pos)
+        w32 = [a.float() for a in vel]
+        x64 = [a.clone() for a in pos]
+        w64 = [a.clone() for a in vel]
+        p64 = pm.Plan(ng, "fp64", "spectral", 4, stream=stream, device=dev)
+        m0_32 = p32.conserved(None, w32, mass)["momentum"]
+        m0_64 = p64.conserved(None, w64, mass)["momentum"]
+        scale = mass * float(sum(a.abs().sum() for a in vel))
+        for ckk, dd in sched:
+            p32.step_split(c32, o32, w32, mass, cp, ckk, dd)
+            p64.step(*x64, *w64, mass, cp, ckk, dd)
+        p32.check()
+        p64.check()
+        xj = p32.join(c32, o32)
+        d2, dmax = 0.0, 0.0
+        for a, b in zip(xj, x64):
+            d = torch.remainder(a - b + 0.5 * ng, float(ng)) - 0.5 * ng
+            d2 += float((d * d).sum())
+            dmax = max(dmax, float(d.abs().max()))
+        vnum = sum(float(((a.double() - b) ** 2).sum()) for a, b in zip(w32, w64))
+        vden = sum(float((b ** 2).sum()) for b in w64)
+        dens32 = p32.deposit_split(c32, o32, mass, p32.workspace_mesh())
+        c_32 = p32.conserved(dens32, w32, mass)
+        dens32 = dens32[:, :, :ng].double()
+        dens64 = p64.deposit(*x64, mass)
+        c_64 = p64.conserved(dens64, w64, mass)
+        dens64 = dens64[:, :, :ng]
+        dnum = float(((dens32 - dens64) ** 2).sum())
+        dden = float(((dens64 + 1.0) ** 2).sum())
+        accuracy = {"steps": nsteps, "dt": DT, "schedule": "leapfrog KDK, half kicks merged",
+                    "force_rel_l2_initial": force_err,
+                    "position_err_rms_cells": math.sqrt(d2 / (3 * np_)), "position_err_max_cells": dmax,
+                    "velocity_rel_l2": math.sqrt(vnum / vden),
+                    "density_rel_l2": math.sqrt(dnum / dden),
+                    "mass_rel_err": {"fp32": c_32["mass"] / (mass * np_) - 1.0,
+                                     "fp64": c_64["mass"] / (mass * np_) - 1.0},
+                    "momentum_drift_rel": {
+                        "fp32": max(abs(a - b) for a, b in zip(c_32["momentum"], m0_32)) / scale,
+                        "fp64": max(abs(a - b) for a, b in zip(c_64["momentum"], m0_64)) / scale},
+                    "note": "FP32 vs FP64 from the same seed; mass and momentum summed in FP64 on the device; "
+                            "density error relative to the FP64 density 1 + delta"}
+        p64.close()
+        del p64, x64, w64, c32, o32, w32, xj, dens32, dens64
+        torch.cuda.empty_cache()
+
     # ---- adjoint step vs forward step, differentiable-PM configuration
     # (128^3 on 128^3; the FP32 split path is the configuration's own, FP64
     # its check path)
@@ -402,18 +458,18 @@ def ours(args):
                     "with_recompute_over_forward": (t_a + t_f) / t_f}
 
         p32a = pm.Plan(na, "fp32", "spectral", 4, stream=stream, device=dev)
-        cell, off = p32a.split(*pa)
-        v32 = [a.float().contiguous() for a in va]
-        cs, os_, vs32 = cell.clone(), [a.clone() for a in off], [a.clone() for a in v32]
-        xb32 = [torch.randn_like(off[0]) for _ in range(3)]
-        vb32 = [torch.randn_like(off[0]) for _ in range(3)]
+        acell, aoff = p32a.split(*pa)
+        av32 = [a.float().contiguous() for a in va]
+        cs, os_, vs32 = acell.clone(), [a.clone() for a in aoff], [a.clone() for a in av32]
+        xb32 = [torch.randn_like(aoff[0]) for _ in range(3)]
+        vb32 = [torch.randn_like(aoff[0]) for _ in range(3)]
         t_f32 = timed(lambda: p32a.step_split(cs, os_, vs32, 1.0, cp, 0.01, 0.01))
-        t_a32 = timed(lambda: p32a.step_adjoint_split(cell, off, 1.0, cp, 0.01, 0.01, xb32, vb32))
+        t_a32 = timed(lambda: p32a.step_adjoint_split(acell, aoff, 1.0, cp, 0.01, 0.01, xb32, vb32))
         adjoint = leg(t_f32, t_a32, "FP32 split positions")
         adjoint["note"] = ("adjoint step = force recomputation at the step's start + transposed pairs; "
                            "checkpointed backprop also re-runs each forward step once")
         p32a.close()
-        del p32a, cell, off, v32, cs, os_, vs32, xb32, vb32
+        del p32a, acell, aoff, av32, cs, os_, vs32, xb32, vb32
         if not args.skip_fp64:
             pla = pm.Plan(na, "fp64", "spectral", 4, stream=stream, device=dev)
             xb = [torch.randn_like(pa[0]) for _ in range(3)]
@@ -540,7 +596,7 @@ def ours(args):
                        "parallelism": f"{world} independent boxes, one per GPU"},
             "fp64": fp64, "force_err": force_err,
             "speedup_fp32_vs_fp64": (value / fp64["value"]) if fp64 else None,
-            "e2e": e2e, "adjoint": adjoint, "ensemble": ensemble, "gpu_launches": launches, "roofline": roofline, "stages": per_stage,
+            "e2e": e2e, "accuracy": accuracy, "adjoint": adjoint, "ensemble": ensemble, "gpu_launches": launches, "roofline": roofline, "stages": per_stage,
             "cpu_baseline": cpu, "clocks": clocks}
     print(json.dumps(line), flush=True)
     return 0

@@ -199,6 +199,19 @@ int pm_step_adjoint_f32(pm_plan* plan, const uint32_t* cell, const float* ox, co
                         const float* oz, int64_t np, float mass, double c_poisson, double c_kick, double dt,
                         float* xbar, float* ybar, float* zbar, float* vxbar, float* vybar, float* vzbar);
 
+/* ------------------------------------------- FP64 reductions (new)
+ * Conserved quantities summed in FP64 whatever the plan's precision, into
+ * the caller's device array out[4]: out[0] = sum over cells of (mesh + 1),
+ * the total mass of a density-contrast mesh (padding ignored; 0 when mesh is
+ * NULL); out[1..3] = mass * sum_p v_p, the total momentum (0 when the
+ * velocity arrays are NULL).  Deterministic: the same data give the same
+ * bits.  Asynchronous on the plan's stream.  No counterpart in the
+ * reference. */
+int pm_reduce_f32(pm_plan* plan, const float* mesh, const float* vx, const float* vy, const float* vz,
+                  int64_t np, double mass, double* out);
+int pm_reduce_f64(pm_plan* plan, const double* mesh, const double* vx, const double* vy, const double* vz,
+                  int64_t np, double mass, double* out);
+
 /* Device pointer to the plan's own mesh [ng][ng][ng+2] (density after the
  * deposit of pm_step_*, potential after it returns). */
 int pm_plan_mesh(pm_plan* plan, void** mesh);

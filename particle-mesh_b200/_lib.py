@@ -52,6 +52,8 @@ SIGNATURES = {
     "pm_interp_f32": [_V, _V, _V, _V, _V, _V, _L, _V, _V, _V],
     "pm_kick_drift_f32": [_V, _V, _V, _V, _V, _V, _V, _V, _V, _L, _D, _D],
     "pm_step_f32": [_V, _V, _V, _V, _V, _V, _V, _V, _L, _F, _D, _D, _D],
+    "pm_reduce_f32": [_V, _V, _V, _V, _V, _L, _D, _V],
+    "pm_reduce_f64": [_V, _V, _V, _V, _V, _L, _D, _V],
     "pm_adjoint_deposit_f32": [_V, _V, _V, _V, _V, _L, _F, _V, _V, _V, _V],
     "pm_adjoint_force_f32": [_V, _V, _V, _V, _V, _L, _F, _D, _V, _V, _V, _D, _V, _V, _V],
     "pm_step_adjoint_f32": [_V, _V, _V, _V, _V, _L, _F, _D, _D, _D, _V, _V, _V, _V, _V, _V],

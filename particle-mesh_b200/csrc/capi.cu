@@ -89,7 +89,8 @@ void release(Plan& p) {
     for (void*& f : p.adj)
         if (f) cudaFree(f), f = nullptr;
     if (p.adjm) cudaFree(p.adjm);
-    p.tw = p.g1d = p.mesh = p.adjm = nullptr;
+    if (p.red) cudaFree(p.red);
+    p.tw = p.g1d = p.mesh = p.adjm = p.red = nullptr;
     p.d_err = nullptr;
     delete p.timers;
     p.timers = nullptr;
@@ -602,6 +603,29 @@ int pm_step_adjoint_f32(pm_plan* plan, const uint32_t* cell, const float* ox, co
     if (dt != 0.0) PM_TRY(axpy3_f32(p, vb, xbc, dt, np));  // x' = x + dt v'  =>  vbar' += dt xbar
     if (c_kick == 0.0) return PM_OK;
     return adjoint_force_f32(p, cell, ox, oy, oz, np, mass, c_poisson, vbc, c_kick, xb);
+}
+
+// ------------------------------------------------------- FP64 reductions
+
+static int reduce_args(pm_plan* plan, int precision, const void* vx, const void* vy, const void* vz, int64_t np,
+                       const double* out) {
+    PM_TRY(check_plan(plan, precision));
+    if (!out) return fail(PM_ERR_ARG, "out is NULL");
+    if (np < 0) return fail(PM_ERR_ARG, "np must be >= 0");
+    if ((vx || vy || vz) && !(vx && vy && vz)) return fail(PM_ERR_ARG, "give all three velocity arrays or none");
+    return set_device(plan->p);
+}
+
+int pm_reduce_f32(pm_plan* plan, const float* mesh, const float* vx, const float* vy, const float* vz,
+                  int64_t np, double mass, double* out) {
+    PM_TRY(reduce_args(plan, PM_FP32, vx, vy, vz, np, out));
+    return reduce_conserved<float>(plan->p, mesh, vx, vy, vz, vx ? np : 0, mass, out);
+}
+
+int pm_reduce_f64(pm_plan* plan, const double* mesh, const double* vx, const double* vy, const double* vz,
+                  int64_t np, double mass, double* out) {
+    PM_TRY(reduce_args(plan, PM_FP64, vx, vy, vz, np, out));
+    return reduce_conserved<double>(plan->p, mesh, vx, vy, vz, vx ? np : 0, mass, out);
 }
 
 // ------------------------------------------------------------------- ICs

@@ -122,6 +122,7 @@ struct Plan {
     void* force[3] = {nullptr, nullptr, nullptr};  // FP64 force arrays
     void* adj[3] = {nullptr, nullptr, nullptr};    // adjoint source arrays (deposited u), plan precision
     void* adjm = nullptr;                          // FP32 adjoint: the second padded mesh (psi)
+    void* red = nullptr;                           // reduction partial sums (FP64)
     size_t bytes = 0;
     StageTimers* timers = nullptr;  // owned by the C-ABI plan object
     TileScratch tiles;
@@ -214,6 +215,9 @@ int adjoint_gather_f32(const Plan& p, const uint32_t* cell, const float* ox, con
 int adjoint_mesh_source_f32(const Plan& p, const uint32_t* cell, const float* ox, const float* oy,
                             const float* oz, const float* u[3], int64_t np, float* ub[3], float* phibar);
 int axpy3_f32(const Plan& p, float* y[3], const float* x[3], double a, int64_t np);
+template <typename T>
+int reduce_conserved(Plan& p, const T* mesh, const T* vx, const T* vy, const T* vz, int64_t np, double mass,
+                     double* out);
 
 // Zel'dovich initial conditions (ic.cu); p is an FP64 plan of size nrow.
 int ic_zeldovich(const Plan& p, double n_s, double rms_cells, uint64_t seed, double vel_factor, int ng,

@@ -291,6 +291,23 @@ class Plan:
         check(self.lib.pm_step_f32(self._h, _vp(cell), *(_vp(t) for t in off), *(_vp(t) for t in vel), np_,
                                    float(mass), float(c_poisson), float(c_kick), float(dt)))
 
+    # ------------------------------------------------------ FP64 reductions
+    def conserved(self, mesh=None, vel=None, mass: float = 1.0) -> dict:
+        """Total mass sum(mesh + 1) and momentum mass * sum(v), summed in FP64
+        on the device (either input may be None)."""
+        out = torch.zeros(4, dtype=torch.float64, device=self.device)
+        np_ = 0
+        if mesh is not None:
+            self._mesh(mesh)
+        if vel is not None:
+            np_ = vel[0].numel()
+            for t, nm in zip(vel, ("vx", "vy", "vz")):
+                _need(t, self.dtype, np_, name=nm)
+        fn = self.lib.pm_reduce_f64 if self.precision == "fp64" else self.lib.pm_reduce_f32
+        check(fn(self._h, _vp(mesh), *(_vp(t) for t in (vel or (None, None, None))), np_, float(mass), _vp(out)))
+        o = out.tolist()
+        return {"mass": o[0], "momentum": o[1:]}
+
     # ------------------------------------------- FP32 split-position adjoints
     def _adj_arrays(self, arrays, np_):
         for t in arrays:

@@ -356,6 +356,42 @@ def test_fused_step_matches_stagewise(pmpkg, O, ng, nrow):
     assert rel(np.stack([H(a) for a in v1]), np.stack([H(a) for a in v])) < 1e-6
 
 
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_conserved_reductions(pmpkg, O, prec):
+    """pm_reduce_*: the FP64 mesh total equals the deposited mass, the
+    momentum equals mass * sum(v) in FP64, repeated calls give identical bits,
+    and a few KDK steps conserve momentum (CIC deposit and interpolation with
+    a centred difference exert no net force)."""
+    ng, nrow = 64, 32
+    pos, vel = O.zeldovich_ic(ng, nrow, -2.0, 0.7, seed=5)
+    mass, cp, dt = ng ** 3 / nrow ** 3, 4 * np.pi, 0.05
+    plan = pmpkg.Plan(ng, prec, "spectral", 4)
+    dt_ = torch.float64 if prec == "fp64" else torch.float32
+    v = [T(a, dt_) for a in vel]
+    if prec == "fp64":
+        x = [T(a) for a in pos]
+        mesh = plan.deposit(*x, mass)
+        step = lambda: plan.step(*x, *v, mass, cp, dt, dt)  # noqa: E731
+    else:
+        cell, off = plan.split(*(T(a) for a in pos))
+        mesh = plan.deposit_split(cell, off, mass)
+        step = lambda: plan.step_split(cell, off, v, mass, cp, dt, dt)  # noqa: E731
+    c1 = plan.conserved(mesh, v, mass)
+    c2 = plan.conserved(mesh, v, mass)
+    assert c1 == c2
+    total = mass * nrow ** 3
+    assert abs(c1["mass"] - total) / total < (1e-12 if prec == "fp64" else 1e-5)
+    ref = [mass * float(t.double().sum()) for t in v]
+    scale = mass * float(sum(t.double().abs().sum() for t in v))
+    assert max(abs(a - b) for a, b in zip(c1["momentum"], ref)) < 1e-12 * scale
+    for _ in range(5):
+        step()
+    c3 = plan.conserved(None, v, mass)
+    assert c3["mass"] == 0.0
+    drift = max(abs(a - b) for a, b in zip(c3["momentum"], c1["momentum"]))
+    assert drift < (1e-9 if prec == "fp64" else 1e-5) * scale, drift / scale
+
+
 def test_split_step_kick_drift(pmpkg, O):
     ng, nrow = 64, 32
     pos, vel = O.zeldovich_ic(ng, nrow, -2.0, 0.5, seed=3)
