@@ -301,6 +301,18 @@ template <int ORDER, bool POW2> struct Stencil {
     }
 };
 
+// Cell indices of a caller-provided cell word reduced into [0, n) (a word
+// from pm_split_positions already is), so every mesh access stays in bounds.
+// Power-of-two meshes need nothing here: every index is masked where used.
+template <bool POW2>
+__device__ __forceinline__ void canon_cell(int& i, int& j, int& k, int n) {
+    if (!POW2) {
+        if (i >= n) i %= n;
+        if (j >= n) j %= n;
+        if (k >= n) k %= n;
+    }
+}
+
 template <int ORDER, bool POW2>
 __device__ __forceinline__ void force_at(const float* __restrict__ phi, int n, int i, int j, int k,
                                          float tx, float ty, float tz, float& gx, float& gy,
@@ -340,6 +352,7 @@ __global__ void __launch_bounds__(256, 4) k_interp_f32(const float* __restrict__
          p += (long long)gridDim.x * blockDim.x) {
         int i, j, k;
         unpack_cell(__ldg(cell + p), i, j, k);
+        canon_cell<POW2>(i, j, k, n);
         float gx, gy, gz;
         force_at<ORDER, POW2>(phi, n, i, j, k, __ldg(ox + p), __ldg(oy + p), __ldg(oz + p), gx, gy, gz);
         fx[p] = gx;
@@ -366,6 +379,7 @@ __global__ void __launch_bounds__(256, 4) k_kick_drift_f32(const float* __restri
          p += (long long)gridDim.x * blockDim.x) {
         int i, j, k;
         unpack_cell(cell[p], i, j, k);
+        canon_cell<POW2>(i, j, k, n);
         const float tx = ox[p], ty = oy[p], tz = oz[p];
         float gx, gy, gz;
         force_at<ORDER, POW2>(phi, n, i, j, k, tx, ty, tz, gx, gy, gz);
@@ -405,12 +419,13 @@ __global__ void __launch_bounds__(256) k_adjoint_gather_f32(
          p += (long long)gridDim.x * blockDim.x) {
         int i, j, k;
         unpack_cell(__ldg(cell + p), i, j, k);
+        canon_cell<POW2>(i, j, k, n);
         const float tx = __ldg(ox + p), ty = __ldg(oy + p), tz = __ldg(oz + p);
         float U[2][2][2] = {};
         if (dbar) {
-            const unsigned x0 = (unsigned)i * plane, x1 = (unsigned)wrap_near<POW2>(i + 1, n) * plane;
-            const unsigned y0 = (unsigned)j * pz, y1 = (unsigned)wrap_near<POW2>(j + 1, n) * pz;
-            const unsigned z0 = (unsigned)k, z1 = (unsigned)wrap_near<POW2>(k + 1, n);
+            const unsigned x0 = (unsigned)wrap_near<POW2>(i, n) * plane, x1 = (unsigned)wrap_near<POW2>(i + 1, n) * plane;
+            const unsigned y0 = (unsigned)wrap_near<POW2>(j, n) * pz, y1 = (unsigned)wrap_near<POW2>(j + 1, n) * pz;
+            const unsigned z0 = (unsigned)wrap_near<POW2>(k, n), z1 = (unsigned)wrap_near<POW2>(k + 1, n);
             const unsigned xs[2] = {x0, x1}, ys[2] = {y0, y1}, zs[2] = {z0, z1};
 #pragma unroll
             for (int a = 0; a < 2; ++a)
@@ -463,12 +478,13 @@ __global__ void k_deposit3_f32(const uint32_t* __restrict__ cell, const float* _
          p += (long long)gridDim.x * blockDim.x) {
         int i, j, k;
         unpack_cell(__ldg(cell + p), i, j, k);
+        canon_cell<POW2>(i, j, k, n);
         const float tx = __ldg(ox + p), ty = __ldg(oy + p), tz = __ldg(oz + p);
         const float w0[2] = {1.0f - tx, tx}, w1[2] = {1.0f - ty, ty}, w2[2] = {1.0f - tz, tz};
         const float u[3] = {__ldg(ux + p), __ldg(uy + p), __ldg(uz + p)};
-        const unsigned xs[2] = {(unsigned)i * n * n, (unsigned)wrap_near<POW2>(i + 1, n) * n * n};
-        const unsigned ys[2] = {(unsigned)j * n, (unsigned)wrap_near<POW2>(j + 1, n) * n};
-        const unsigned zs[2] = {(unsigned)k, (unsigned)wrap_near<POW2>(k + 1, n)};
+        const unsigned xs[2] = {(unsigned)wrap_near<POW2>(i, n) * n * n, (unsigned)wrap_near<POW2>(i + 1, n) * n * n};
+        const unsigned ys[2] = {(unsigned)wrap_near<POW2>(j, n) * n, (unsigned)wrap_near<POW2>(j + 1, n) * n};
+        const unsigned zs[2] = {(unsigned)wrap_near<POW2>(k, n), (unsigned)wrap_near<POW2>(k + 1, n)};
 #pragma unroll
         for (int a = 0; a < 2; ++a)
 #pragma unroll
