@@ -321,6 +321,41 @@ __constant__ int kColC1[kColRuns] = {4, 2, 4, 4, 4};
 
 template <int N> constexpr int zcol_threads() { return kCTRows * (N / 2) / Radix<N / 2>::R2; }
 
+// The CIC corners of one particle that land in this block's 4 x 4 columns.
+// Q: the tile it is binned in, 0 this one, bit 0 the x - 1 tile (then
+// i & 3 == 3 and only the a = 1 corners land here, in column 0), bit 1 the
+// y - 1 tile (likewise in y).  Two z cells per corner, FP32 shared atomics
+// into the padded complex rows (real index k at 2 zpad(k / 2) + k % 2).
+template <int N, int R1, int RS, int Q>
+__device__ __forceinline__ void zcol_corners(uint32_t c, float fx, float fy, float fz, float mass, float* Sf) {
+    int i, j, k;
+    unpack(c, i, j, k);
+    if (k >= N) k %= N;
+    const int k1 = (k + 1) & (N - 1);
+    const int z0 = 2 * zpad<R1>(k >> 1) + (k & 1), z1 = 2 * zpad<R1>(k1 >> 1) + (k1 & 1);
+    const float wz0 = mass * (1.0f - fz), wz1 = mass * fz;
+    auto put = [&](int ci, int cj, float w) {
+        float* row = Sf + (ci * kCT + cj) * (2 * RS);
+        atomicAdd(row + z0, w * wz0);
+        atomicAdd(row + z1, w * wz1);
+    };
+    const int li = i & (kCT - 1), lj = j & (kCT - 1);
+    if (Q == 0) {
+        put(li, lj, (1.0f - fx) * (1.0f - fy));
+        if (li < kCT - 1) put(li + 1, lj, fx * (1.0f - fy));
+        if (lj < kCT - 1) put(li, lj + 1, (1.0f - fx) * fy);
+        if (li < kCT - 1 && lj < kCT - 1) put(li + 1, lj + 1, fx * fy);
+    } else if (Q == 1) {
+        put(0, lj, fx * (1.0f - fy));
+        if (lj < kCT - 1) put(0, lj + 1, fx * fy);
+    } else if (Q == 2) {
+        put(li, 0, (1.0f - fx) * fy);
+        if (li < kCT - 1) put(li + 1, 0, fx * fy);
+    } else {
+        put(0, 0, fx * fy);
+    }
+}
+
 // Three blocks per SM (80 registers; 3 x 67.6 KB of rows at N = 1024): the
 // particle phase of one block overlaps the FFT and store phases of another.
 template <int N>
@@ -352,6 +387,10 @@ k_deposit_zr2c(const uint32_t* __restrict__ cell, const float* __restrict__ ox, 
     }
     __syncthreads();
     const uint32_t total = rpre[kColRuns];
+    // run r covers t in [rpre[r], rpre[r+1]) at perm index t + rbeg[r] - rpre[r]
+    // (unsigned wrap-around is exact); the boundaries stay in registers
+    const uint32_t p1 = rpre[1], p2 = rpre[2], p3 = rpre[3], p4 = rpre[4];
+    const uint32_t d0 = rbeg[0], d1 = rbeg[1] - p1, d2 = rbeg[2] - p2, d3 = rbeg[3] - p3, d4 = rbeg[4] - p4;
     // four particles per thread per round, their loads issued together
     constexpr int U = 4;
     for (uint32_t t0 = threadIdx.x; t0 < total; t0 += U * NTH) {
@@ -360,14 +399,15 @@ k_deposit_zr2c(const uint32_t* __restrict__ cell, const float* __restrict__ ox, 
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             const uint32_t t = t0 + u * NTH;
-            qq[u] = -1;
-            pidx[u] = 0;
-            if (t < total) {
-                int r = 0;
-                while (t >= rpre[r + 1]) ++r;
-                pidx[u] = __ldg(perm + rbeg[r] + (t - rpre[r]));
-                qq[u] = kColQ[r];
-            }
+            uint32_t d = d0;
+            int q = 0;
+            if (t >= p1) d = d1, q = 1;
+            if (t >= p2) d = d2;  // the x - 1 tile's second class, still q = 1
+            if (t >= p3) d = d3, q = 2;
+            if (t >= p4) d = d4, q = 3;
+            const bool ok = t < total;
+            pidx[u] = ok ? __ldg(perm + (t + d)) : 0u;
+            qq[u] = ok ? q : -1;
         }
         uint32_t cc[U];
         float fx[U], fy[U], fz[U];
@@ -381,31 +421,13 @@ k_deposit_zr2c(const uint32_t* __restrict__ cell, const float* __restrict__ ox, 
         }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            const int q = qq[u];
-            if (q < 0) continue;
-            int i, j, k;
-            unpack(cc[u], i, j, k);
-            if (k >= N) k %= N;
-            const int li = (i & (kCT - 1)) - ((q & 1) ? kCT : 0), lj = (j & (kCT - 1)) - ((q & 2) ? kCT : 0);
-            const float wx[2] = {1.0f - fx[u], fx[u]}, wy[2] = {1.0f - fy[u], fy[u]};
-            const float wz[2] = {mass * (1.0f - fz[u]), mass * fz[u]};
-            const int kz[2] = {k, (k + 1) & (N - 1)};
-            int zo[2];
-#pragma unroll
-            for (int c = 0; c < 2; ++c) zo[c] = 2 * zpad<R1>(kz[c] >> 1) + (kz[c] & 1);
-#pragma unroll
-            for (int a = 0; a < 2; ++a) {
-                const int ci = li + a;
-                if (ci < 0 || ci >= kCT) continue;
-#pragma unroll
-                for (int b = 0; b < 2; ++b) {
-                    const int cj = lj + b;
-                    if (cj < 0 || cj >= kCT) continue;
-                    float* row = Sf + (ci * kCT + cj) * (2 * RS);
-                    const float wab = wx[a] * wy[b];
-#pragma unroll
-                    for (int c = 0; c < 2; ++c) atomicAdd(row + zo[c], wab * wz[c]);
-                }
+            // q is uniform across a warp except at run boundaries
+            switch (qq[u]) {
+                case 0: zcol_corners<N, R1, RS, 0>(cc[u], fx[u], fy[u], fz[u], mass, Sf); break;
+                case 1: zcol_corners<N, R1, RS, 1>(cc[u], fx[u], fy[u], fz[u], mass, Sf); break;
+                case 2: zcol_corners<N, R1, RS, 2>(cc[u], fx[u], fy[u], fz[u], mass, Sf); break;
+                case 3: zcol_corners<N, R1, RS, 3>(cc[u], fx[u], fy[u], fz[u], mass, Sf); break;
+                default: break;
             }
         }
     }
