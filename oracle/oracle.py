@@ -245,6 +245,25 @@ def kdk(ng, x, y, z, vx, vy, vz, mass, c_poisson, dt, steps, green_kind=1, grad_
             drift(ng, x, y, z, vx, vy, vz, dt)
 
 
+def function_a(a: float) -> float:
+    """include/utils/utils_inline.h:51-53 with Omega_m = 0.3, Omega_lambda = 0.7."""
+    return 1.0 / np.sqrt(0.3 / a + 0.0 + 0.7 * a * a)
+
+
+def cosmo_kdk(ng, x, y, z, px, py, pz, mass, a0, da, steps, green_kind=0, grad_order=2):
+    """Leapfrog KDK in the scale factor (new: src/utils/utils.cpp:141-143
+    sketches it): force s at a_s = a0 + s da with c_poisson = 3 / (2 a_s) and
+    kick function_a(a_s) da (halved at both ends), drift a^-2 function_a(a) da
+    at a = a0 + (s + 1/2) da."""
+    for s in range(steps + 1):
+        a = a0 + s * da
+        w = 0.5 if s in (0, steps) else 1.0
+        force_step(ng, x, y, z, px, py, pz, mass, 3.0 / (2.0 * a), w * function_a(a) * da, green_kind, grad_order)
+        if s < steps:
+            ah = a0 + (s + 0.5) * da
+            drift(ng, x, y, z, px, py, pz, function_a(ah) * da / (ah * ah))
+
+
 # ------------------------------------------------ the reference, single box
 
 def green_table_reference(ng: int, c_poisson: float) -> np.ndarray:

@@ -5,6 +5,7 @@ is the Python host side over it, with the reference's stage names.
 """
 from ._lib import PMError, load  # noqa: F401
 from .pm import (  # noqa: F401
-    DA, FFT, OMEGA_0, Ensemble, OMEGA_K, OMEGA_L, OMEGA_M, START_A, Plan, centered_derivatives, deposit_particles,
-    function_a, reference_coefficients, unit_box_coefficients, update_particles, zeldovich_ic,
+    DA, FFT, OMEGA_0, Ensemble, OMEGA_K, OMEGA_L, OMEGA_M, START_A, Plan, centered_derivatives, cosmo_run,
+    cosmo_schedule, deposit_particles, function_a, read_snapshot, reference_coefficients, unit_box_coefficients,
+    update_particles, write_snapshot, zeldovich_ic,
 )

@@ -18,6 +18,8 @@
 #include <random>
 #include <stdexcept>
 #include <string>
+#include <vector>
+#include <cstdio>
 
 #include "pm_b200.h"
 
@@ -113,6 +115,57 @@ inline void update_particles(Plan& plan, const double* posx, const double* posy,
                              double* py, double* pz, const double a, const size_t Np_local) {
     check(pm_interp_kick_f64(plan.get(), posx, posy, posz, d_dx, d_dy, d_dz, px, py, pz,
                              static_cast<int64_t>(Np_local), function_a(a) * Da));
+}
+
+// ---------------------------------------------- cosmological time stepping
+// Leapfrog kick-drift-kick in the scale factor a, the integration the
+// reference sketches but does not run (src/utils/utils.cpp:141-143: kick with
+// function_a(a) Da at the Poisson prefactor 3 Omega_0 / (2a) of
+// src/fft/fftw/fft.cpp:55; drift with a^-2 function_a(a) Da at the half
+// step).  Force evaluation s = 0..nsteps happens at a_s = a0 + s da with the
+// half kicks of neighbouring steps merged; after evaluation s < nsteps the
+// particles drift with a_{s+1/2}.  Each entry is one pm_step_* call.
+struct CosmoStep {
+    double a, c_poisson, c_kick, dt;
+};
+inline std::vector<CosmoStep> cosmo_schedule(double a0, double da, int nsteps) {
+    std::vector<CosmoStep> out;
+    for (int s = 0; s <= nsteps; ++s) {
+        const double a = a0 + s * da, ah = a0 + (s + 0.5) * da;
+        const double w = (s == 0 || s == nsteps) ? 0.5 : 1.0;
+        out.push_back({a, 3.0 * Omega_0 / (2.0 * a), w * function_a(a) * da,
+                       s < nsteps ? function_a(ah) * da / (ah * ah) : 0.0});
+    }
+    return out;
+}
+
+// Snapshot file (new; the reference writes no output): little-endian,
+// a 72-byte header then six float64 arrays of np values
+// (x, y, z in cell units, then the momenta or velocities vx, vy, vz).
+//   0  char[8] "PMSNAP1"   8 uint32 version (1)   12 uint32 flags (0)
+//   16 int64 ng   24 int64 np   32 double a   40 double mass
+//   48 double Omega_m   56 double Omega_lambda   64 double Omega_0
+struct SnapshotHeader {
+    char magic[8] = {'P', 'M', 'S', 'N', 'A', 'P', '1', '\0'};
+    uint32_t version = 1, flags = 0;
+    int64_t ng = 0, np = 0;
+    double a = 0, mass = 0, omega_m = Omega_m, omega_lambda = Omega_lambda, omega_0 = Omega_0;
+};
+static_assert(sizeof(SnapshotHeader) == 72, "snapshot header layout");
+
+// Writes the snapshot from six host arrays of np doubles.
+inline void write_snapshot(const char* path, int ng, double a, double mass, const double* const host[6], size_t np) {
+    FILE* f = std::fopen(path, "wb");
+    if (!f) throw Error(PM_ERR_ARG, std::string("cannot open ") + path);
+    SnapshotHeader h;
+    h.ng = ng;
+    h.np = static_cast<int64_t>(np);
+    h.a = a;
+    h.mass = mass;
+    bool ok = std::fwrite(&h, sizeof h, 1, f) == 1;
+    for (int c = 0; c < 6 && ok; ++c) ok = std::fwrite(host[c], sizeof(double), np, f) == np;
+    ok = (std::fclose(f) == 0) && ok;
+    if (!ok) throw Error(PM_ERR_ARG, std::string("writing ") + path + " failed");
 }
 
 }  // namespace pm

@@ -2,6 +2,7 @@
 // one B200 through the C ABI.
 //
 //   pm_main Ng Nrow [--steps N] [--warmup W] [--dump FILE]
+//           [--cosmo STEPS] [--snapshot FILE]
 //
 // Same inputs as the reference (main.cpp:18-21): Ng mesh cells per side,
 // Nrow^3 particles from init_particles (uniform, seeds 0/1/2), zero momenta,
@@ -11,7 +12,11 @@
 // exchange buckets (Alltoallv, reorder, reorder-back, Alltoallv-back) are 0:
 // one GPU holds the whole box.  Stage times come from CUDA events on the
 // plan's stream.  --dump writes positions then momenta (6 Np doubles) after
-// the run, for checking against the reference.
+// the run, for checking against the reference.  --cosmo then advances the
+// particles by STEPS leapfrog steps in the scale factor from Start_a with
+// da = Da (pm::cosmo_schedule, FP64 step, the reference's discrete Green's
+// function and 2-point gradient), and --snapshot writes the final state in
+// the pm::SnapshotHeader format.
 #include <cuda_runtime.h>
 
 #include <array>
@@ -34,17 +39,22 @@
 
 int main(int argc, char** argv) {
     if (argc < 3) {
-        std::fprintf(stderr, "usage: %s Ng Nrow [--steps N] [--warmup W] [--dump FILE]\n", argv[0]);
+        std::fprintf(stderr, "usage: %s Ng Nrow [--steps N] [--warmup W] [--dump FILE] [--cosmo STEPS] "
+                             "[--snapshot FILE]\n", argv[0]);
         return 1;
     }
     const int Ng = std::atoi(argv[1]);
     const int Nrow = std::atoi(argv[2]);
     int loop = 20, worm_up = 10;
     const char* dump = nullptr;
+    const char* snapshot = nullptr;
+    int cosmo = 0;
     for (int i = 3; i + 1 < argc; i += 2) {
         if (!std::strcmp(argv[i], "--steps")) loop = std::atoi(argv[i + 1]);
         else if (!std::strcmp(argv[i], "--warmup")) worm_up = std::atoi(argv[i + 1]);
         else if (!std::strcmp(argv[i], "--dump")) dump = argv[i + 1];
+        else if (!std::strcmp(argv[i], "--cosmo")) cosmo = std::atoi(argv[i + 1]);
+        else if (!std::strcmp(argv[i], "--snapshot")) snapshot = argv[i + 1];
     }
     const size_t Ng3 = static_cast<size_t>(Ng) * Ng * Ng;
     const size_t Np = static_cast<size_t>(Nrow) * Nrow * Nrow;
@@ -104,6 +114,22 @@ int main(int argc, char** argv) {
                 std::fwrite(h.data(), sizeof(double), Np, f);
             }
             std::fclose(f);
+        }
+        if (cosmo > 0) {
+            for (const pm::CosmoStep& c : pm::cosmo_schedule(pm::Start_a, pm::Da, cosmo))
+                pm::check(pm_step_f64(plan.get(), pos[0], pos[1], pos[2], mom[0], mom[1], mom[2],
+                                      static_cast<int64_t>(Np), mass, c.c_poisson, c.c_kick, c.dt));
+            plan.check_positions();
+        }
+        if (snapshot) {
+            std::vector<std::vector<double>> h(6, std::vector<double>(Np));
+            const double* dev[6] = {pos[0], pos[1], pos[2], mom[0], mom[1], mom[2]};
+            const double* host[6];
+            for (int c = 0; c < 6; ++c) {
+                CUDA_OK(cudaMemcpy(h[c].data(), dev[c], sizeof(double) * Np, cudaMemcpyDeviceToHost));
+                host[c] = h[c].data();
+            }
+            pm::write_snapshot(snapshot, Ng, pm::Start_a + cosmo * pm::Da, mass, host, Np);
         }
         cudaFree(real_buf);
         for (auto q : d) cudaFree(q);

@@ -487,3 +487,75 @@ def update_particles(posx, posy, posz, d_dx, d_dy, d_dz, px, py, pz, a: float, p
     (src/utils/utils.cpp:141-170)."""
     plan = plan or _default_plan(d_dx.shape[0], d_dx.device)
     plan.interp_kick(posx, posy, posz, (d_dx, d_dy, d_dz), px, py, pz, function_a(a) * DA)
+
+
+# ----------------------------------------------- cosmological time stepping
+def cosmo_schedule(a0: float = START_A, da: float = DA, nsteps: int = 1):
+    """Leapfrog KDK in the scale factor, the integration the reference sketches
+    in update_particles (src/utils/utils.cpp:141-143): force evaluation
+    s = 0..nsteps at a_s = a0 + s da with Poisson prefactor 3 Omega_0 / (2 a_s)
+    (src/fft/fftw/fft.cpp:55) and kick function_a(a_s) da (halved at the two
+    ends, the inner half kicks merged); after evaluation s < nsteps a drift of
+    a^-2 function_a(a) da at a = a0 + (s + 1/2) da.  One (a, c_poisson,
+    c_kick, dt) tuple per Plan.step / Plan.step_split call."""
+    out = []
+    for s in range(nsteps + 1):
+        a = a0 + s * da
+        ah = a0 + (s + 0.5) * da
+        w = 0.5 if s in (0, nsteps) else 1.0
+        out.append((a, 3.0 * OMEGA_0 / (2.0 * a), w * function_a(a) * da,
+                    function_a(ah) * da / (ah * ah) if s < nsteps else 0.0))
+    return out
+
+
+def cosmo_run(plan: Plan, pos, mom, mass: float, a0: float = START_A, da: float = DA, nsteps: int = 1):
+    """Advances FP64 positions / momenta (or, on an FP32 plan, split positions
+    (cell, off) and FP32 velocities) through cosmo_schedule; returns the final
+    scale factor."""
+    for _, cp, ck, dt in cosmo_schedule(a0, da, nsteps):
+        if plan.precision == "fp64":
+            plan.step(*pos, *mom, mass, cp, ck, dt)
+        else:
+            plan.step_split(pos[0], pos[1], mom, mass, cp, ck, dt)
+    return a0 + nsteps * da
+
+
+# -------------------------------------------------------------- snapshots
+# Little-endian file: a 72-byte header, then x, y, z (cell units), vx, vy, vz
+# as float64 arrays of np values.  The reference writes no output; this is
+# the format of the C++ mirror's pm::write_snapshot as well.
+_SNAP_MAGIC = b"PMSNAP1\0"
+_SNAP_HEAD = "<8sIIqqddddd"
+
+
+def write_snapshot(path: str, ng: int, a: float, mass: float, pos, vel):
+    """Writes positions and velocities (any device, any float dtype)."""
+    import struct
+    np_ = pos[0].numel()
+    with open(path, "wb") as f:
+        f.write(struct.pack(_SNAP_HEAD, _SNAP_MAGIC, 1, 0, ng, np_, float(a), float(mass), OMEGA_M, OMEGA_L,
+                            OMEGA_0))
+        for t in (*pos, *vel):
+            if t.numel() != np_:
+                raise PMError(L.PM_ERR_ARG, "snapshot arrays must all have np values")
+            f.write(t.detach().to("cpu", torch.float64).contiguous().numpy().tobytes())
+
+
+def read_snapshot(path: str) -> dict:
+    """{ng, np, a, mass, omega_m, omega_lambda, omega_0, pos: [3], vel: [3]}
+    (float64 CPU tensors)."""
+    import struct
+    size = struct.calcsize(_SNAP_HEAD)
+    with open(path, "rb") as f:
+        head = f.read(size)
+        if len(head) != size:
+            raise PMError(L.PM_ERR_ARG, f"{path}: truncated header")
+        magic, ver, _flags, ng, np_, a, mass, om, ol, o0 = struct.unpack(_SNAP_HEAD, head)
+        if magic != _SNAP_MAGIC or ver != 1:
+            raise PMError(L.PM_ERR_ARG, f"{path}: not a version-1 particle-mesh snapshot")
+        body = f.read()
+    if len(body) != 6 * 8 * np_:
+        raise PMError(L.PM_ERR_ARG, f"{path}: expected {6 * 8 * np_} bytes of particle data, got {len(body)}")
+    arr = torch.frombuffer(bytearray(body), dtype=torch.float64).view(6, np_)
+    return {"ng": ng, "np": np_, "a": a, "mass": mass, "omega_m": om, "omega_lambda": ol, "omega_0": o0,
+            "pos": [arr[i].clone() for i in range(3)], "vel": [arr[3 + i].clone() for i in range(3)]}
