@@ -613,6 +613,13 @@ int deposit_zr2c_prepare(const Plan& p) {
     }
 }
 
+template <int N>
+static void launch_zcol(const Plan& p, unsigned blocks, const uint32_t* cell, const float* ox, const float* oy,
+                        const float* oz, float mass, float* mesh, const float2* tw, int nt) {
+    k_deposit_zr2c<N><<<blocks, zcol_threads<N>(), kCTRows * z_row_stride<N>() * sizeof(float2), p.stream>>>(
+        cell, ox, oy, oz, p.tiles.perm, p.tiles.off, mass, mesh, tw, nt);
+}
+
 // Deposit + z R2C in one pass over the mesh (FP32, power-of-two ng >= 32):
 // mesh receives the z-transformed density contrast, ready for the y pass.
 int deposit_zr2c_f32(Plan& p, const uint32_t* cell, const float* ox, const float* oy, const float* oz, int64_t np,
@@ -627,17 +634,15 @@ int deposit_zr2c_f32(Plan& p, const uint32_t* cell, const float* ox, const float
     {
         Timed t(p, ST_DEPOSIT);
         const unsigned blocks = (unsigned)(nt * nt);
-#define PMB_ZCOL(NN)                                                                                         case NN:                                                                                                     k_deposit_zr2c<NN><<<blocks, zcol_threads<NN>(), kCTRows * z_row_stride<NN>() * sizeof(float2),                              p.stream>>>(cell, ox, oy, oz, p.tiles.perm, p.tiles.off, mass, mesh, tw, nt);         break;
         switch (p.ng) {
-            PMB_ZCOL(32)
-            PMB_ZCOL(64)
-            PMB_ZCOL(128)
-            PMB_ZCOL(256)
-            PMB_ZCOL(512)
-            PMB_ZCOL(1024)
+            case 32: launch_zcol<32>(p, blocks, cell, ox, oy, oz, mass, mesh, tw, nt); break;
+            case 64: launch_zcol<64>(p, blocks, cell, ox, oy, oz, mass, mesh, tw, nt); break;
+            case 128: launch_zcol<128>(p, blocks, cell, ox, oy, oz, mass, mesh, tw, nt); break;
+            case 256: launch_zcol<256>(p, blocks, cell, ox, oy, oz, mass, mesh, tw, nt); break;
+            case 512: launch_zcol<512>(p, blocks, cell, ox, oy, oz, mass, mesh, tw, nt); break;
+            case 1024: launch_zcol<1024>(p, blocks, cell, ox, oy, oz, mass, mesh, tw, nt); break;
             default: return fail(PM_ERR_SIZE, "fused deposit needs a power-of-two ng >= 32");
         }
-#undef PMB_ZCOL
     }
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;
