@@ -373,7 +373,11 @@ def ours(args):
         barrier()
         t64 = max_over_ranks(e0.elapsed_time(e1))
         st64 = p64.read_timing(reset=True)
+        b64 = sum(stage_bytes(s, ng, np_, 8) * n / args.steps for s, (_, n) in st64.items())
         fp64 = {"value": throughput(world, np_, args.steps, t64), "unit": UNIT, "ms_per_step": t64 / args.steps,
+                "roofline": {"bound": "hbm", "algorithmic_bytes_per_step": b64,
+                             "achieved": b64 / (t64 / args.steps / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                             "frac": b64 / (t64 / args.steps / 1e3) / 1e9 / peak},
                 "dtype": "f64", "path": "plain FP64: separate deposit, 3+3 FFT passes, Green, gradient to 3 force "
                                         "meshes, interpolate + kick, drift",
                 "stages": {s: {"ms_per_step": ms / args.steps, "launches": n,
