@@ -97,6 +97,12 @@ const char* pm_last_error(void);
  * launches[PM_STAGE_COUNT] (either may be NULL); reset != 0 zeroes both. */
 #define PM_STAGE_COUNT 19
 int pm_plan_set_timing(pm_plan* plan, int on);
+/* Shape of the strided FFT passes (new; the knobs the ensemble autotuner
+ * turns): tile_cols kz columns per block (0 the default; 8, 16 or 32 on FP32
+ * plans with ng <= 128) and the first radix of the two-pass line split (0
+ * the default; FP32 plans with power-of-two ng in 16..128 also take the
+ * smaller alternative, see pm_ensemble_info).  PM_ERR_ARG otherwise. */
+int pm_plan_set_fft_shape(pm_plan* plan, int tile_cols, int radix1);
 int pm_plan_read_timing(pm_plan* plan, double* ms, int64_t* launches, int reset);
 /* Name of stage i ("mesh_init", "deposit", "fft_z_r2c", ...), "" if out of range. */
 const char* pm_stage_name(int stage);
@@ -302,10 +308,12 @@ int pm_ensemble_step_f32(pm_ensemble* ensemble, uint32_t* cell, float* ox, float
  * while the arrays, c_poisson, dt and steps stay the same. */
 int pm_ensemble_run_f32(pm_ensemble* ensemble, uint32_t* cell, float* ox, float* oy, float* oz,
                         float* vx, float* vy, float* vz, double c_poisson, double dt, int steps);
-/* Classes (mesh size, boxes, chosen tile width), device bytes held and the
- * node count of the last captured graph; any output may be NULL. */
+/* Classes (mesh size, boxes, chosen tile width, first radix of the chosen
+ * two-pass split of the strided FFT passes; 0 for the mixed-radix 48 / 96),
+ * device bytes held and the node count of the last captured graph; any
+ * output may be NULL. */
 int pm_ensemble_info(const pm_ensemble* ensemble, int* nclasses, int* class_ng, int* class_nbox,
-                     int* class_tk, size_t* device_bytes, size_t* graph_nodes);
+                     int* class_tk, int* class_radix, size_t* device_bytes, size_t* graph_nodes);
 
 /* ---------------------------------------------- initial conditions (new)
  * Zel'dovich particles on an nrow^3 lattice q = (i + 1/2) ng/nrow from a

@@ -52,6 +52,7 @@ SIGNATURES = {
     "pm_interp_f32": [_V, _V, _V, _V, _V, _V, _L, _V, _V, _V],
     "pm_kick_drift_f32": [_V, _V, _V, _V, _V, _V, _V, _V, _V, _L, _D, _D],
     "pm_step_f32": [_V, _V, _V, _V, _V, _V, _V, _V, _L, _F, _D, _D, _D],
+    "pm_plan_set_fft_shape": [_V, _I, _I],
     "pm_reduce_f32": [_V, _V, _V, _V, _V, _L, _D, _V],
     "pm_reduce_f64": [_V, _V, _V, _V, _V, _L, _D, _V],
     "pm_adjoint_deposit_f32": [_V, _V, _V, _V, _V, _L, _F, _V, _V, _V, _V],
@@ -63,7 +64,7 @@ SIGNATURES = {
     "pm_ensemble_sync": [_V],
     "pm_ensemble_step_f32": [_V, _V, _V, _V, _V, _V, _V, _V, _D, _D, _D],
     "pm_ensemble_run_f32": [_V, _V, _V, _V, _V, _V, _V, _V, _D, _D, _I],
-    "pm_ensemble_info": [_V, _V, _V, _V, _V, _V, _V],
+    "pm_ensemble_info": [_V, _V, _V, _V, _V, _V, _V, _V],
     "pm_ic_zeldovich": [_I, _I, _D, _D, _U64, _D, _V, _V, _V, _V, _V, _V, _V],
 }
 

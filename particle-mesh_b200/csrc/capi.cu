@@ -260,6 +260,20 @@ int pm_plan_check(pm_plan* plan) {
     return PM_OK;
 }
 
+int pm_plan_set_fft_shape(pm_plan* plan, int tile_cols, int radix1) {
+    if (!plan) return fail(PM_ERR_ARG, "plan is NULL");
+    Plan& p = plan->p;
+    if (!tk_variant_supported(p.ng, p.precision, tile_cols))
+        return fail(PM_ERR_ARG, "tile_cols must be 0, or 8 / 16 / 32 on an FP32 plan with ng <= 128");
+    int rv = -1;
+    if (radix1 == 0 || radix1 == strided_radix1(p.ng, 0)) rv = 0;
+    else if (radix_variant_supported(p.ng, p.precision, 1) && radix1 == strided_radix1(p.ng, 1)) rv = 1;
+    if (rv < 0) return fail(PM_ERR_ARG, "radix1 is not a split of this plan's strided passes");
+    p.tk = tile_cols;
+    p.rv = rv;
+    return PM_OK;
+}
+
 int pm_plan_set_timing(pm_plan* plan, int on) {
     if (!plan) return fail(PM_ERR_ARG, "plan is NULL");
     plan->p.timers->on = on != 0;

@@ -86,37 +86,45 @@ std::string gpu_name() {
     return s;
 }
 
-// Tune cache lines: "<gpu> <ng> <green> <order> <tk>".
-std::map<std::string, int> read_cache(const char* path) {
-    std::map<std::string, int> m;
+// Tune cache lines: "<gpu> <ng> <green> <order> <tk> <rv>" (tile width and
+// radix split; a line without <rv> means the default split).
+using TuneCache = std::map<std::string, std::pair<int, int>>;
+
+TuneCache read_cache(const char* path) {
+    TuneCache m;
     if (!path) return m;
     FILE* f = std::fopen(path, "r");
     if (!f) return m;
-    char gpu[256];
-    int ng, gk, go, tk;
-    while (std::fscanf(f, "%255s %d %d %d %d", gpu, &ng, &gk, &go, &tk) == 5)
-        m[std::string(gpu) + " " + std::to_string(ng) + " " + std::to_string(gk) + " " + std::to_string(go)] = tk;
+    char line[512], gpu[256];
+    while (std::fgets(line, sizeof line, f)) {
+        int ng, gk, go, tk, rv = 0;
+        const int n = std::sscanf(line, "%255s %d %d %d %d %d", gpu, &ng, &gk, &go, &tk, &rv);
+        if (n < 5) continue;
+        m[std::string(gpu) + " " + std::to_string(ng) + " " + std::to_string(gk) + " " + std::to_string(go)] = {tk, rv};
+    }
     std::fclose(f);
     return m;
 }
 
-void write_cache(const char* path, const std::map<std::string, int>& m) {
+void write_cache(const char* path, const TuneCache& m) {
     if (!path) return;
     FILE* f = std::fopen(path, "w");
     if (!f) return;
-    for (auto& kv : m) std::fprintf(f, "%s %d\n", kv.first.c_str(), kv.second);
+    for (auto& kv : m) std::fprintf(f, "%s %d %d\n", kv.first.c_str(), kv.second.first, kv.second.second);
     std::fclose(f);
 }
 
 // Times the class's batched Poisson solve for each column-tile width and
-// keeps the fastest.
-int autotune_class(EnsembleClass& c, std::map<std::string, int>& cache, bool measure) {
+// radix split of the strided passes and keeps the fastest pair.
+int autotune_class(EnsembleClass& c, TuneCache& cache, bool measure) {
     Plan& p = c.plan->p;
     const std::string key = gpu_name() + " " + std::to_string(c.ng) + " " + std::to_string(p.green_kind) + " " +
                             std::to_string(p.grad_order);
     auto it = cache.find(key);
-    if (it != cache.end() && tk_variant_supported(c.ng, PM_FP32, it->second)) {
-        p.tk = it->second;
+    if (it != cache.end() && tk_variant_supported(c.ng, PM_FP32, it->second.first) &&
+        radix_variant_supported(c.ng, PM_FP32, it->second.second)) {
+        p.tk = it->second.first;
+        p.rv = it->second.second;
         return PM_OK;
     }
     if (!measure || c.ng > 128) return PM_OK;
@@ -126,32 +134,38 @@ int autotune_class(EnsembleClass& c, std::map<std::string, int>& cache, bool mea
     PMB_CUDA_CHECK(cudaEventCreate(&a));
     PMB_CUDA_CHECK(cudaEventCreate(&b));
     float best = 1e30f;
-    int best_tk = 0;
-    for (int tk : {0, 8, 16, 32}) {
-        if (!tk_variant_supported(c.ng, PM_FP32, tk)) continue;
-        p.tk = tk;
-        int rc = PM_OK;
-        for (int r = 0; r < 2 && rc == PM_OK; ++r) rc = poisson_fused<float>(p, c.mesh, 1.0, nbox);
-        cudaEventRecord(a, p.stream);
-        for (int r = 0; r < 5 && rc == PM_OK; ++r) rc = poisson_fused<float>(p, c.mesh, 1.0, nbox);
-        cudaEventRecord(b, p.stream);
-        if (rc != PM_OK) {
-            cudaEventDestroy(a);
-            cudaEventDestroy(b);
-            return rc;
-        }
-        cudaEventSynchronize(b);
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, a, b);
-        if (ms < best) {
-            best = ms;
-            best_tk = tk;
+    int best_tk = 0, best_rv = 0;
+    for (int rv : {0, 1}) {
+        if (!radix_variant_supported(c.ng, PM_FP32, rv)) continue;
+        for (int tk : {0, 8, 16, 32}) {
+            if (!tk_variant_supported(c.ng, PM_FP32, tk)) continue;
+            p.tk = tk;
+            p.rv = rv;
+            int rc = PM_OK;
+            for (int r = 0; r < 2 && rc == PM_OK; ++r) rc = poisson_fused<float>(p, c.mesh, 1.0, nbox);
+            cudaEventRecord(a, p.stream);
+            for (int r = 0; r < 5 && rc == PM_OK; ++r) rc = poisson_fused<float>(p, c.mesh, 1.0, nbox);
+            cudaEventRecord(b, p.stream);
+            if (rc != PM_OK) {
+                cudaEventDestroy(a);
+                cudaEventDestroy(b);
+                return rc;
+            }
+            cudaEventSynchronize(b);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, a, b);
+            if (ms < best) {
+                best = ms;
+                best_tk = tk;
+                best_rv = rv;
+            }
         }
     }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     p.tk = best_tk;
-    cache[key] = best_tk;
+    p.rv = best_rv;
+    cache[key] = {best_tk, best_rv};
     return PM_OK;
 }
 
@@ -293,13 +307,15 @@ int pm_ensemble_sync(pm_ensemble* e) {
 }
 
 int pm_ensemble_info(const pm_ensemble* e, int* nclasses, int* class_ng, int* class_nbox, int* class_tk,
-                     size_t* device_bytes, size_t* graph_nodes) {
+                     int* class_radix, size_t* device_bytes, size_t* graph_nodes) {
     if (!e) return fail(PM_ERR_ARG, "ensemble is NULL");
     if (nclasses) *nclasses = (int)e->classes.size();
     for (size_t i = 0; i < e->classes.size(); ++i) {
+        const Plan& p = e->classes[i].plan->p;
         if (class_ng) class_ng[i] = e->classes[i].ng;
         if (class_nbox) class_nbox[i] = (int)e->classes[i].boxes.size();
-        if (class_tk) class_tk[i] = e->classes[i].plan->p.tk;
+        if (class_tk) class_tk[i] = p.tk;
+        if (class_radix) class_radix[i] = strided_radix1(p.ng, p.rv);
     }
     if (device_bytes) *device_bytes = e->bytes;
     if (graph_nodes) *graph_nodes = e->graph_nodes;

@@ -145,15 +145,15 @@ k_fft_z_c2r(T* __restrict__ mesh, long long nrows, const typename Cx<T>::t* __re
 // ------------------------------------------------------ strided C2C passes
 // Lines of N complex at element stride `es`; block (bx, by) owns columns
 // [bx*TK, bx*TK+TK) of plane `by` (plane base = by * os).
-template <int N, int TK> constexpr int strided_threads() { return TK * threads_per_line<N>(); }
-template <int N, int TK> constexpr int strided_smem_elems() { return (N + N / Radix<N>::R1) * TK; }
+template <int N, int TK, int RV = 0> constexpr int strided_threads() { return TK * threads_per_line_v<N, RV>(); }
+template <int N, int TK, int RV = 0> constexpr int strided_smem_elems() { return (N + N / RadixV<N, RV>::R1) * TK; }
 
-template <typename T, int N, int DIR, int TK>
-__global__ void __launch_bounds__(strided_threads<N, TK>(), 2)
+template <typename T, int N, int DIR, int TK, int RV = 0>
+__global__ void __launch_bounds__(strided_threads<N, TK, RV>(), 2)
 k_fft_strided(typename Cx<T>::t* __restrict__ data, long long es, long long os, long long bs, int ncols,
               const typename Cx<T>::t* __restrict__ tw) {
     using C = typename Cx<T>::t;
-    constexpr int R1 = Radix<N>::R1, R2 = Radix<N>::R2;
+    constexpr int R1 = RadixV<N, RV>::R1, R2 = RadixV<N, RV>::R2;
     extern __shared__ __align__(16) unsigned char smraw[];
     C* S = reinterpret_cast<C*>(smraw);
     const int tx = threadIdx.x % TK, ty = threadIdx.x / TK;
@@ -199,12 +199,12 @@ __device__ __forceinline__ T green_value(int kx, int ky, int kz, int kind, doubl
 
 // Fused x pass of the Poisson solve: forward FFT along x, multiply by G,
 // inverse FFT along x, for TK kz columns of one ky plane.
-template <typename T, int N, int TK>
-__global__ void __launch_bounds__(strided_threads<N, TK>(), 2)
+template <typename T, int N, int TK, int RV = 0>
+__global__ void __launch_bounds__(strided_threads<N, TK, RV>(), 2)
 k_fft_x_green(typename Cx<T>::t* __restrict__ data, long long es, long long os, long long bs, int ncols,
               const typename Cx<T>::t* __restrict__ tw, const T* __restrict__ g1d, double cg, int kind) {
     using C = typename Cx<T>::t;
-    constexpr int R1 = Radix<N>::R1, R2 = Radix<N>::R2;
+    constexpr int R1 = RadixV<N, RV>::R1, R2 = RadixV<N, RV>::R2;
     extern __shared__ __align__(16) unsigned char smraw[];
     C* S = reinterpret_cast<C*>(smraw);
     const int tx = threadIdx.x % TK, ty = threadIdx.x / TK;
@@ -379,17 +379,17 @@ template <typename T, int N, int TK = kGTK> struct LaunchG {
 };
 
 // ------------------------------------------------------------- launchers
-template <typename T, int N, int TK = tk_cols<T, N>()> struct Launch {
+template <typename T, int N, int TK = tk_cols<T, N>(), int RV = 0> struct Launch {
     using C = typename Cx<T>::t;
     static constexpr int H = N / 2 + 1;
     static size_t smem_z() { return (size_t)z_rows_per_block<T, N>() * z_row_stride<N>() * sizeof(C); }
-    static size_t smem_s() { return (size_t)strided_smem_elems<N, TK>() * sizeof(C); }
+    static size_t smem_s() { return (size_t)strided_smem_elems<N, TK, RV>() * sizeof(C); }
     static int prepare() {
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_z_r2c<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_z()));
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_z_c2r<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_z()));
-        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, -1, TK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
-        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, +1, TK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
-        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_x_green<T, N, TK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
+        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, -1, TK, RV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
+        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, +1, TK, RV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
+        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_x_green<T, N, TK, RV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         return PM_OK;
     }
     static void z(const Plan& p, T* mesh, bool forward, int nbox = 1) {
@@ -413,15 +413,15 @@ template <typename T, int N, int TK = tk_cols<T, N>()> struct Launch {
         const C* tw = static_cast<const C*>(p.tw);
         Timed t(p, axis == 1 ? (dir < 0 ? ST_FFT_Y_FWD : ST_FFT_Y_INV) : (dir < 0 ? ST_FFT_X_FWD : ST_FFT_X_INV));
         if (dir < 0)
-            k_fft_strided<T, N, -1, TK><<<grid, strided_threads<N, TK>(), smem_s(), p.stream>>>(d, es, os, bs, H, tw);
+            k_fft_strided<T, N, -1, TK, RV><<<grid, strided_threads<N, TK, RV>(), smem_s(), p.stream>>>(d, es, os, bs, H, tw);
         else
-            k_fft_strided<T, N, +1, TK><<<grid, strided_threads<N, TK>(), smem_s(), p.stream>>>(d, es, os, bs, H, tw);
+            k_fft_strided<T, N, +1, TK, RV><<<grid, strided_threads<N, TK, RV>(), smem_s(), p.stream>>>(d, es, os, bs, H, tw);
     }
     static void xgreen(const Plan& p, T* mesh, double cg, int nbox = 1) {
         C* d = reinterpret_cast<C*>(mesh);
         dim3 grid((H + TK - 1) / TK, N * nbox);
         Timed t(p, ST_FFT_X_GREEN);
-        k_fft_x_green<T, N, TK><<<grid, strided_threads<N, TK>(), smem_s(), p.stream>>>(
+        k_fft_x_green<T, N, TK, RV><<<grid, strided_threads<N, TK, RV>(), smem_s(), p.stream>>>(
             d, (long long)N * H, H, (long long)N * N * H, H, static_cast<const C*>(p.tw),
             static_cast<const T*>(p.g1d), cg, p.green_kind);
     }
@@ -448,9 +448,9 @@ bool fft_size_supported(int ng) {
 
 // Launcher of a mesh size: the two-pass power-of-two kernels, or the
 // generic mixed-radix ones for 48 and 96.
-template <typename T, int N, int TK = 0>
+template <typename T, int N, int TK = 0, int RV = 0>
 using LaunchFor = typename std::conditional<
-    (N & (N - 1)) == 0, Launch<T, N, TK == 0 ? tk_cols<T, N>() : TK>, LaunchG<T, N, TK == 0 ? kGTK : TK>>::type;
+    (N & (N - 1)) == 0, Launch<T, N, TK == 0 ? tk_cols<T, N>() : TK, RV>, LaunchG<T, N, TK == 0 ? kGTK : TK>>::type;
 
 // Column-tile widths the autotuner may pick for small FP32 meshes (ng <= 128);
 // Plan::tk == 0 keeps the default width.
@@ -458,13 +458,43 @@ bool tk_variant_supported(int ng, int precision, int tk) {
     return tk == 0 || (precision == PM_FP32 && ng <= 128 && (tk == 8 || tk == 16 || tk == 32));
 }
 
-// Runs BODY with the launcher L_ of the plan's mesh size and tile width.
+// The alternative radix split (RadixV<ng, 1>) exists for FP32 power-of-two
+// meshes 16..128.
+bool radix_variant_supported(int ng, int precision, int rv) {
+    return rv == 0 || (rv == 1 && precision == PM_FP32 && ng >= 16 && ng <= 128 && (ng & (ng - 1)) == 0);
+}
+
+// First radix of the strided passes' two-pass split (0 for the mixed-radix
+// 48 / 96 schedules).
+int strided_radix1(int ng, int rv) {
+    switch (ng) {
+        case 8: return Radix<8>::R1;
+        case 16: return rv ? RadixV<16, 1>::R1 : Radix<16>::R1;
+        case 32: return rv ? RadixV<32, 1>::R1 : Radix<32>::R1;
+        case 64: return rv ? RadixV<64, 1>::R1 : Radix<64>::R1;
+        case 128: return rv ? RadixV<128, 1>::R1 : Radix<128>::R1;
+        case 256: return Radix<256>::R1;
+        case 512: return Radix<512>::R1;
+        case 1024: return Radix<1024>::R1;
+        default: return 0;
+    }
+}
+
+// Runs BODY with the launcher L_ of the plan's mesh size, tile width and
+// radix split.
+#define PMB_LAUNCH_TK(P, T_, RV_, ...)                                                                 \
+    if ((P).tk == 8) { using L_ = LaunchFor<T_, N_, 8, RV_>; __VA_ARGS__; break; }                     \
+    if ((P).tk == 16) { using L_ = LaunchFor<T_, N_, 16, RV_>; __VA_ARGS__; break; }                   \
+    if ((P).tk == 32) { using L_ = LaunchFor<T_, N_, 32, RV_>; __VA_ARGS__; break; }                   \
+    { using L_ = LaunchFor<T_, N_, 0, RV_>; __VA_ARGS__; break; }
+
 #define PMB_LAUNCH(P, T_, ...)                                                                         \
     PMB_FFT_DISPATCH((P).ng, {                                                                         \
         if constexpr (sizeof(T_) == 4 && N_ <= 128) {                                                  \
-            if ((P).tk == 8) { using L_ = LaunchFor<T_, N_, 8>; __VA_ARGS__; break; }                  \
-            if ((P).tk == 16) { using L_ = LaunchFor<T_, N_, 16>; __VA_ARGS__; break; }                \
-            if ((P).tk == 32) { using L_ = LaunchFor<T_, N_, 32>; __VA_ARGS__; break; }                \
+            if constexpr (N_ >= 16 && (N_ & (N_ - 1)) == 0) {                                          \
+                if ((P).rv == 1) { PMB_LAUNCH_TK(P, T_, 1, __VA_ARGS__) }                              \
+            }                                                                                          \
+            PMB_LAUNCH_TK(P, T_, 0, __VA_ARGS__)                                                       \
         }                                                                                              \
         using L_ = LaunchFor<T_, N_>;                                                                  \
         __VA_ARGS__;                                                                                   \
@@ -481,6 +511,12 @@ int fft_prepare(const Plan& p) {
                 if (rc == PM_OK) rc = LaunchFor<float, N_, 8>::prepare();
                 if (rc == PM_OK) rc = LaunchFor<float, N_, 16>::prepare();
                 if (rc == PM_OK) rc = LaunchFor<float, N_, 32>::prepare();
+                if constexpr (N_ >= 16 && (N_ & (N_ - 1)) == 0) {
+                    if (rc == PM_OK) rc = LaunchFor<float, N_, 0, 1>::prepare();
+                    if (rc == PM_OK) rc = LaunchFor<float, N_, 8, 1>::prepare();
+                    if (rc == PM_OK) rc = LaunchFor<float, N_, 16, 1>::prepare();
+                    if (rc == PM_OK) rc = LaunchFor<float, N_, 32, 1>::prepare();
+                }
             }
         });
     }

@@ -101,6 +101,16 @@ template <> struct Radix<1024> { static constexpr int R1 = 32, R2 = 32; };
 // R2 / R1 radix-R1 butterflies per thread.
 template <int L> constexpr int threads_per_line() { return L / Radix<L>::R2; }
 
+// Split variants of a strided line for the autotuner: RV = 0 is Radix<L>,
+// RV = 1 a smaller first radix and a larger second one (more work per
+// thread, fewer threads per line), still with R2 % R1 == 0.
+template <int L, int RV> struct RadixV : Radix<L> {};
+template <> struct RadixV<16, 1> { static constexpr int R1 = 2, R2 = 8; };
+template <> struct RadixV<32, 1> { static constexpr int R1 = 2, R2 = 16; };
+template <> struct RadixV<64, 1> { static constexpr int R1 = 4, R2 = 16; };
+template <> struct RadixV<128, 1> { static constexpr int R1 = 4, R2 = 32; };
+template <int L, int RV> constexpr int threads_per_line_v() { return L / RadixV<L, RV>::R2; }
+
 // Stockham pass 1 (Ns = 1, radix R1) of a line of L = R1 R2: thread tj owns
 // the butterflies j = tj + it R1 (it < R2/R1).  ld(j, r) returns element
 // j + r R2; st(j, k, v) stores output k of butterfly j, element j R1 + k.

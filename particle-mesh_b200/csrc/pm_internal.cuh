@@ -127,6 +127,7 @@ struct Plan {
     StageTimers* timers = nullptr;  // owned by the C-ABI plan object
     TileScratch tiles;
     int tk = 0;  // column-tile width of the strided FFT passes (0: default)
+    int rv = 0;  // strided-pass radix split: 0 the default, 1 the alternative (autotuned)
 };
 
 // Brackets one kernel launch with the plan's stage timer.
@@ -161,6 +162,8 @@ template <typename T> int green_apply(const Plan& p, T* mesh, double c_poisson);
 template <typename T> int poisson_fused(const Plan& p, T* mesh, double c_poisson, int nbox = 1);
 bool fft_size_supported(int ng);
 bool tk_variant_supported(int ng, int precision, int tk);
+bool radix_variant_supported(int ng, int precision, int rv);
+int strided_radix1(int ng, int rv);
 int fft_prepare(const Plan& p);  // one-time kernel attributes (large smem)
 
 // Particle and mesh kernels (particles.cu).

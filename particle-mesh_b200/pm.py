@@ -119,6 +119,10 @@ class Plan:
         check(self.lib.pm_plan_device_bytes(self._h, ctypes.byref(b)))
         return b.value
 
+    def set_fft_shape(self, tile_cols: int = 0, radix1: int = 0):
+        """Column-tile width and first radix of the strided FFT passes (0: default)."""
+        check(self.lib.pm_plan_set_fft_shape(self._h, int(tile_cols), int(radix1)))
+
     def set_timing(self, on: bool = True):
         check(self.lib.pm_plan_set_timing(self._h, 1 if on else 0))
 
@@ -402,10 +406,12 @@ class Ensemble:
         ng = (ctypes.c_int * 64)()
         nb = (ctypes.c_int * 64)()
         tk = (ctypes.c_int * 64)()
+        r1 = (ctypes.c_int * 64)()
         by = ctypes.c_size_t()
         nodes = ctypes.c_size_t()
-        check(self.lib.pm_ensemble_info(self._h, ctypes.byref(nc), ng, nb, tk, ctypes.byref(by), ctypes.byref(nodes)))
-        return {"classes": [{"ng": ng[i], "boxes": nb[i], "tile_cols": tk[i]} for i in range(nc.value)],
+        check(self.lib.pm_ensemble_info(self._h, ctypes.byref(nc), ng, nb, tk, r1, ctypes.byref(by),
+                                        ctypes.byref(nodes)))
+        return {"classes": [{"ng": ng[i], "boxes": nb[i], "tile_cols": tk[i], "radix1": r1[i]} for i in range(nc.value)],
                 "device_bytes": by.value, "graph_nodes": nodes.value}
 
     def step(self, cell, off, vel, c_poisson: float, c_kick: float, dt: float):

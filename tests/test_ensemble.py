@@ -78,6 +78,39 @@ def test_ensemble_graph_matches_boxes_alone(pmpkg, tmp_path):
         ens.step(c2, o2, v2, cp, ck, dt if s < steps else 0.0)
     torch.cuda.synchronize()
     assert max(float((a - b).abs().max()) for a, b in zip(v2, v)) < 1e-4 * max(float(t.abs().max()) for t in v)
-    # a second ensemble reads its tile widths from the cache
+    # a second ensemble reads its tile widths and radix splits from the cache
     ens2 = pmpkg.Ensemble(sizes, [n ** 3 for n in sizes], [1.0] * len(sizes), tune_cache=str(cache))
-    assert [c["tile_cols"] for c in ens2.info()["classes"]] == [c["tile_cols"] for c in info["classes"]]
+    shape = lambda i: [(c["tile_cols"], c["radix1"]) for c in i["classes"]]  # noqa: E731
+    assert shape(ens2.info()) == shape(info)
+    # a hand-written cache line (the old five-field form too) is taken as given
+    gpu = cache.read_text().split()[0]
+    cache.write_text(f"{gpu} 32 1 4 16 1\n{gpu} 64 1 4 8\n")
+    ens3 = pmpkg.Ensemble([32, 64], [32 ** 3, 64 ** 3], [1.0, 1.0], tune_cache=str(cache))
+    got = {c["ng"]: (c["tile_cols"], c["radix1"]) for c in ens3.info()["classes"]}
+    assert got == {32: (16, 2), 64: (8, 8)}
+
+
+@pytest.mark.parametrize("ng", [16, 32, 64, 128])
+def test_fft_shapes_agree(pmpkg, ng):
+    """Every tile width x radix split the autotuner may pick gives the same
+    Poisson solution as the default shape (FP32 rounding)."""
+    g = torch.Generator(device="cuda").manual_seed(ng)
+    x = torch.randn((ng, ng, ng), generator=g, device="cuda")
+    plan = pmpkg.Plan(ng, "fp32", "spectral", 4)
+    ref = plan.new_mesh()
+    ref[:, :, :ng] = x
+    plan.poisson(ref, 2.0)
+    default_r1 = {16: 4, 32: 4, 64: 8, 128: 8}[ng]
+    alt_r1 = {16: 2, 32: 2, 64: 4, 128: 4}[ng]
+    for tk in (0, 8, 16, 32):
+        for r1 in (default_r1, alt_r1):
+            plan.set_fft_shape(tk, r1)
+            m = plan.new_mesh()
+            m[:, :, :ng] = x
+            plan.poisson(m, 2.0)
+            err = float((m[:, :, :ng] - ref[:, :, :ng]).norm() / ref[:, :, :ng].norm())
+            assert err < 1e-6, (tk, r1, err)
+    with pytest.raises(pmpkg.PMError):
+        plan.set_fft_shape(12, 0)
+    with pytest.raises(pmpkg.PMError):
+        plan.set_fft_shape(0, 3)
