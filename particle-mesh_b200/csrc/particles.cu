@@ -377,26 +377,30 @@ __global__ void __launch_bounds__(256, 4) k_kick_drift_f32(const float* __restri
     if (pbeg) phi += blockIdx.y * mesh_stride;
     for (long long p = lo + blockIdx.x * (long long)blockDim.x + threadIdx.x; p < hi;
          p += (long long)gridDim.x * blockDim.x) {
+        // the particle arrays are touched once per step: streaming (evict-
+        // first) loads and stores leave L2 to the potential, which the
+        // neighbouring particles re-read
         int i, j, k;
-        unpack_cell(cell[p], i, j, k);
+        unpack_cell(__ldcs(cell + p), i, j, k);
         canon_cell<POW2>(i, j, k, n);
-        const float tx = ox[p], ty = oy[p], tz = oz[p];
+        const float tx = __ldcs(ox + p), ty = __ldcs(oy + p), tz = __ldcs(oz + p);
         float gx, gy, gz;
         force_at<ORDER, POW2>(phi, n, i, j, k, tx, ty, tz, gx, gy, gz);
-        const float ux = vx[p] + gx * c_kick, uy = vy[p] + gy * c_kick, uz = vz[p] + gz * c_kick;
-        vx[p] = ux;
-        vy[p] = uy;
-        vz[p] = uz;
+        const float ux = __ldcs(vx + p) + gx * c_kick, uy = __ldcs(vy + p) + gy * c_kick,
+                    uz = __ldcs(vz + p) + gz * c_kick;
+        __stcs(vx + p, ux);
+        __stcs(vy + p, uy);
+        __stcs(vz + p, uz);
         if (dt != 0.0) {
             int a, b, c;
             float qa, qb, qc;
             split1((double)i + (double)tx + (double)ux * dt, n, a, qa);
             split1((double)j + (double)ty + (double)uy * dt, n, b, qb);
             split1((double)k + (double)tz + (double)uz * dt, n, c, qc);
-            cell[p] = pack_cell(a, b, c);
-            ox[p] = qa;
-            oy[p] = qb;
-            oz[p] = qc;
+            __stcs(cell + p, pack_cell(a, b, c));
+            __stcs(ox + p, qa);
+            __stcs(oy + p, qb);
+            __stcs(oz + p, qc);
         }
     }
 }
