@@ -257,8 +257,11 @@ int pm_interp_f32(pm_plan* plan, const float* phi, const uint32_t* cell, const f
 int pm_kick_drift_f32(pm_plan* plan, const float* phi, uint32_t* cell, float* ox, float* oy,
                       float* oz, float* vx, float* vy, float* vz, int64_t np, double c_kick,
                       double dt);
-/* One full FP32 step on the plan's workspace: deposit, fused Poisson,
- * kick + drift. */
+/* One full FP32 step on the plan's workspace: binning by 4 x 4-cell column
+ * tile, the deposit fused with the z R2C pass (power-of-two ng >= 32; the
+ * tile deposit otherwise), the y / x + Green / y passes, z C2R, then
+ * gradient + interpolation + kick + drift in one pass.  A cell word whose
+ * indices lie outside [0, ng) is taken as the same periodic cell. */
 int pm_step_f32(pm_plan* plan, uint32_t* cell, float* ox, float* oy, float* oz, float* vx,
                 float* vy, float* vz, int64_t np, float mass, double c_poisson, double c_kick,
                 double dt);
