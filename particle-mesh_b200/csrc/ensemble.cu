@@ -2,14 +2,15 @@
 //
 // No counterpart in the reference, which advances one box.  Boxes are grouped
 // into size classes (same ng); each class is one batch: its meshes lie back to
-// back and every kernel of the step (binning, tile deposit, the five FFT
-// passes with the Green multiply, gather + kick + drift) covers all boxes of
-// the class in one launch.  Classes run on their own streams; a whole KDK run
-// is captured once into a CUDA graph with one branch per class and replayed.
-// The column-tile width of the strided FFT passes is chosen per class by
-// timing the candidates (autotune), optionally cached in a text file keyed by
-// GPU name and mesh size (the analogue of the reference's FFTW wisdom file,
-// src/fft/fftw/fft.cpp:28-49).
+// back and every kernel of the step (binning, the deposit - fused with the z
+// R2C pass for power-of-two sizes -, the FFT passes with the Green multiply,
+// gather + kick + drift) covers all boxes of the class in one launch.  Classes
+// run on their own streams; a whole KDK run is captured once into a CUDA graph
+// with one branch per class and replayed.  The shape of the strided FFT
+// passes (column-tile width and radix split) is chosen per class by timing
+// the candidates (autotune), optionally cached in a text file keyed by GPU
+// name, mesh size, Green kind and gradient order (the analogue of the
+// reference's FFTW wisdom file, src/fft/fftw/fft.cpp:28-49).
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
@@ -173,8 +174,14 @@ int enqueue_step(pm_ensemble* e, EnsembleClass& c, uint32_t* cell, float* ox, fl
                  float* vy, float* vz, double c_poisson, double c_kick, double dt) {
     Plan& p = c.plan->p;
     const int nbox = (int)c.boxes.size();
-    int rc = deposit_f32_tiles_batch(p, cell, ox, oy, oz, c.d_pbeg, c.d_pend, nbox, c.np, c.d_mass, c.mesh);
-    if (rc == PM_OK) rc = poisson_fused<float>(p, c.mesh, c_poisson, nbox);
+    int rc;
+    if (zcol_supported(c.ng)) {  // deposit fused with the z R2C pass, as in pm_step_f32
+        rc = deposit_zr2c_f32_batch(p, cell, ox, oy, oz, c.d_pbeg, c.d_pend, nbox, c.np, c.d_mass, c.mesh);
+        if (rc == PM_OK) rc = poisson_after_z_f32(p, c.mesh, c_poisson, nbox);
+    } else {
+        rc = deposit_f32_tiles_batch(p, cell, ox, oy, oz, c.d_pbeg, c.d_pend, nbox, c.np, c.d_mass, c.mesh);
+        if (rc == PM_OK) rc = poisson_fused<float>(p, c.mesh, c_poisson, nbox);
+    }
     if (rc == PM_OK)
         rc = kick_drift_f32_batch(p, c.mesh, cell, ox, oy, oz, vx, vy, vz, c.d_pbeg, c.d_pend, nbox, c.np, c_kick,
                                   dt);

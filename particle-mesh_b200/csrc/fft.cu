@@ -571,13 +571,13 @@ template <typename T> int poisson_fused(const Plan& p, T* mesh, double c_poisson
     return PM_OK;
 }
 
-int poisson_after_z_f32(const Plan& p, float* mesh, double c_poisson) {
+int poisson_after_z_f32(const Plan& p, float* mesh, double c_poisson, int nbox) {
     const double cg = green_scale(p, c_poisson);
     PMB_LAUNCH(p, float, {
-        L_::strided(p, mesh, 1, -1, 1);
-        L_::xgreen(p, mesh, cg, 1);
-        L_::strided(p, mesh, 1, +1, 1);
-        L_::z(p, mesh, false, 1);
+        L_::strided(p, mesh, 1, -1, nbox);
+        L_::xgreen(p, mesh, cg, nbox);
+        L_::strided(p, mesh, 1, +1, nbox);
+        L_::z(p, mesh, false, nbox);
     });
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;

@@ -198,7 +198,10 @@ bool zcol_supported(int ng);
 int deposit_zr2c_prepare(const Plan& p);
 int deposit_zr2c_f32(Plan& p, const uint32_t* cell, const float* ox, const float* oy, const float* oz, int64_t np,
                      float mass, float* mesh);
-int poisson_after_z_f32(const Plan& p, float* mesh, double c_poisson);
+int poisson_after_z_f32(const Plan& p, float* mesh, double c_poisson, int nbox = 1);
+int deposit_zr2c_f32_batch(Plan& p, const uint32_t* cell, const float* ox, const float* oy, const float* oz,
+                           const long long* pbeg, const long long* pend, int nbox, int64_t np_total,
+                           const float* box_mass, float* mesh);
 void tile_scratch_release(Plan& p);
 int interp_f32(const Plan& p, const float* phi, const uint32_t* cell, const float* ox,
                const float* oy, const float* oz, int64_t np, float* fx, float* fy, float* fz);

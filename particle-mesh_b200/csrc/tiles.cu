@@ -362,7 +362,12 @@ template <int N>
 __global__ void __launch_bounds__(zcol_threads<N>(), 3)
 k_deposit_zr2c(const uint32_t* __restrict__ cell, const float* __restrict__ ox, const float* __restrict__ oy,
                const float* __restrict__ oz, const uint32_t* __restrict__ perm, const uint32_t* __restrict__ off,
-               float mass, float* __restrict__ mesh, const float2* __restrict__ tw, int nt) {
+               float mass, float* __restrict__ mesh, const float2* __restrict__ tw, int nt, long long nb_box = 0,
+               long long mesh_stride = 0, const float* __restrict__ box_mass = nullptr) {
+    // a batch of boxes: box blockIdx.y has its own buckets, mesh and mass
+    if (box_mass) mass = __ldg(box_mass + blockIdx.y);
+    off += blockIdx.y * nb_box;
+    mesh += blockIdx.y * mesh_stride;
     constexpr int M = N / 2, R1 = Radix<M>::R1, R2 = Radix<M>::R2, NT = M / R2, RS = z_row_stride<N>();
     constexpr int NTH = zcol_threads<N>();
     using I = ZIdx<R1, R2>;
@@ -615,9 +620,11 @@ int deposit_zr2c_prepare(const Plan& p) {
 
 template <int N>
 static void launch_zcol(const Plan& p, unsigned blocks, const uint32_t* cell, const float* ox, const float* oy,
-                        const float* oz, float mass, float* mesh, const float2* tw, int nt) {
-    k_deposit_zr2c<N><<<blocks, zcol_threads<N>(), kCTRows * z_row_stride<N>() * sizeof(float2), p.stream>>>(
-        cell, ox, oy, oz, p.tiles.perm, p.tiles.off, mass, mesh, tw, nt);
+                        const float* oz, float mass, float* mesh, const float2* tw, int nt, int nbox = 1,
+                        long long nb_box = 0, const float* box_mass = nullptr) {
+    k_deposit_zr2c<N><<<dim3(blocks, nbox), zcol_threads<N>(), kCTRows * z_row_stride<N>() * sizeof(float2),
+                        p.stream>>>(cell, ox, oy, oz, p.tiles.perm, p.tiles.off, mass, mesh, tw, nt, nb_box,
+                                    (long long)mesh_elems(N), box_mass);
 }
 
 // Deposit + z R2C in one pass over the mesh (FP32, power-of-two ng >= 32):
@@ -641,6 +648,47 @@ int deposit_zr2c_f32(Plan& p, const uint32_t* cell, const float* ox, const float
             case 256: launch_zcol<256>(p, blocks, cell, ox, oy, oz, mass, mesh, tw, nt); break;
             case 512: launch_zcol<512>(p, blocks, cell, ox, oy, oz, mass, mesh, tw, nt); break;
             case 1024: launch_zcol<1024>(p, blocks, cell, ox, oy, oz, mass, mesh, tw, nt); break;
+            default: return fail(PM_ERR_SIZE, "fused deposit needs a power-of-two ng >= 32");
+        }
+    }
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+// The same for a batch of nbox boxes of one mesh size (meshes back to back,
+// particles of box b in [pbeg[b], pend[b]), masses box_mass[b]).
+int deposit_zr2c_f32_batch(Plan& p, const uint32_t* cell, const float* ox, const float* oy, const float* oz,
+                           const long long* pbeg, const long long* pend, int nbox, int64_t np_total,
+                           const float* box_mass, float* mesh) {
+    const int nt = p.ng / kCT, cl = 2;  // log2 kCT
+    const long long nb_box = (long long)nt * nt * 4, nb = nb_box * nbox;
+    int rc = tile_scratch_ensure(p, np_total > 0 ? np_total : 1, nbox);
+    if (rc != PM_OK) return rc;
+    TileScratch& s = p.tiles;
+    const long long nscan = (nb + kScanThreads * kScanItems - 1) / (kScanThreads * kScanItems);
+    PMB_CUDA_CHECK(cudaMemsetAsync(s.count, 0, nb * sizeof(uint32_t), p.stream));
+    const long long per_box = (np_total + nbox - 1) / nbox;
+    dim3 g(grid_for(p, per_box, 256, 2), nbox);
+    {
+        Timed t(p, ST_BIN);
+        k_bucket_count<KEY_COLUMN><<<g, 256, 0, p.stream>>>(cell, np_total, cl, nt, s.count, pbeg, pend, nb_box);
+        k_scan_local<<<(unsigned)nscan, kScanThreads, 0, p.stream>>>(s.count, nb, s.off, s.bsum);
+        k_scan_sums<<<1, kScanThreads, 0, p.stream>>>(s.bsum, (int)nscan, s.off + nb);
+        k_scan_add<<<(unsigned)nscan, kScanThreads, 0, p.stream>>>(s.off, s.cursor, nb, s.bsum);
+        k_bucket_scatter<KEY_COLUMN><<<g, 256, 0, p.stream>>>(cell, np_total, cl, nt, s.cursor, s.perm, pbeg, pend,
+                                                              nb_box);
+    }
+    const float2* tw = static_cast<const float2*>(p.tw);
+    {
+        Timed t(p, ST_DEPOSIT);
+        const unsigned blocks = (unsigned)(nt * nt);
+        switch (p.ng) {
+            case 32: launch_zcol<32>(p, blocks, cell, ox, oy, oz, 0.f, mesh, tw, nt, nbox, nb_box, box_mass); break;
+            case 64: launch_zcol<64>(p, blocks, cell, ox, oy, oz, 0.f, mesh, tw, nt, nbox, nb_box, box_mass); break;
+            case 128: launch_zcol<128>(p, blocks, cell, ox, oy, oz, 0.f, mesh, tw, nt, nbox, nb_box, box_mass); break;
+            case 256: launch_zcol<256>(p, blocks, cell, ox, oy, oz, 0.f, mesh, tw, nt, nbox, nb_box, box_mass); break;
+            case 512: launch_zcol<512>(p, blocks, cell, ox, oy, oz, 0.f, mesh, tw, nt, nbox, nb_box, box_mass); break;
+            case 1024: launch_zcol<1024>(p, blocks, cell, ox, oy, oz, 0.f, mesh, tw, nt, nbox, nb_box, box_mass); break;
             default: return fail(PM_ERR_SIZE, "fused deposit needs a power-of-two ng >= 32");
         }
     }
