@@ -89,6 +89,18 @@ __device__ __forceinline__ uint32_t morton_tile(uint32_t c, int ts_log, int nt) 
 // count[key(p)] += 1, aggregated over the lanes of a warp that share a key.
 // Batches: with pbeg != null, grid row blockIdx.y handles the particles
 // [pbeg[b], pend[b]) of box b, whose buckets start at b * nb_box.
+constexpr int kBinU = 4;  // chunks of 32 particles per warp and round in the binning kernels
+
+// Bucket key of particle p (0xffffffff past the end; no bucket has that key).
+template <int KEY>
+__device__ __forceinline__ uint32_t bin_key(const uint32_t* __restrict__ cell, long long p, long long hi, uint32_t kb,
+                                            int ts_log, int nt) {
+    if (p >= hi) return 0xffffffffu;
+    const uint32_t c = __ldg(cell + p);
+    return kb + (KEY == KEY_MORTON ? morton_tile(c, ts_log, nt)
+                                   : (KEY == KEY_COLUMN ? column_bucket_of(c, ts_log, nt) : bucket_of(c, ts_log, nt)));
+}
+
 template <int KEY>
 __global__ void k_bucket_count(const uint32_t* __restrict__ cell, long long np, int ts_log, int nt,
                                uint32_t* __restrict__ count, const long long* __restrict__ pbeg = nullptr,
@@ -98,17 +110,16 @@ __global__ void k_bucket_count(const uint32_t* __restrict__ cell, long long np, 
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
     const long long lo = pbeg ? pbeg[blockIdx.y] : 0, hi = pbeg ? pend[blockIdx.y] : np;
     const uint32_t kb = pbeg ? (uint32_t)(blockIdx.y * nb_box) : 0u;
-    for (long long base = lo + warp * 32; base < hi; base += nwarps * 32) {
-        const long long p = base + lane;
-        const bool valid = p < hi;
-        uint32_t key = 0xffffffffu;
-        if (valid) {
-            const uint32_t c = __ldg(cell + p);
-            key = kb + (KEY == KEY_MORTON ? morton_tile(c, ts_log, nt)
-                                          : (KEY == KEY_COLUMN ? column_bucket_of(c, ts_log, nt) : bucket_of(c, ts_log, nt)));
+    // kBinU chunks of 32 particles per warp and round, their loads in flight together
+    for (long long base = lo + warp * 32 * kBinU; base < hi; base += nwarps * 32 * kBinU) {
+        uint32_t key[kBinU];
+#pragma unroll
+        for (int u = 0; u < kBinU; ++u) key[u] = bin_key<KEY>(cell, base + u * 32 + lane, hi, kb, ts_log, nt);
+#pragma unroll
+        for (int u = 0; u < kBinU; ++u) {
+            const unsigned peers = __match_any_sync(0xffffffffu, key[u]);
+            if (key[u] != 0xffffffffu && lane == __ffs(peers) - 1) atomicAdd(count + key[u], (uint32_t)__popc(peers));
         }
-        const unsigned peers = __match_any_sync(0xffffffffu, key);
-        if (valid && lane == __ffs(peers) - 1) atomicAdd(count + key, (uint32_t)__popc(peers));
     }
 }
 
@@ -124,21 +135,25 @@ __global__ void k_bucket_scatter(const uint32_t* __restrict__ cell, long long np
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
     const long long lo = pbeg ? pbeg[blockIdx.y] : 0, hi = pbeg ? pend[blockIdx.y] : np;
     const uint32_t kb = pbeg ? (uint32_t)(blockIdx.y * nb_box) : 0u;
-    for (long long base = lo + warp * 32; base < hi; base += nwarps * 32) {
-        const long long p = base + lane;
-        const bool valid = p < hi;
-        uint32_t key = 0xffffffffu;
-        if (valid) {
-            const uint32_t c = __ldg(cell + p);
-            key = kb + (KEY == KEY_MORTON ? morton_tile(c, ts_log, nt)
-                                          : (KEY == KEY_COLUMN ? column_bucket_of(c, ts_log, nt) : bucket_of(c, ts_log, nt)));
+    // kBinU chunks per round: loads, then all cursor atomics, then the stores,
+    // so the round trips of the chunks overlap
+    for (long long base = lo + warp * 32 * kBinU; base < hi; base += nwarps * 32 * kBinU) {
+        uint32_t key[kBinU], at[kBinU];
+        unsigned peers[kBinU];
+#pragma unroll
+        for (int u = 0; u < kBinU; ++u) key[u] = bin_key<KEY>(cell, base + u * 32 + lane, hi, kb, ts_log, nt);
+#pragma unroll
+        for (int u = 0; u < kBinU; ++u) {
+            peers[u] = __match_any_sync(0xffffffffu, key[u]);
+            at[u] = 0;
+            if (key[u] != 0xffffffffu && lane == __ffs(peers[u]) - 1)
+                at[u] = atomicAdd(cursor + key[u], (uint32_t)__popc(peers[u]));
         }
-        const unsigned peers = __match_any_sync(0xffffffffu, key);
-        const int leader = __ffs(peers) - 1;
-        uint32_t at = 0;
-        if (valid && lane == leader) at = atomicAdd(cursor + key, (uint32_t)__popc(peers));
-        at = __shfl_sync(0xffffffffu, at, leader);
-        if (valid) perm[at + __popc(peers & lt)] = (uint32_t)p;
+#pragma unroll
+        for (int u = 0; u < kBinU; ++u) {
+            const uint32_t a = __shfl_sync(0xffffffffu, at[u], __ffs(peers[u]) - 1);
+            if (key[u] != 0xffffffffu) perm[a + __popc(peers[u] & lt)] = (uint32_t)(base + u * 32 + lane);
+        }
     }
 }
 
