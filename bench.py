@@ -325,20 +325,22 @@ def ours(args):
     value = throughput(world, np_, args.steps, t_ms)
     launches = sum(n for _, n in stages.values())
 
+    # every stage runs once per step (binning is five kernel launches, every
+    # other stage one), so bytes and times are per step, launches counted apart
     peak, peak_kind = measured_peaks()
     dom = max(stages, key=lambda s: stages[s][0])
-    dom_ms = stages[dom][0] / stages[dom][1]
+    dom_ms = stages[dom][0] / args.steps
     dom_bytes = stage_bytes(dom, ng, np_, 4)
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9
     traffic = ncu_traffic(dom, ng)
-    step_bytes = sum(stage_bytes(s, ng, np_, 4) * n / args.steps for s, (_, n) in stages.items())
+    step_bytes = sum(stage_bytes(s, ng, np_, 4) for s in stages)
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs (copy bandwidth)",
                 "traffic": traffic, "algorithmic_bytes_per_launch": dom_bytes, "ms_per_launch": dom_ms,
                 "step": {"algorithmic_bytes": step_bytes, "achieved": step_bytes / (t_ms / args.steps / 1e3) / 1e9,
                          "frac": step_bytes / (t_ms / args.steps / 1e3) / 1e9 / peak}}
     per_stage = {s: {"ms_per_step": ms / args.steps, "launches": n,
-                     "gbs": stage_bytes(s, ng, np_, 4) * n / (ms / 1e3) / 1e9 if ms > 0 else None}
+                     "gbs": stage_bytes(s, ng, np_, 4) * args.steps / (ms / 1e3) / 1e9 if ms > 0 else None}
                  for s, (ms, n) in stages.items()}
 
     # ---- FP64 plain path on the same initial state + force error
@@ -373,7 +375,7 @@ def ours(args):
         barrier()
         t64 = max_over_ranks(e0.elapsed_time(e1))
         st64 = p64.read_timing(reset=True)
-        b64 = sum(stage_bytes(s, ng, np_, 8) * n / args.steps for s, (_, n) in st64.items())
+        b64 = sum(stage_bytes(s, ng, np_, 8) for s in st64)
         fp64 = {"value": throughput(world, np_, args.steps, t64), "unit": UNIT, "ms_per_step": t64 / args.steps,
                 "roofline": {"bound": "hbm", "algorithmic_bytes_per_step": b64,
                              "achieved": b64 / (t64 / args.steps / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
@@ -381,7 +383,7 @@ def ours(args):
                 "dtype": "f64", "path": "plain FP64: separate deposit, 3+3 FFT passes, Green, gradient to 3 force "
                                         "meshes, interpolate + kick, drift",
                 "stages": {s: {"ms_per_step": ms / args.steps, "launches": n,
-                               "gbs": stage_bytes(s, ng, np_, 8) * n / (ms / 1e3) / 1e9 if ms > 0 else None}
+                               "gbs": stage_bytes(s, ng, np_, 8) * args.steps / (ms / 1e3) / 1e9 if ms > 0 else None}
                            for s, (ms, n) in st64.items()}}
         p64.close()
         del p64, x, y, z, pv

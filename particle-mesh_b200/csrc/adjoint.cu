@@ -186,7 +186,7 @@ int adjoint_mesh_source_f64(const Plan& p, const double* x, const double* y, con
     const size_t cells = (size_t)p.ng * p.ng * p.ng;
     for (int a = 0; a < 3; ++a) PMB_CUDA_CHECK(cudaMemsetAsync(ub[a], 0, cells * sizeof(double), p.stream));
     {
-        Timed t(p, ST_ADJOINT);
+        Timed t(p, ST_ADJOINT, np > 0 ? 2 : 1);
         if (np > 0)
             k_deposit3_f64<<<grid_for(p, np, 256), 256, 0, p.stream>>>(x, y, z, u[0], u[1], u[2], np, ub[0], ub[1],
                                                                       ub[2], p.ng);

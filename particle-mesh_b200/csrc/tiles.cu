@@ -495,7 +495,7 @@ int bucket_sort(const Plan& p, const uint32_t* cell, int64_t np, int ts_log, int
     PMB_CUDA_CHECK(cudaMemsetAsync(s.count, 0, nb * sizeof(uint32_t), p.stream));
     const unsigned g = grid_for(p, np, 256);
     {
-        Timed t(p, ST_BIN);
+        Timed t(p, ST_BIN, np > 0 ? 5 : 3);  // count, three scan kernels, scatter
         if (np > 0) k_bucket_count<KEY><<<g, 256, 0, p.stream>>>(cell, np, ts_log, nt, s.count);
         k_scan_local<<<(unsigned)nscan, kScanThreads, 0, p.stream>>>(s.count, nb, s.off, s.bsum);
         k_scan_sums<<<1, kScanThreads, 0, p.stream>>>(s.bsum, (int)nscan, s.off + nb);
@@ -591,7 +591,7 @@ int deposit_f32_tiles_batch(Plan& p, const uint32_t* cell, const float* ox, cons
     const long long per_box = (np_total + nbox - 1) / nbox;
     dim3 g(grid_for(p, per_box, 256, 2), nbox);
     {
-        Timed t(p, ST_BIN);
+        Timed t(p, ST_BIN, 5);  // count, three scan kernels, scatter
         k_bucket_count<KEY_TILE3><<<g, 256, 0, p.stream>>>(cell, np_total, tl, nt, s.count, pbeg, pend, nb_box);
         k_scan_local<<<(unsigned)nscan, kScanThreads, 0, p.stream>>>(s.count, nb, s.off, s.bsum);
         k_scan_sums<<<1, kScanThreads, 0, p.stream>>>(s.bsum, (int)nscan, s.off + nb);
@@ -685,7 +685,7 @@ int deposit_zr2c_f32_batch(Plan& p, const uint32_t* cell, const float* ox, const
     const long long per_box = (np_total + nbox - 1) / nbox;
     dim3 g(grid_for(p, per_box, 256, 2), nbox);
     {
-        Timed t(p, ST_BIN);
+        Timed t(p, ST_BIN, 5);  // count, three scan kernels, scatter
         k_bucket_count<KEY_COLUMN><<<g, 256, 0, p.stream>>>(cell, np_total, cl, nt, s.count, pbeg, pend, nb_box);
         k_scan_local<<<(unsigned)nscan, kScanThreads, 0, p.stream>>>(s.count, nb, s.off, s.bsum);
         k_scan_sums<<<1, kScanThreads, 0, p.stream>>>(s.bsum, (int)nscan, s.off + nb);

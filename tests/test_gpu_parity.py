@@ -446,6 +446,26 @@ def test_split_run_tracks_fp64_over_50_kdk_steps(pmpkg, O):
     assert float((d32 - d64).norm() / (d64 + 1.0).norm()) < 1e-4
 
 
+def test_stage_timers_count_every_kernel_of_a_step(pmpkg, O):
+    """The stage timers that bench.py's gpu_launches comes from count each
+    kernel launch of pm_step_f32: binning (count, three scans, scatter), the
+    fused deposit, y / x + Green / y passes, z C2R and the gather: 11."""
+    ng, nrow = 64, 32
+    pos, vel = O.zeldovich_ic(ng, nrow, -2.0, 0.5, seed=9)
+    plan = pmpkg.Plan(ng, "fp32", "spectral", 4)
+    cell, off = plan.split(*(T(a) for a in pos))
+    v = [T(a, torch.float32) for a in vel]
+    plan.read_timing(reset=True)
+    plan.set_timing(True)
+    plan.step_split(cell, off, v, ng ** 3 / nrow ** 3, 4 * np.pi, 0.01, 0.01)
+    t = plan.read_timing(reset=True)
+    plan.set_timing(False)
+    n = {k: c for k, (_, c) in t.items()}
+    assert n == {"bin": 5, "deposit": 1, "fft_y_fwd": 1, "fft_x_green": 1, "fft_y_inv": 1, "fft_z_c2r": 1,
+                 "kick_drift": 1}, n
+    assert all(ms > 0 for ms, _ in t.values())
+
+
 def test_split_step_kick_drift(pmpkg, O):
     ng, nrow = 64, 32
     pos, vel = O.zeldovich_ic(ng, nrow, -2.0, 0.5, seed=3)
