@@ -466,6 +466,30 @@ def test_stage_timers_count_every_kernel_of_a_step(pmpkg, O):
     assert all(ms > 0 for ms, _ in t.values())
 
 
+@pytest.mark.parametrize("ng", [48, 64])
+def test_empty_particle_set_through_every_step(pmpkg, ng):
+    """np = 0: the FP64 and FP32 steps (fused deposit at 64, tile deposit at
+    48), the adjoints and the reductions run without error; the density is
+    the uniform -1 background, so the potential vanishes."""
+    e64 = [torch.zeros(0, dtype=torch.float64, device=DEV) for _ in range(6)]
+    e32 = [torch.zeros(0, dtype=torch.float32, device=DEV) for _ in range(6)]
+    ecell = torch.zeros(0, dtype=torch.int32, device=DEV)
+    p32 = pmpkg.Plan(ng, "fp32", "spectral", 4)
+    p32.step_split(ecell, e32[:3], e32[3:], 1.0, 4 * np.pi, 0.01, 0.01)
+    assert float(p32.workspace_mesh()[:, :, :ng].abs().max()) < 1e-6
+    p32.step_adjoint_split(ecell, e32[:3], 1.0, 4 * np.pi, 0.01, 0.01, e32[:3], e32[3:])
+    m = p32.deposit_split(ecell, e32[:3], 1.0)
+    assert torch.all(m[:, :, :ng] == -1.0)
+    c = p32.conserved(m, e32[3:], 1.0)
+    assert c["mass"] == 0.0 and c["momentum"] == [0.0, 0.0, 0.0]
+    if ng & (ng - 1) == 0:
+        p64 = pmpkg.Plan(ng, "fp64", "spectral", 4)
+        p64.step(*e64, 1.0, 4 * np.pi, 0.01, 0.01)
+        assert float(p64.workspace_mesh()[:, :, :ng].abs().max()) < 1e-12
+        p64.step_adjoint(*e64[:3], 1.0, 4 * np.pi, 0.01, 0.01, e64[:3], e64[3:])
+    p32.check()
+
+
 def test_split_step_kick_drift(pmpkg, O):
     ng, nrow = 64, 32
     pos, vel = O.zeldovich_ic(ng, nrow, -2.0, 0.5, seed=3)
