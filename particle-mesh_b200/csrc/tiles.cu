@@ -509,6 +509,8 @@ int bucket_sort(const Plan& p, const uint32_t* cell, int64_t np, int ts_log, int
 }  // namespace
 
 int tile_scratch_ensure(Plan& p, int64_t np, int nbox) {
+    // the permutation and the bucket offsets are 32-bit particle indices
+    if (np > (int64_t)0xffffffffll) return fail(PM_ERR_SIZE, "the FP32 binning holds at most 2^32 - 1 particles");
     const int ts = 1 << tile_log(p.ng), nt = p.ng / ts;
     int nt2 = 1;  // the sort's Morton keys need nt2^3 buckets
     while (nt2 < nt) nt2 <<= 1;

@@ -490,6 +490,24 @@ def test_empty_particle_set_through_every_step(pmpkg, ng):
     p32.check()
 
 
+def test_fp32_paths_reject_more_than_2_32_particles(pmpkg):
+    """The FP32 binning indexes particles with 32 bits: a count of 2^32 is
+    refused with PM_ERR_SIZE before any kernel runs (the small arrays passed
+    here are never read)."""
+    import ctypes
+    plan = pmpkg.Plan(64, "fp32")
+    a = [torch.zeros(16, dtype=torch.float32, device=DEV) for _ in range(7)]
+    c = torch.zeros(16, dtype=torch.int32, device=DEV)
+    mesh = plan.new_mesh()
+    vp = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    big = 1 << 32
+    rc = plan.lib.pm_deposit_f32(plan.handle, vp(c), vp(a[0]), vp(a[1]), vp(a[2]), big, 1.0, vp(mesh))
+    assert rc == 2 and b"2^32" in plan.lib.pm_last_error()
+    rc = plan.lib.pm_step_f32(plan.handle, vp(c), *(vp(t) for t in a[:6]), big, 1.0, 1.0, 0.01, 0.01)
+    assert rc == 2
+    torch.cuda.synchronize()
+
+
 def test_split_step_kick_drift(pmpkg, O):
     ng, nrow = 64, 32
     pos, vel = O.zeldovich_ic(ng, nrow, -2.0, 0.5, seed=3)
