@@ -148,12 +148,18 @@ k_fft_z_c2r(T* __restrict__ mesh, long long nrows, const typename Cx<T>::t* __re
 template <int N, int TK, int RV = 0> constexpr int strided_threads() { return TK * threads_per_line_v<N, RV>(); }
 template <int N, int TK, int RV = 0> constexpr int strided_smem_elems() { return (N + N / RadixV<N, RV>::R1) * TK; }
 
-template <typename T, int N, int DIR, int TK, int RV = 0>
+template <typename T, int N, int DIR, int TK, int RV = 0, int AX = -1>
 __global__ void __launch_bounds__(strided_threads<N, TK, RV>(), 2)
-k_fft_strided(typename Cx<T>::t* __restrict__ data, long long es, long long os, long long bs, int ncols,
+k_fft_strided(typename Cx<T>::t* __restrict__ data, long long es_, long long os_, long long bs, int ncols,
               const typename Cx<T>::t* __restrict__ tw) {
     using C = typename Cx<T>::t;
     constexpr int R1 = RadixV<N, RV>::R1, R2 = RadixV<N, RV>::R2;
+    // AX = 1 (y) or 0 (x): the element and plane strides of the padded
+    // spectrum are compile-time constants, so the 2 R2 accesses of a thread
+    // are one base address plus constant offsets; AX = -1 takes them as given
+    constexpr long long H = N / 2 + 1;
+    const long long es = AX == 1 ? H : (AX == 0 ? (long long)N * H : es_);
+    const long long os = AX == 1 ? (long long)N * H : (AX == 0 ? H : os_);
     extern __shared__ __align__(16) unsigned char smraw[];
     C* S = reinterpret_cast<C*>(smraw);
     const int tx = threadIdx.x % TK, ty = threadIdx.x / TK;
@@ -201,10 +207,15 @@ __device__ __forceinline__ T green_value(int kx, int ky, int kz, int kind, doubl
 // inverse FFT along x, for TK kz columns of one ky plane.
 template <typename T, int N, int TK, int RV = 0>
 __global__ void __launch_bounds__(strided_threads<N, TK, RV>(), 2)
-k_fft_x_green(typename Cx<T>::t* __restrict__ data, long long es, long long os, long long bs, int ncols,
+k_fft_x_green(typename Cx<T>::t* __restrict__ data, long long es_, long long os_, long long bs, int ncols,
               const typename Cx<T>::t* __restrict__ tw, const T* __restrict__ g1d, double cg, int kind) {
     using C = typename Cx<T>::t;
     constexpr int R1 = RadixV<N, RV>::R1, R2 = RadixV<N, RV>::R2;
+    // x lines of the padded spectrum: compile-time strides (es_ = N H and
+    // os_ = H are what every caller passes)
+    constexpr long long es = (long long)N * (N / 2 + 1), os = N / 2 + 1;
+    (void)es_;
+    (void)os_;
     extern __shared__ __align__(16) unsigned char smraw[];
     C* S = reinterpret_cast<C*>(smraw);
     const int tx = threadIdx.x % TK, ty = threadIdx.x / TK;
@@ -387,8 +398,10 @@ template <typename T, int N, int TK = tk_cols<T, N>(), int RV = 0> struct Launch
     static int prepare() {
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_z_r2c<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_z()));
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_z_c2r<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_z()));
-        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, -1, TK, RV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
-        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, +1, TK, RV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
+        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, -1, TK, RV, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
+        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, +1, TK, RV, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
+        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, -1, TK, RV, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
+        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, +1, TK, RV, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_x_green<T, N, TK, RV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         return PM_OK;
     }
@@ -412,10 +425,18 @@ template <typename T, int N, int TK = tk_cols<T, N>(), int RV = 0> struct Launch
         dim3 grid((H + TK - 1) / TK, N * nbox);
         const C* tw = static_cast<const C*>(p.tw);
         Timed t(p, axis == 1 ? (dir < 0 ? ST_FFT_Y_FWD : ST_FFT_Y_INV) : (dir < 0 ? ST_FFT_X_FWD : ST_FFT_X_INV));
-        if (dir < 0)
-            k_fft_strided<T, N, -1, TK, RV><<<grid, strided_threads<N, TK, RV>(), smem_s(), p.stream>>>(d, es, os, bs, H, tw);
-        else
-            k_fft_strided<T, N, +1, TK, RV><<<grid, strided_threads<N, TK, RV>(), smem_s(), p.stream>>>(d, es, os, bs, H, tw);
+        auto go = [&](auto dirc, auto axc) {
+            k_fft_strided<T, N, decltype(dirc)::value, TK, RV, decltype(axc)::value>
+                <<<grid, strided_threads<N, TK, RV>(), smem_s(), p.stream>>>(d, es, os, bs, H, tw);
+        };
+        using F = std::integral_constant<int, -1>;
+        using B = std::integral_constant<int, +1>;
+        using AY = std::integral_constant<int, 1>;
+        using AXc = std::integral_constant<int, 0>;
+        if (dir < 0 && axis == 1) go(F{}, AY{});
+        else if (dir < 0) go(F{}, AXc{});
+        else if (axis == 1) go(B{}, AY{});
+        else go(B{}, AXc{});
     }
     static void xgreen(const Plan& p, T* mesh, double cg, int nbox = 1) {
         C* d = reinterpret_cast<C*>(mesh);
