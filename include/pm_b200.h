@@ -53,7 +53,7 @@ extern "C" {
 /* status codes */
 #define PM_OK 0
 #define PM_ERR_ARG 1          /* null pointer, negative count, bad enum   */
-#define PM_ERR_SIZE 2         /* mesh size not supported by this build    */
+#define PM_ERR_SIZE 2         /* size not supported by the library         */
 #define PM_ERR_CUDA 3         /* CUDA runtime error                        */
 #define PM_ERR_NOMEM 4        /* device allocation failed                  */
 #define PM_ERR_RANGE 5        /* a particle position was NaN or outside

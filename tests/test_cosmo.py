@@ -145,7 +145,7 @@ def test_driver_cosmo_snapshot(pmpkg, tmp_path):
     d = pmpkg.read_snapshot(str(snap))
     assert (d["ng"], d["np"]) == (16, 16 ** 3)
     assert d["a"] == pytest.approx(0.9 + 5 * 0.001)
-    # the same run through the Python mirror from the driver's initial state
+    # the same run through the Python mirror from pm_main's initial state
     g = load_golden("ref_step_ng16_np16.npz")
     pos = [torch.tensor(g["pos"][i], device="cuda") for i in range(3)]
     mom = [torch.zeros(16 ** 3, dtype=torch.float64, device="cuda") for _ in range(3)]
