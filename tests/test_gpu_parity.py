@@ -119,6 +119,24 @@ def test_fft_and_poisson_f32_large_match_f64(pmpkg, ng, kind):
     torch.cuda.empty_cache()
 
 
+@pytest.mark.parametrize("ng", [64, 512])
+def test_fft_f32_cross_checks_against_cufft(pmpkg, ng):
+    """The hand-written FP32 R2C against cuFFT (torch.fft.rfftn on the GPU),
+    cuFFT only as an independent cross-check: relative L2 < 2e-6."""
+    g = torch.Generator(device=DEV).manual_seed(ng + 3)
+    x = torch.randn((ng, ng, ng), generator=g, device=DEV, dtype=torch.float32)
+    plan = pmpkg.Plan(ng, "fp32")
+    d = plan.new_mesh()
+    d[:, :, :ng] = x
+    plan.fft_r2c(d)
+    ours = torch.view_as_complex(d.view(ng, ng, ng // 2 + 1, 2))
+    ref = torch.fft.rfftn(x.double())
+    err = float((ours.to(torch.complex128) - ref).abs().norm() / ref.abs().norm())
+    assert err < 2e-6, err
+    del d, x, ours, ref
+    torch.cuda.empty_cache()
+
+
 @pytest.mark.parametrize("kind", ["discrete", "spectral"])
 @pytest.mark.parametrize("prec", ["fp64", "fp32"])
 def test_green_and_fused_poisson(pmpkg, O, kind, prec):
