@@ -16,6 +16,7 @@ over every particle; particle-updates/s = particles x steps / time.
   roofline   dominant kernel, algorithmic bytes / CUDA-event time, vs the
              measured HBM copy bandwidth
   cpu_baseline the reference's CPU code on a bounded sample (rank 0, N = 1)
+  fp64_256   the FP64 path on 256^3 particles / 256^3 mesh, 20 KDK steps
   accuracy   FP32 vs FP64 after the configuration's 50 KDK steps (positions,
              velocities, density) and FP64-summed mass / momentum drift
   adjoint    adjoint step vs forward step at 128^3 (FP32 split path; FP64 check
@@ -496,6 +497,32 @@ def ours(args):
             del pla, xb, vb, xs, vs
         del pa, va
 
+    # ---- the FP64 configuration checked against the reference: 256^3
+    # particles on a 256^3 mesh, P(k) ~ k^-2, rms 0.5 cell, 20 KDK steps at
+    # dt = 0.01 (parity with the reference is in the tests; this times it)
+    c2 = None
+    if not args.skip_fp64:
+        n2 = 256
+        pos2, vel2 = pm.zeldovich_ic(n2, n2, -2.0, 0.5, 21 + rank, device=dev)
+        p2 = pm.Plan(n2, "fp64", "spectral", 4, stream=stream, device=dev)
+        s2, d2 = 20, 0.01
+        sched2 = [(0.5 * d2 if s in (0, s2) else d2, d2 if s < s2 else 0.0) for s in range(s2 + 1)]
+        p2.step(*pos2, *vel2, 1.0, cp, 0.0, 0.0)  # warm-up (no kick, no drift)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for ckk, dd in sched2:
+            p2.step(*pos2, *vel2, 1.0, cp, ckk, dd)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        p2.check()
+        t2 = e0.elapsed_time(e1)
+        c2 = {"config": "256^3 particles on 256^3 mesh, FP64, P(k)~k^-2, rms 0.5 cell, 20 KDK steps dt=0.01 "
+                        "(21 force evaluations)",
+              "value": n2 ** 3 * len(sched2) / (t2 / 1e3), "unit": UNIT, "ms_per_step": t2 / len(sched2)}
+        p2.close()
+        del p2, pos2, vel2
+        torch.cuda.empty_cache()
+
     # ---- batched ensemble: 256 boxes of mixed mesh sizes, 20 KDK steps per graph
     ensemble = None
     if not args.skip_ensemble:
@@ -609,7 +636,7 @@ def ours(args):
                        "parallelism": f"{world} independent boxes, one per GPU"},
             "fp64": fp64, "force_err": force_err,
             "speedup_fp32_vs_fp64": (value / fp64["value"]) if fp64 and "value" in fp64 else None,
-            "e2e": e2e, "accuracy": accuracy, "adjoint": adjoint, "ensemble": ensemble, "gpu_launches": launches, "roofline": roofline, "stages": per_stage,
+            "e2e": e2e, "accuracy": accuracy, "fp64_256": c2, "adjoint": adjoint, "ensemble": ensemble, "gpu_launches": launches, "roofline": roofline, "stages": per_stage,
             "cpu_baseline": cpu, "clocks": clocks}
     print(json.dumps(line), flush=True)
     return 0
