@@ -50,20 +50,26 @@ template <int R1, int R2, int TK> struct SIdx {  // strided passes, row stride T
 // Real rows of N (+2 padding) at a row stride of N+2 reals; as complex a row
 // is M+1 = N/2+1 entries.  NT threads per row, LPB rows per block.
 template <int N> constexpr int z_threads_per_row() { return threads_per_line<N / 2>(); }
-template <typename T, int N> constexpr int z_rows_per_block() {
-    constexpr int l = (sizeof(T) == 4 ? 256 : 128) / z_threads_per_row<N>();
+// Small blocks (64 threads: 4 rows of 1024 in FP32) let many independent
+// blocks per SM interleave their load and compute phases; the FP64 R2C runs
+// best with 128 (measured on B200).
+template <typename T, int N, bool C2R> constexpr int z_rows_per_block() {
+    constexpr int thr = (sizeof(T) == 4 || C2R) ? 64 : 128;
+    constexpr int l = thr / z_threads_per_row<N>();
     return l < 1 ? 1 : (l > 64 ? 64 : l);
 }
-template <typename T, int N> constexpr int z_threads() { return z_threads_per_row<N>() * z_rows_per_block<T, N>(); }
+template <typename T, int N, bool C2R> constexpr int z_threads() {
+    return z_threads_per_row<N>() * z_rows_per_block<T, N, C2R>();
+}
 
 // R2C along z: complex FFT of the M packed pairs (x[2n], x[2n+1]), then
 // X[k] = E[k] + W_N^k O[k], E = (Z[k] + conj Z[M-k]) / 2, O = -i (Z[k] - conj Z[M-k]) / 2.
 template <typename T, int N>
-__global__ void __launch_bounds__(z_threads<T, N>(), 2)
+__global__ void __launch_bounds__(z_threads<T, N, false>(), 2)
 k_fft_z_r2c(T* __restrict__ mesh, long long nrows, const typename Cx<T>::t* __restrict__ tw) {
     using C = typename Cx<T>::t;
     constexpr int M = N / 2, R1 = Radix<M>::R1, R2 = Radix<M>::R2;
-    constexpr int NT = z_threads_per_row<N>(), LPB = z_rows_per_block<T, N>();
+    constexpr int NT = z_threads_per_row<N>(), LPB = z_rows_per_block<T, N, false>();
     extern __shared__ __align__(16) unsigned char smraw[];
     C* S = reinterpret_cast<C*>(smraw) + (threadIdx.x / NT) * z_row_stride<N>();
     const int tj = threadIdx.x % NT;
@@ -97,11 +103,11 @@ k_fft_z_r2c(T* __restrict__ mesh, long long nrows, const typename Cx<T>::t* __re
 // inverse complex FFT of M, unpacked to reals.  The imaginary parts of X[0]
 // and X[M] are ignored (FFTW c2r semantics); the row padding is zeroed.
 template <typename T, int N>
-__global__ void __launch_bounds__(z_threads<T, N>(), 2)
+__global__ void __launch_bounds__(z_threads<T, N, true>(), 2)
 k_fft_z_c2r(T* __restrict__ mesh, long long nrows, const typename Cx<T>::t* __restrict__ tw) {
     using C = typename Cx<T>::t;
     constexpr int M = N / 2, R1 = Radix<M>::R1, R2 = Radix<M>::R2;
-    constexpr int NT = z_threads_per_row<N>(), LPB = z_rows_per_block<T, N>();
+    constexpr int NT = z_threads_per_row<N>(), LPB = z_rows_per_block<T, N, true>();
     extern __shared__ __align__(16) unsigned char smraw[];
     C* S = reinterpret_cast<C*>(smraw) + (threadIdx.x / NT) * z_row_stride<N>();
     const int tj = threadIdx.x % NT;
@@ -393,11 +399,14 @@ template <typename T, int N, int TK = kGTK> struct LaunchG {
 template <typename T, int N, int TK = tk_cols<T, N>(), int RV = 0> struct Launch {
     using C = typename Cx<T>::t;
     static constexpr int H = N / 2 + 1;
-    static size_t smem_z() { return (size_t)z_rows_per_block<T, N>() * z_row_stride<N>() * sizeof(C); }
+    static size_t smem_z(bool c2r) {
+        return (size_t)(c2r ? z_rows_per_block<T, N, true>() : z_rows_per_block<T, N, false>()) * z_row_stride<N>() *
+               sizeof(C);
+    }
     static size_t smem_s() { return (size_t)strided_smem_elems<N, TK, RV>() * sizeof(C); }
     static int prepare() {
-        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_z_r2c<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_z()));
-        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_z_c2r<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_z()));
+        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_z_r2c<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_z(false)));
+        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_z_c2r<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_z(true)));
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, -1, TK, RV, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, +1, TK, RV, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, -1, TK, RV, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
@@ -407,14 +416,15 @@ template <typename T, int N, int TK = tk_cols<T, N>(), int RV = 0> struct Launch
     }
     static void z(const Plan& p, T* mesh, bool forward, int nbox = 1) {
         const long long rows = (long long)nbox * N * N;
-        const unsigned grid = (unsigned)((rows + z_rows_per_block<T, N>() - 1) / z_rows_per_block<T, N>());
-        const int thr = z_threads_per_row<N>() * z_rows_per_block<T, N>();
+        const int lpb = forward ? z_rows_per_block<T, N, false>() : z_rows_per_block<T, N, true>();
+        const unsigned grid = (unsigned)((rows + lpb - 1) / lpb);
+        const int thr = z_threads_per_row<N>() * lpb;
         const C* tw = static_cast<const C*>(p.tw);
         Timed t(p, forward ? ST_FFT_Z_R2C : ST_FFT_Z_C2R);
         if (forward)
-            k_fft_z_r2c<T, N><<<grid, thr, smem_z(), p.stream>>>(mesh, rows, tw);
+            k_fft_z_r2c<T, N><<<grid, thr, smem_z(false), p.stream>>>(mesh, rows, tw);
         else
-            k_fft_z_c2r<T, N><<<grid, thr, smem_z(), p.stream>>>(mesh, rows, tw);
+            k_fft_z_c2r<T, N><<<grid, thr, smem_z(true), p.stream>>>(mesh, rows, tw);
     }
     // axis 1 = y (stride H, planes x), axis 0 = x (stride N H, planes y); a
     // batch of nbox meshes lies at a stride of N^2 H complex
