@@ -90,15 +90,31 @@ void release(Plan& p) {
         if (f) cudaFree(f), f = nullptr;
     if (p.adjm) cudaFree(p.adjm);
     if (p.red) cudaFree(p.red);
-    p.tw = p.g1d = p.mesh = p.adjm = p.red = nullptr;
+    if (p.xspec) cudaFree(p.xspec);
+    p.tw = p.g1d = p.mesh = p.adjm = p.red = p.xspec = nullptr;
     p.d_err = nullptr;
     delete p.timers;
     p.timers = nullptr;
     tile_scratch_release(p);
 }
 
+// FP32 plans of a power-of-two mesh >= 512 get the transposed half spectrum
+// that lets the x + Green pass write its lines at element stride H (the
+// Poisson solve runs in place without it, e.g. when this allocation fails).
+void ensure_xspec(Plan& p) {
+    if (p.xspec || p.precision != PM_FP32 || p.ng < 512 || (p.ng & (p.ng - 1)) != 0) return;
+    const size_t b = (size_t)p.ng * p.ng * (p.ng / 2 + 1) * 2 * sizeof(float);
+    if (cudaMalloc(&p.xspec, b) != cudaSuccess) {
+        cudaGetLastError();
+        p.xspec = nullptr;
+        return;
+    }
+    p.bytes += b;
+}
+
 int ensure_workspace(Plan& p, bool forces, bool adjoint = false) {
     const size_t esz = p.precision == PM_FP64 ? sizeof(double) : sizeof(float);
+    ensure_xspec(p);
     if (!p.mesh) {
         if (cudaMalloc(&p.mesh, mesh_elems(p.ng) * esz) != cudaSuccess) {
             cudaGetLastError();
@@ -514,6 +530,7 @@ int pm_poisson_f32(pm_plan* plan, float* mesh, double c_poisson) {
     PM_TRY(check_plan(plan, PM_FP32));
     if (!mesh) return fail(PM_ERR_ARG, "mesh is NULL");
     PM_TRY(set_device(plan->p));
+    ensure_xspec(plan->p);
     return poisson_fused<float>(plan->p, mesh, c_poisson);
 }
 

@@ -157,32 +157,40 @@ template <int N, int TK, int RV = 0> constexpr int strided_smem_elems() { return
 template <typename T, int N, int DIR, int TK, int RV = 0, int AX = -1>
 __global__ void __launch_bounds__(strided_threads<N, TK, RV>(), 2)
 k_fft_strided(typename Cx<T>::t* __restrict__ data, long long es_, long long os_, long long bs, int ncols,
-              const typename Cx<T>::t* __restrict__ tw) {
+              const typename Cx<T>::t* __restrict__ tw, typename Cx<T>::t* out) {
     using C = typename Cx<T>::t;
     constexpr int R1 = RadixV<N, RV>::R1, R2 = RadixV<N, RV>::R2;
     // AX = 1 (y) or 0 (x): the element and plane strides of the padded
     // spectrum are compile-time constants, so the 2 R2 accesses of a thread
-    // are one base address plus constant offsets; AX = -1 takes them as given
+    // are one base address plus constant offsets; AX = -1 takes them as given.
+    // AX = 2: lines read along the outer axis of `data` (element stride N H,
+    // plane stride H: y lines of the transposed spectrum [ky][kx][kz]) and
+    // written along the middle axis of `out` (element stride H, plane stride
+    // N H: the spectrum [kx][y][kz]); every other AX works in place.
     constexpr long long H = N / 2 + 1;
-    const long long es = AX == 1 ? H : (AX == 0 ? (long long)N * H : es_);
-    const long long os = AX == 1 ? (long long)N * H : (AX == 0 ? H : os_);
+    constexpr bool OUTER = AX == 0 || AX == 2;
+    const long long es = AX == 1 ? H : (OUTER ? (long long)N * H : es_);
+    const long long os = AX == 1 ? (long long)N * H : (OUTER ? H : os_);
+    const long long oes = AX == 2 ? H : es, oos = AX == 2 ? (long long)N * H : os;
     extern __shared__ __align__(16) unsigned char smraw[];
     C* S = reinterpret_cast<C*>(smraw);
     const int tx = threadIdx.x % TK, ty = threadIdx.x / TK;
     const int col = blockIdx.x * TK + tx;
     const bool active = col < ncols;
     // plane blockIdx.y % N of box blockIdx.y / N (boxes of a batch at stride bs)
-    C* base = data + (long long)(blockIdx.y / N) * bs + (long long)(blockIdx.y % N) * os + (active ? col : 0);
+    const long long box = blockIdx.y / N, plane = blockIdx.y % N;
+    C* base = data + box * bs + plane * os + (active ? col : 0);
+    C* obase = AX == 2 ? out + box * bs + plane * oos + (active ? col : 0) : base;
 
     using I = SIdx<R1, R2, TK>;
-    const long long es1 = es * R2, es2 = es * R1;
+    const long long es1 = es * R2, oes2 = oes * R1;
     stockham_pass1<R1, R2, DIR, false, C>(
         ty, [&](int j, int r) { return active ? base[j * es + r * es1] : cmake<C>(0, 0); },
         [&](int j, int k, C v) { S[I::out1(j, k, tx)] = v; });
     __syncthreads();
     stockham_pass2<R1, R2, DIR, false, C>(
         ty, [&](int j, int r) { return S[I::p2(j, r, tx)]; },
-        [&](int j, int k, C v) { if (active) base[j * es + k * es2] = v; },
+        [&](int j, int k, C v) { if (active) obase[j * oes + k * oes2] = v; },
         [&](int e) { return twiddle<DIR>(tw, e); });
 }
 
@@ -205,21 +213,28 @@ __device__ __forceinline__ T green_value(int kx, int ky, int kz, int kind, doubl
         return (T)(-cg / ((double)__ldg(g1d + kx) + (double)__ldg(g1d + ky) + (double)__ldg(g1d + kz)));
     } else {
         const float s = __ldg(g1d + kx) + __ldg(g1d + ky) + __ldg(g1d + kz);
-        return (float)(-cg) * __frcp_rn(s);
+        // fast division (2 ulp): the correctly rounded reciprocal cost a
+        // sixth of the x + Green pass
+        return __fdividef((float)(-cg), s);
     }
 }
 
 // Fused x pass of the Poisson solve: forward FFT along x, multiply by G,
-// inverse FFT along x, for TK kz columns of one ky plane.
-template <typename T, int N, int TK, int RV = 0>
+// inverse FFT along x, for TK kz columns of one ky plane.  XT: the lines are
+// written to `out` in the transposed layout [ky][kx][kz] (element stride H),
+// so that neither this pass nor the next one both reads and writes lines
+// whose elements lie N H apart; otherwise in place.
+template <typename T, int N, int TK, int RV = 0, bool XT = false>
 __global__ void __launch_bounds__(strided_threads<N, TK, RV>(), 2)
 k_fft_x_green(typename Cx<T>::t* __restrict__ data, long long es_, long long os_, long long bs, int ncols,
-              const typename Cx<T>::t* __restrict__ tw, const T* __restrict__ g1d, double cg, int kind) {
+              const typename Cx<T>::t* __restrict__ tw, const T* __restrict__ g1d, double cg, int kind,
+              typename Cx<T>::t* out) {
     using C = typename Cx<T>::t;
     constexpr int R1 = RadixV<N, RV>::R1, R2 = RadixV<N, RV>::R2;
     // x lines of the padded spectrum: compile-time strides (es_ = N H and
     // os_ = H are what every caller passes)
     constexpr long long es = (long long)N * (N / 2 + 1), os = N / 2 + 1;
+    constexpr long long oes = XT ? os : es, oos = XT ? es : os;
     (void)es_;
     (void)os_;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -229,9 +244,10 @@ k_fft_x_green(typename Cx<T>::t* __restrict__ data, long long es_, long long os_
     const bool active = col < ncols;
     const int ky = blockIdx.y % N;
     C* base = data + (long long)(blockIdx.y / N) * bs + (long long)ky * os + (active ? col : 0);
+    C* obase = XT ? out + (long long)(blockIdx.y / N) * bs + (long long)ky * oos + (active ? col : 0) : base;
 
     using I = SIdx<R1, R2, TK>;
-    const long long es1 = es * R2, es2 = es * R1;
+    const long long es1 = es * R2, oes2 = oes * R1;
     auto p2ld = [&](int j, int r) { return S[I::p2(j, r, tx)]; };
     stockham_pass1<R1, R2, -1, false, C>(
         ty, [&](int j, int r) { return active ? base[j * es + r * es1] : cmake<C>(0, 0); },
@@ -248,7 +264,7 @@ k_fft_x_green(typename Cx<T>::t* __restrict__ data, long long es_, long long os_
         ty, [&](int j, int r) { return S[I::in1(j, r, tx)]; }, [&](int j, int k, C v) { S[I::out1(j, k, tx)] = v; });
     __syncthreads();
     stockham_pass2<R1, R2, +1, false, C>(
-        ty, p2ld, [&](int j, int k, C v) { if (active) base[j * es + k * es2] = v; },
+        ty, p2ld, [&](int j, int k, C v) { if (active) obase[j * oes + k * oes2] = v; },
         [&](int e) { return twiddle<+1>(tw, e); });
 }
 
@@ -359,6 +375,8 @@ k_fftg_strided(typename Cx<T>::t* __restrict__ data, long long es, long long os,
 template <typename T, int N, int TK = kGTK> struct LaunchG {
     using C = typename Cx<T>::t;
     static constexpr int H = N / 2 + 1;
+    static constexpr bool kTransposedX = false;
+    static void xgreen_yinv_transposed(const Plan&, T*, T*, double) {}
     static size_t smem_z() { return (size_t)g_z_rows<N>() * 2 * (N / 2 + 1) * sizeof(C); }
     static size_t smem_s() { return (size_t)2 * N * TK * sizeof(C); }
     static int prepare() { return PM_OK; }
@@ -412,8 +430,11 @@ template <typename T, int N, int TK = tk_cols<T, N>(), int RV = 0> struct Launch
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, -1, TK, RV, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, +1, TK, RV, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_x_green<T, N, TK, RV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
+        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_x_green<T, N, TK, RV, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
+        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, +1, TK, RV, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         return PM_OK;
     }
+    static constexpr bool kTransposedX = true;
     static void z(const Plan& p, T* mesh, bool forward, int nbox = 1) {
         const long long rows = (long long)nbox * N * N;
         const int lpb = forward ? z_rows_per_block<T, N, false>() : z_rows_per_block<T, N, true>();
@@ -437,7 +458,7 @@ template <typename T, int N, int TK = tk_cols<T, N>(), int RV = 0> struct Launch
         Timed t(p, axis == 1 ? (dir < 0 ? ST_FFT_Y_FWD : ST_FFT_Y_INV) : (dir < 0 ? ST_FFT_X_FWD : ST_FFT_X_INV));
         auto go = [&](auto dirc, auto axc) {
             k_fft_strided<T, N, decltype(dirc)::value, TK, RV, decltype(axc)::value>
-                <<<grid, strided_threads<N, TK, RV>(), smem_s(), p.stream>>>(d, es, os, bs, H, tw);
+                <<<grid, strided_threads<N, TK, RV>(), smem_s(), p.stream>>>(d, es, os, bs, H, tw, d);
         };
         using F = std::integral_constant<int, -1>;
         using B = std::integral_constant<int, +1>;
@@ -454,7 +475,25 @@ template <typename T, int N, int TK = tk_cols<T, N>(), int RV = 0> struct Launch
         Timed t(p, ST_FFT_X_GREEN);
         k_fft_x_green<T, N, TK, RV><<<grid, strided_threads<N, TK, RV>(), smem_s(), p.stream>>>(
             d, (long long)N * H, H, (long long)N * N * H, H, static_cast<const C*>(p.tw),
-            static_cast<const T*>(p.g1d), cg, p.green_kind);
+            static_cast<const T*>(p.g1d), cg, p.green_kind, d);
+    }
+    // One box through the transposed spectrum `xt` ([ky][kx][kz], N^2 H
+    // complex): x forward + Green + x inverse from `mesh` into `xt`, then the
+    // inverse y pass from `xt` back into `mesh` ([x][y][kz]).
+    static void xgreen_yinv_transposed(const Plan& p, T* mesh, T* xt, double cg) {
+        C* d = reinterpret_cast<C*>(mesh);
+        C* o = reinterpret_cast<C*>(xt);
+        const C* tw = static_cast<const C*>(p.tw);
+        const dim3 grid((H + TK - 1) / TK, N);
+        {
+            Timed t(p, ST_FFT_X_GREEN);
+            k_fft_x_green<T, N, TK, RV, true><<<grid, strided_threads<N, TK, RV>(), smem_s(), p.stream>>>(
+                d, (long long)N * H, H, (long long)N * N * H, H, tw, static_cast<const T*>(p.g1d), cg, p.green_kind,
+                o);
+        }
+        Timed t(p, ST_FFT_Y_INV);
+        k_fft_strided<T, N, +1, TK, RV, 2><<<grid, strided_threads<N, TK, RV>(), smem_s(), p.stream>>>(
+            o, (long long)N * H, H, (long long)N * N * H, H, tw, d);
     }
 };
 
@@ -589,13 +628,23 @@ template <typename T> int green_apply(const Plan& p, T* mesh, double c_poisson) 
     return PM_OK;
 }
 
+// The y forward, x + Green and y inverse passes of a solve (launcher L_):
+// through the plan's transposed spectrum when it has one (a single box of a
+// power-of-two mesh >= 512), else in place.
+#define PMB_XY_PASSES(P, T_, MESH, CG, NBOX)                                   \
+    L_::strided(P, MESH, 1, -1, NBOX);                                         \
+    if (L_::kTransposedX && (NBOX) == 1 && (P).xspec) {                        \
+        L_::xgreen_yinv_transposed(P, MESH, static_cast<T_*>((P).xspec), CG);  \
+    } else {                                                                   \
+        L_::xgreen(P, MESH, CG, NBOX);                                         \
+        L_::strided(P, MESH, 1, +1, NBOX);                                     \
+    }
+
 template <typename T> int poisson_fused(const Plan& p, T* mesh, double c_poisson, int nbox) {
     const double cg = green_scale(p, c_poisson);
     PMB_LAUNCH(p, T, {
         L_::z(p, mesh, true, nbox);
-        L_::strided(p, mesh, 1, -1, nbox);
-        L_::xgreen(p, mesh, cg, nbox);
-        L_::strided(p, mesh, 1, +1, nbox);
+        PMB_XY_PASSES(p, T, mesh, cg, nbox);
         L_::z(p, mesh, false, nbox);
     });
     PMB_CUDA_CHECK(cudaGetLastError());
@@ -605,9 +654,7 @@ template <typename T> int poisson_fused(const Plan& p, T* mesh, double c_poisson
 int poisson_after_z_f32(const Plan& p, float* mesh, double c_poisson, int nbox) {
     const double cg = green_scale(p, c_poisson);
     PMB_LAUNCH(p, float, {
-        L_::strided(p, mesh, 1, -1, nbox);
-        L_::xgreen(p, mesh, cg, nbox);
-        L_::strided(p, mesh, 1, +1, nbox);
+        PMB_XY_PASSES(p, float, mesh, cg, nbox);
         L_::z(p, mesh, false, nbox);
     });
     PMB_CUDA_CHECK(cudaGetLastError());

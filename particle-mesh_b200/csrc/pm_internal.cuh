@@ -123,6 +123,7 @@ struct Plan {
     void* adj[3] = {nullptr, nullptr, nullptr};    // adjoint source arrays (deposited u), plan precision
     void* adjm = nullptr;                          // FP32 adjoint: the second padded mesh (psi)
     void* red = nullptr;                           // reduction partial sums (FP64)
+    void* xspec = nullptr;                         // transposed half spectrum [ky][kx][kz] (ng >= 512)
     size_t bytes = 0;
     StageTimers* timers = nullptr;  // owned by the C-ABI plan object
     TileScratch tiles;
