@@ -261,7 +261,10 @@ int pm_kick_drift_f32(pm_plan* plan, const float* phi, uint32_t* cell, float* ox
  * tile, the deposit fused with the z R2C pass (power-of-two ng >= 32; the
  * tile deposit otherwise), the y / x + Green / y passes, z C2R, then
  * gradient + interpolation + kick + drift in one pass.  A cell word whose
- * indices lie outside [0, ng) is taken as the same periodic cell. */
+ * indices lie outside [0, ng) is taken as the same periodic cell.  For
+ * ng >= 512 this call and pm_poisson_f32 also give the plan a second half
+ * spectrum (ng^2 (ng/2+1) complex, 4.3 GB at 1024) that the x + Green pass
+ * writes transposed; pm_plan_device_bytes counts it. */
 int pm_step_f32(pm_plan* plan, uint32_t* cell, float* ox, float* oy, float* oz, float* vx,
                 float* vy, float* vz, int64_t np, float mass, double c_poisson, double c_kick,
                 double dt);
