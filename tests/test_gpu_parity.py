@@ -606,3 +606,27 @@ def test_errors_are_reported(pmpkg):
         p32.deposit(x, y, z, 1.0)  # FP64 entry point on an FP32 plan
     with pytest.raises(pmpkg.PMError):
         plan.deposit(x.float(), y, z, 1.0)
+
+
+@pytest.mark.parametrize("ng", [256, 512])
+def test_poisson_f32_transposed_spectrum(pmpkg, ng):
+    """FP32 plans of ng >= 512 route the x + Green pass through a second half
+    spectrum laid out [ky][kx][kz]: the first pm_poisson_f32 adds exactly
+    ng^2 (ng/2+1) complex64 to the plan's device bytes (nothing for smaller
+    meshes, which solve in place), later solves add nothing, and solving the
+    same mesh twice gives the same bits."""
+    g = torch.Generator(device=DEV).manual_seed(ng + 11)
+    plan = pmpkg.Plan(ng, "fp32")
+    d = plan.new_mesh()
+    d[:, :, :ng] = torch.randn((ng, ng, ng), generator=g, device=DEV, dtype=torch.float32)
+    x = d.clone()
+    b0 = plan.device_bytes()
+    plan.poisson(d, 2.5)
+    grown = plan.device_bytes() - b0
+    assert grown == (ng * ng * (ng // 2 + 1) * 8 if ng >= 512 else 0)
+    e = x.clone()
+    plan.poisson(e, 2.5)
+    assert plan.device_bytes() - b0 == grown
+    assert torch.equal(d, e)
+    del d, e, x
+    torch.cuda.empty_cache()
