@@ -13,6 +13,8 @@
 // that one thread owns one radix-R butterfly held in registers.
 #pragma once
 
+#include <type_traits>
+
 #include "pm_internal.cuh"
 
 namespace pmb {
@@ -85,6 +87,36 @@ __device__ __forceinline__ C twiddle(const C* __restrict__ tw, int e) {
     return DIR < 0 ? w : cconj(w);
 }
 
+// Pass-2 twiddles W_N^(r j) of one thread (fixed j, r < 32) from 10 table
+// loads instead of 31: W^(m j), m < 8, held in registers and W^(8 q j) loaded
+// per q, multiplied for r = 8 q + m (one extra complex product, ~1 ulp).
+template <int DIR, typename C> struct TwSplit8 {
+    const C* __restrict__ tw;
+    int j;
+    C wm[8];
+    __device__ __forceinline__ TwSplit8(const C* __restrict__ tw_, int j_) : tw(tw_), j(j_) {
+        wm[0] = cmake<C>(1, 0);
+#pragma unroll
+        for (int m = 1; m < 8; ++m) wm[m] = twiddle<DIR>(tw, m * j);
+    }
+    __device__ __forceinline__ C operator()(int r, int) const {
+        const int q = r >> 3, m = r & 7;
+        if (q == 0) return wm[m];
+        const C b = twiddle<DIR>(tw, 8 * q * j);
+        return m == 0 ? b : cmul(b, wm[m]);
+    }
+};
+
+// The pass-2 twiddle functor of thread j: split (TwSplit8, needs R2 >= 16 so
+// that every index stays below L = R1 R2) or one table load per twiddle.
+template <int DIR, bool SPLIT, typename C>
+__device__ __forceinline__ auto pass2_twiddles(const C* __restrict__ tw, int j) {
+    if constexpr (SPLIT)
+        return TwSplit8<DIR, C>(tw, j);
+    else
+        return [tw](int e) { return twiddle<DIR>(tw, e); };
+}
+
 // Two-pass radix choice for a line of length L = R1 * R2, R1 <= R2.
 template <int L> struct Radix;
 template <> struct Radix<4> { static constexpr int R1 = 2, R2 = 2; };
@@ -146,7 +178,12 @@ __device__ __forceinline__ void stockham_pass2(int j, const LD& ld, const ST& st
 #pragma unroll
     for (int r = 0; r < R2; ++r) v[r] = ld(j, r);
 #pragma unroll
-    for (int r = 1; r < R2; ++r) v[r] = cmul(v[r], twf(r * j));
+    for (int r = 1; r < R2; ++r) {
+        if constexpr (std::is_invocable_v<const TW&, int, int>)
+            v[r] = cmul(v[r], twf(r, j));
+        else
+            v[r] = cmul(v[r], twf(r * j));
+    }
     dft<R2, DIR>(v);
     if (SYNC) __syncthreads();
 #pragma unroll
