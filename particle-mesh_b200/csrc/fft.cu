@@ -85,7 +85,7 @@ k_fft_z_r2c(T* __restrict__ mesh, long long nrows, const typename Cx<T>::t* __re
     __syncthreads();
     stockham_pass2<R1, R2, -1, true, C>(
         tj, [&](int j, int r) { return S[I::p2(j, r)]; }, [&](int j, int k, C v) { S[I::p2(j, k)] = v; },
-        [&](int e) { return twiddle<-1>(tw, 2 * e); });
+        pass2_twiddles<-1, (R2 >= 16 && sizeof(T) == 4), 2>(tw, tj));
     __syncthreads();
     if (active) {
         for (int k = tj; k <= M; k += NT) {
@@ -144,7 +144,8 @@ k_fft_z_c2r(T* __restrict__ mesh, long long nrows, const typename Cx<T>::t* __re
     __syncthreads();
     stockham_pass2<R1, R2, +1, false, C>(
         tj, [&](int j, int r) { return S[I::p2(j, r)]; },
-        [&](int j, int k, C v) { if (active) crow[j + k * R1] = v; }, [&](int e) { return twiddle<+1>(tw, 2 * e); });
+        [&](int j, int k, C v) { if (active) crow[j + k * R1] = v; },
+        pass2_twiddles<+1, (R2 >= 16 && sizeof(T) == 4), 2>(tw, tj));
     if (active && tj == 0) crow[M] = cmake<C>(0, 0);  // padding
 }
 

@@ -87,34 +87,35 @@ __device__ __forceinline__ C twiddle(const C* __restrict__ tw, int e) {
     return DIR < 0 ? w : cconj(w);
 }
 
-// Pass-2 twiddles W_N^(r j) of one thread (fixed j, r < 32) from 10 table
-// loads instead of 31: W^(m j), m < 8, held in registers and W^(8 q j) loaded
-// per q, multiplied for r = 8 q + m (one extra complex product, ~1 ulp).
-template <int DIR, typename C> struct TwSplit8 {
+// Pass-2 twiddles W_N^(S r j) of one thread (fixed j, r < 32; S = 2 for the
+// half-length line of the z passes) from 10 table loads instead of 31:
+// W^(S m j), m < 8, held in registers and W^(8 S q j) loaded per q,
+// multiplied for r = 8 q + m (one extra complex product, ~1 ulp).
+template <int DIR, typename C, int S = 1> struct TwSplit8 {
     const C* __restrict__ tw;
     int j;
     C wm[8];
     __device__ __forceinline__ TwSplit8(const C* __restrict__ tw_, int j_) : tw(tw_), j(j_) {
         wm[0] = cmake<C>(1, 0);
 #pragma unroll
-        for (int m = 1; m < 8; ++m) wm[m] = twiddle<DIR>(tw, m * j);
+        for (int m = 1; m < 8; ++m) wm[m] = twiddle<DIR>(tw, S * m * j);
     }
     __device__ __forceinline__ C operator()(int r, int) const {
         const int q = r >> 3, m = r & 7;
         if (q == 0) return wm[m];
-        const C b = twiddle<DIR>(tw, 8 * q * j);
+        const C b = twiddle<DIR>(tw, 8 * S * q * j);
         return m == 0 ? b : cmul(b, wm[m]);
     }
 };
 
 // The pass-2 twiddle functor of thread j: split (TwSplit8, needs R2 >= 16 so
 // that every index stays below L = R1 R2) or one table load per twiddle.
-template <int DIR, bool SPLIT, typename C>
+template <int DIR, bool SPLIT, int S = 1, typename C>
 __device__ __forceinline__ auto pass2_twiddles(const C* __restrict__ tw, int j) {
     if constexpr (SPLIT)
-        return TwSplit8<DIR, C>(tw, j);
+        return TwSplit8<DIR, C, S>(tw, j);
     else
-        return [tw](int e) { return twiddle<DIR>(tw, e); };
+        return [tw](int e) { return twiddle<DIR>(tw, S * e); };
 }
 
 // Two-pass radix choice for a line of length L = R1 * R2, R1 <= R2.
