@@ -73,8 +73,8 @@ typedef struct pm_plan pm_plan;
 
 /* ------------------------------------------------------------ plans */
 
-/* Creates a plan for an ng^3 mesh.  ng must be a power of two in [8, 1024].
- * grad_order is 2 (the reference's 2-point centred difference,
+/* Creates a plan for an ng^3 mesh.  ng must be a power of two in [8, 1024];
+ * FP32 plans also take the mixed-radix sizes 48 and 96.  grad_order is 2 (the reference's 2-point centred difference,
  * src/utils/utils.cpp:115-137) or 4.  stream may be NULL (legacy default
  * stream).  Replaces the setup of src/core/main.cpp:30-81 and the FFT
  * constructor src/fft/fftw/fft.cpp:3-59 (plans, Green's table). */

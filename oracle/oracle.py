@@ -29,7 +29,6 @@ import subprocess
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_SRC = "/root/reference"
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _lib = None
@@ -74,16 +73,18 @@ def _cpu_has_v3() -> bool:
 def ref_lib():
     """The reference's own kernels (oracle/_ref), or None if not built.
 
-    Built from the reference sources when they are present on this machine;
-    elsewhere only a prebuilt copy can be used."""
+    Built from the reference sources by oracle/Makefile (target
+    ref-if-present: the tree named by PM_REFERENCE_DIR, or the Makefile's
+    default) when they are present on this machine; elsewhere only a
+    prebuilt copy can be used."""
     global _ref
     if _ref is not None:
         return _ref
     d = os.path.join(HERE, "_ref")
     names = (["libpmref_v3.so"] if _cpu_has_v3() and platform.machine() == "x86_64" else []) + ["libpmref.so"]
     paths = [os.path.join(d, n) for n in names]
-    if not any(os.path.exists(p) for p in paths) and os.path.isdir(REF_SRC):
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+    if not any(os.path.exists(p) for p in paths):
+        subprocess.run(["make", "-s", "-C", HERE, "ref-if-present"], check=True)
     path = next((p for p in paths if os.path.exists(p)), None)
     if path is None:
         return None

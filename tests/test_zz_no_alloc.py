@@ -25,15 +25,23 @@ def _vp(t):
     return ctypes.c_void_p(t.data_ptr())
 
 
-def test_no_alloc_deposit_matches_allocating_entry_point(pmpkg):
+# (ng, particle counts of the calls in a row): the 16^3-tile kernel at 128;
+# the 8^3-tile kernel of the smallest mesh; the largest mesh with a particle
+# set that fills the static permutation exactly; and empty sets before and
+# after a full one (an empty call must not see the previous call's buckets).
+CASES = [(128, (300000, 200000)), (8, (300, 1000)), (256, (1 << 21, (1 << 21) - 12345)),
+         (64, (0, 5000, 0))]
+
+
+@pytest.mark.parametrize("ng,counts", CASES, ids=[f"ng{c[0]}" for c in CASES])
+def test_no_alloc_deposit_matches_allocating_entry_point(pmpkg, ng, counts):
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
     lib = pmpkg.load()
-    ng = 128
     plan = pmpkg.Plan(ng, "fp32", device=DEV)
     stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
-    for seed, np_ in ((1, 300000), (2, 200000)):
-        rng = np.random.default_rng(seed)
+    for seed, np_ in enumerate(counts, start=1):
+        rng = np.random.default_rng(seed + ng)
         pos = [torch.tensor(rng.uniform(0, ng, np_), dtype=torch.float64, device=DEV) for _ in range(3)]
         cell, off = plan.split(*pos)
         mass = 0.37 * seed
@@ -43,7 +51,10 @@ def test_no_alloc_deposit_matches_allocating_entry_point(pmpkg):
         assert rc == 0, lib.pm_last_error()
         torch.cuda.synchronize()
         assert torch.isfinite(out).all()
-        assert float((out - ref).abs().max()) < TOL
+        assert float((out - ref).abs().max()) < TOL * max(1.0, mass * np_ / ng ** 3 * 8)
+        if np_ == 0:
+            assert torch.equal(out[:, :, :ng], torch.full_like(out[:, :, :ng], -1.0))
+        assert torch.equal(out[:, :, ng:], torch.zeros_like(out[:, :, ng:]))
 
 
 def test_no_alloc_deposit_rejects_sizes_beyond_its_limits(pmpkg):
