@@ -321,6 +321,72 @@ int pm_ensemble_run_f32(pm_ensemble* ensemble, uint32_t* cell, float* ox, float*
 int pm_ensemble_info(const pm_ensemble* ensemble, int* nclasses, int* class_ng, int* class_nbox,
                      int* class_tk, int* class_radix, size_t* device_bytes, size_t* graph_nodes);
 
+/* ------------------------------------------ x-slab decomposition (FP32)
+ * One periodic ng^3 mesh split over nranks ranks (one GPU each) as x-slabs
+ * of nx = ng / nranks planes, rank r owning planes [r nx, (r + 1) nx) and the
+ * particles whose cell lies there (split positions as for pm_step_f32).  The
+ * reference's slab layout: FFTW-MPI's local_n0 slabs (src/fft/fftw/fft.cpp:16)
+ * fed by TransposeSlab + ReorderSlab (src/decomp/slab/transpose_slab.cpp:3-39,
+ * reorder_slab.cpp:43-68) and read back through ReorderSlabBack +
+ * TransposeSlabBack (reorder_slab_back.cpp:37-49, transpose_slab_back.cpp:3-49).
+ * ng a power of two in [32, 1024]; nranks a power of two with nx a multiple
+ * of 4.  The caller moves the data between ranks (NCCL, or copies between
+ * slabs of one process); one step is, on every rank in the same order:
+ *
+ *   pm_slab_deposit_f32      deposit + z R2C into the own planes, and the +1
+ *                            corners of the last plane into the ghost plane
+ *   exchange A               ghost plane (buffer plane nx + 2) to rank r + 1
+ *   pm_slab_fold_f32         add the ghost plane received from rank r - 1
+ *   pm_slab_forward_f32      y forward; rows packed into `send`
+ *   exchange B               all-to-all: block d of `send` (nx ng (ng + 2)
+ *                            / nranks floats) to rank d, into block r of
+ *                            `recv` on rank d
+ *   pm_slab_xgreen_f32       x forward, Green, x inverse; packed into `send`
+ *   exchange B again
+ *   pm_slab_backward_f32     y inverse, z C2R: the potential in planes
+ *                            2 .. nx + 1 of the buffer
+ *   exchange C               buffer planes nx, nx + 1 to rank r + 1's planes
+ *                            0, 1; planes 2, 3, 4 to rank r - 1's planes
+ *                            nx + 2 .. nx + 4 (the potential halo)
+ *   pm_slab_kick_drift_f32   fused gradient + gather + kick + drift
+ *   pm_slab_migrate_sort     particles counted by new owner (host counts)
+ *   pm_slab_migrate_pack     particles packed in owner order, W words each
+ *   exchange D               counts, then the packed particles, all-to-all
+ *   pm_slab_migrate_unpack   received (and kept) particles into the arrays
+ *
+ * The particle migration is new: the reference never moves particles. */
+typedef struct pm_slab pm_slab;
+int pm_slab_create(int ng, int nranks, int rank, int green_kind, int grad_order, void* stream, pm_slab** slab);
+int pm_slab_destroy(pm_slab* slab);
+/* Geometry and device buffers: nx own planes starting at x0; plane_floats =
+ * ng (ng + 2) floats per buffer plane; buf = [nx + 6] planes (0-1 lower
+ * halo, 2 .. nx + 1 own, nx + 2 ghost plane / upper halo); send and recv =
+ * xfer_floats floats each.  Any output may be NULL. */
+int pm_slab_info(const pm_slab* slab, int* nx, int* x0, size_t* plane_floats, void** buf, void** send, void** recv,
+                 size_t* xfer_floats, size_t* device_bytes);
+/* The slab's FP32 plan (stream, stage timers, pm_plan_check). */
+int pm_slab_plan(pm_slab* slab, pm_plan** plan);
+int pm_slab_deposit_f32(pm_slab* slab, const uint32_t* cell, const float* ox, const float* oy, const float* oz,
+                        int64_t np, float mass);
+int pm_slab_fold_f32(pm_slab* slab, const float* ghost);
+int pm_slab_forward_f32(pm_slab* slab);
+int pm_slab_xgreen_f32(pm_slab* slab, double c_poisson);
+int pm_slab_backward_f32(pm_slab* slab);
+/* A particle whose cell is outside the slab is clamped into it and reported
+ * by pm_slab_check (PM_ERR_RANGE). */
+int pm_slab_kick_drift_f32(pm_slab* slab, uint32_t* cell, float* ox, float* oy, float* oz, float* vx, float* vy,
+                           float* vz, int64_t np, double c_kick, double dt);
+/* counts: host array of nranks; waits for the slab's stream. */
+int pm_slab_migrate_sort(pm_slab* slab, const uint32_t* cell, int64_t np, int64_t* counts);
+/* arrays: host array of narrays (<= 8) device arrays of 32-bit words;
+ * packed[i * narrays + w] = arrays[w][p_i], p_i in the order of the last
+ * pm_slab_migrate_sort (owner rank ascending). */
+int pm_slab_migrate_pack(pm_slab* slab, void* const* arrays, int narrays, int64_t np, uint32_t* packed);
+/* arrays[w][at + i] = packed[i * narrays + w], i < n. */
+int pm_slab_migrate_unpack(pm_slab* slab, const uint32_t* packed, int64_t n, void* const* arrays, int narrays,
+                           int64_t at);
+int pm_slab_check(pm_slab* slab);
+
 /* ---------------------------------------------- initial conditions (new)
  * Zel'dovich particles on an nrow^3 lattice q = (i + 1/2) ng/nrow from a
  * Gaussian random field with P(k) ~ k^n_s, scaled to an rms 3D displacement

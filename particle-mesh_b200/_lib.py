@@ -66,6 +66,20 @@ SIGNATURES = {
     "pm_ensemble_run_f32": [_V, _V, _V, _V, _V, _V, _V, _V, _D, _D, _I],
     "pm_ensemble_info": [_V, _V, _V, _V, _V, _V, _V, _V],
     "pm_ic_zeldovich": [_I, _I, _D, _D, _U64, _D, _V, _V, _V, _V, _V, _V, _V],
+    "pm_slab_create": [_I, _I, _I, _I, _I, _V, ctypes.POINTER(_V)],
+    "pm_slab_destroy": [_V],
+    "pm_slab_info": [_V, _V, _V, _V, _V, _V, _V, _V, _V],
+    "pm_slab_plan": [_V, ctypes.POINTER(_V)],
+    "pm_slab_deposit_f32": [_V, _V, _V, _V, _V, _L, _F],
+    "pm_slab_fold_f32": [_V, _V],
+    "pm_slab_forward_f32": [_V],
+    "pm_slab_xgreen_f32": [_V, _D],
+    "pm_slab_backward_f32": [_V],
+    "pm_slab_kick_drift_f32": [_V, _V, _V, _V, _V, _V, _V, _V, _L, _D, _D],
+    "pm_slab_migrate_sort": [_V, _V, _L, _V],
+    "pm_slab_migrate_pack": [_V, _V, _I, _L, _V],
+    "pm_slab_migrate_unpack": [_V, _V, _L, _V, _I, _L],
+    "pm_slab_check": [_V],
 }
 
 _lib = None

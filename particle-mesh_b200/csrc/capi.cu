@@ -244,6 +244,12 @@ static int plan_create(int ng, int precision, int green_kind, int grad_order, vo
     return PM_OK;
 }
 
+namespace pmb {
+int plan_create_internal(int ng, int precision, int green_kind, int grad_order, void* stream, pm_plan** out) {
+    return plan_create(ng, precision, green_kind, grad_order, stream, out, false);
+}
+}  // namespace pmb
+
 extern "C" {
 
 int pm_plan_create(int ng, int precision, int green_kind, int grad_order, void* stream, pm_plan** out) {

@@ -225,16 +225,19 @@ __device__ __forceinline__ T green_value(int kx, int ky, int kz, int kind, doubl
 // written to `out` in the transposed layout [ky][kx][kz] (element stride H),
 // so that neither this pass nor the next one both reads and writes lines
 // whose elements lie N H apart; otherwise in place.
-template <typename T, int N, int TK, int RV = 0, bool XT = false>
+// SLABX: the x lines of one slab's share of the spectrum after the global
+// transpose, laid out [ky - ky0][kx][kz] (element stride H, plane stride N H,
+// in place), plane blockIdx.y holding ky = ky0 + blockIdx.y.
+template <typename T, int N, int TK, int RV = 0, bool XT = false, bool SLABX = false>
 __global__ void __launch_bounds__(strided_threads<N, TK, RV>(), 2)
 k_fft_x_green(typename Cx<T>::t* __restrict__ data, long long es_, long long os_, long long bs, int ncols,
               const typename Cx<T>::t* __restrict__ tw, const T* __restrict__ g1d, double cg, int kind,
-              typename Cx<T>::t* out) {
+              typename Cx<T>::t* out, int ky0 = 0) {
     using C = typename Cx<T>::t;
     constexpr int R1 = RadixV<N, RV>::R1, R2 = RadixV<N, RV>::R2;
     // x lines of the padded spectrum: compile-time strides (es_ = N H and
     // os_ = H are what every caller passes)
-    constexpr long long es = (long long)N * (N / 2 + 1), os = N / 2 + 1;
+    constexpr long long es = SLABX ? N / 2 + 1 : (long long)N * (N / 2 + 1), os = SLABX ? (long long)N * (N / 2 + 1) : N / 2 + 1;
     constexpr long long oes = XT ? os : es, oos = XT ? es : os;
     // FP32: pass-2 twiddles from 10 table loads per thread (2.97 vs 3.10 ms)
     constexpr bool kSplitTw = R2 >= 16 && sizeof(T) == 4;
@@ -245,8 +248,9 @@ k_fft_x_green(typename Cx<T>::t* __restrict__ data, long long es_, long long os_
     const int tx = threadIdx.x % TK, ty = threadIdx.x / TK;
     const int col = blockIdx.x * TK + tx;
     const bool active = col < ncols;
-    const int ky = blockIdx.y % N;
-    C* base = data + (long long)(blockIdx.y / N) * bs + (long long)ky * os + (active ? col : 0);
+    const int ky = SLABX ? ky0 + (int)blockIdx.y : (int)(blockIdx.y % N);
+    C* base = SLABX ? data + (long long)blockIdx.y * os + (active ? col : 0)
+                    : data + (long long)(blockIdx.y / N) * bs + (long long)ky * os + (active ? col : 0);
     C* obase = XT ? out + (long long)(blockIdx.y / N) * bs + (long long)ky * oos + (active ? col : 0) : base;
 
     using I = SIdx<R1, R2, TK>;
@@ -435,7 +439,43 @@ template <typename T, int N, int TK = tk_cols<T, N>(), int RV = 0> struct Launch
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_x_green<T, N, TK, RV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_x_green<T, N, TK, RV, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, +1, TK, RV, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
+        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_x_green<T, N, TK, RV, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         return PM_OK;
+    }
+    // ---- x-slab decomposition: passes over part of a mesh
+    // z pass over `rows` rows of N reals (+2 padding)
+    static void z_rows(const Plan& p, T* mesh, bool forward, long long rows) {
+        const int lpb = forward ? z_rows_per_block<T, N, false>() : z_rows_per_block<T, N, true>();
+        const unsigned grid = (unsigned)((rows + lpb - 1) / lpb);
+        const int thr = z_threads_per_row<N>() * lpb;
+        const C* tw = static_cast<const C*>(p.tw);
+        Timed t(p, forward ? ST_FFT_Z_R2C : ST_FFT_Z_C2R);
+        if (forward)
+            k_fft_z_r2c<T, N><<<grid, thr, smem_z(false), p.stream>>>(mesh, rows, tw);
+        else
+            k_fft_z_c2r<T, N><<<grid, thr, smem_z(true), p.stream>>>(mesh, rows, tw);
+    }
+    // y lines of `planes` consecutive x planes [x][y][kz]
+    static void y_planes(const Plan& p, T* mesh, int dir, int planes) {
+        C* d = reinterpret_cast<C*>(mesh);
+        const dim3 grid((H + TK - 1) / TK, planes);
+        const C* tw = static_cast<const C*>(p.tw);
+        Timed t(p, dir < 0 ? ST_FFT_Y_FWD : ST_FFT_Y_INV);
+        if (dir < 0)
+            k_fft_strided<T, N, -1, TK, RV, 1><<<grid, strided_threads<N, TK, RV>(), smem_s(), p.stream>>>(
+                d, H, (long long)N * H, 0, H, tw, d);
+        else
+            k_fft_strided<T, N, +1, TK, RV, 1><<<grid, strided_threads<N, TK, RV>(), smem_s(), p.stream>>>(
+                d, H, (long long)N * H, 0, H, tw, d);
+    }
+    // x forward + Green + x inverse over `planes` ky planes [ky - ky0][kx][kz]
+    static void xgreen_slab(const Plan& p, T* spec, double cg, int planes, int ky0) {
+        C* d = reinterpret_cast<C*>(spec);
+        const dim3 grid((H + TK - 1) / TK, planes);
+        Timed t(p, ST_FFT_X_GREEN);
+        k_fft_x_green<T, N, TK, RV, false, true><<<grid, strided_threads<N, TK, RV>(), smem_s(), p.stream>>>(
+            d, H, (long long)N * H, 0, H, static_cast<const C*>(p.tw), static_cast<const T*>(p.g1d), cg,
+            p.green_kind, d, ky0);
     }
     static constexpr bool kTransposedX = true;
     static void z(const Plan& p, T* mesh, bool forward, int nbox = 1) {
@@ -659,6 +699,43 @@ int poisson_after_z_f32(const Plan& p, float* mesh, double c_poisson, int nbox) 
     PMB_LAUNCH(p, float, {
         PMB_XY_PASSES(p, float, mesh, cg, nbox);
         L_::z(p, mesh, false, nbox);
+    });
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+// ------------------------------------------------ x-slab decomposition
+// The FFT passes of one slab (power-of-two FP32 meshes): the y forward pass
+// over the slab's nx own planes (after the deposit's z R2C), the x forward +
+// Green + x inverse over the nyl ky planes the slab holds after the global
+// transpose, and the y inverse + z C2R over its own planes again.
+#define PMB_SLAB_LAUNCH(P, ...)                                                    \
+    PMB_FFT_DISPATCH((P).ng, {                                                     \
+        if constexpr ((N_ & (N_ - 1)) == 0) {                                      \
+            using L_ = Launch<float, N_>;                                          \
+            __VA_ARGS__;                                                           \
+        } else {                                                                   \
+            return fail(PM_ERR_SIZE, "the slab path needs a power-of-two mesh");   \
+        }                                                                          \
+    })
+
+int slab_fft_forward_y_f32(const Plan& p, float* own, int nx) {
+    PMB_SLAB_LAUNCH(p, L_::y_planes(p, own, -1, nx));
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+int slab_fft_xgreen_f32(const Plan& p, float* spec, double c_poisson, int nyl, int ky0) {
+    const double cg = green_scale(p, c_poisson);
+    PMB_SLAB_LAUNCH(p, L_::xgreen_slab(p, spec, cg, nyl, ky0));
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+int slab_fft_backward_f32(const Plan& p, float* own, int nx) {
+    PMB_SLAB_LAUNCH(p, {
+        L_::y_planes(p, own, +1, nx);
+        L_::z_rows(p, own, false, (long long)nx * N_);
     });
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;

@@ -247,7 +247,9 @@ __device__ __forceinline__ int wrap_near(int c, int n) {
 // The potential values the 2- or 4-point centred differences need at the 8
 // CIC corners (i+a, j+b, k+c), each loaded once: the core rows (i+a, j+b)
 // over the whole z stencil, and the x and y stencil rows at columns k, k+1.
-template <int ORDER, bool POW2> struct Stencil {
+// XPLAIN: the x planes are not periodic -- phi is one slab of a decomposed
+// mesh with its halo planes, and i already indexes the buffer's planes.
+template <int ORDER, bool POW2, bool XPLAIN = false> struct Stencil {
     static constexpr int LO = ORDER == 4 ? -2 : -1, W = ORDER == 4 ? 6 : 4;  // offsets LO..LO+W-1
     static constexpr int C0 = -LO;                                            // slot of offset 0
     float Z[2][2][W], X[W][2][2], Y[2][W][2];
@@ -257,7 +259,7 @@ template <int ORDER, bool POW2> struct Stencil {
         unsigned xo[W], yo[W], kc[W];
 #pragma unroll
         for (int d = 0; d < W; ++d) {
-            xo[d] = (unsigned)wrap_near<POW2>(i + LO + d, n) * plane;
+            xo[d] = (unsigned)(XPLAIN ? i + LO + d : wrap_near<POW2>(i + LO + d, n)) * plane;
             yo[d] = (unsigned)wrap_near<POW2>(j + LO + d, n) * pz;
             kc[d] = (unsigned)wrap_near<POW2>(k + LO + d, n);
         }
@@ -313,11 +315,11 @@ __device__ __forceinline__ void canon_cell(int& i, int& j, int& k, int n) {
     }
 }
 
-template <int ORDER, bool POW2>
+template <int ORDER, bool POW2, bool XPLAIN = false>
 __device__ __forceinline__ void force_at(const float* __restrict__ phi, int n, int i, int j, int k,
                                          float tx, float ty, float tz, float& gx, float& gy,
                                          float& gz) {
-    using St = Stencil<ORDER, POW2>;
+    using St = Stencil<ORDER, POW2, XPLAIN>;
     constexpr int W = St::W, C0 = St::C0;
     const St s(phi, n, i, j, k);
     const float w0[2] = {1.0f - tx, tx}, w1[2] = {1.0f - ty, ty}, w2[2] = {1.0f - tz, tz};
@@ -366,13 +368,17 @@ __global__ void __launch_bounds__(256, 4) k_interp_f32(const float* __restrict__
 // [pbeg[b], pend[b]) of box b in the mesh phi + b * mesh_stride.
 // (at most 64 registers: four 256-thread blocks per SM keep enough warps in
 // flight for the ~60 outstanding gathers per particle)
-template <int ORDER, bool POW2>
+// SLAB: phi is one x-slab [x0, x0 + nxl) of the mesh with two halo planes
+// below and three above (buffer plane = x - x0 + 2); a particle outside the
+// slab is recorded in *err and clamped into it.
+template <int ORDER, bool POW2, bool SLAB = false>
 __global__ void __launch_bounds__(256, 4) k_kick_drift_f32(const float* __restrict__ phi, uint32_t* __restrict__ cell,
                                  float* __restrict__ ox, float* __restrict__ oy, float* __restrict__ oz,
                                  float* __restrict__ vx, float* __restrict__ vy, float* __restrict__ vz,
                                  long long np, float c_kick, double dt, int n,
                                  const long long* __restrict__ pbeg = nullptr,
-                                 const long long* __restrict__ pend = nullptr, long long mesh_stride = 0) {
+                                 const long long* __restrict__ pend = nullptr, long long mesh_stride = 0,
+                                 int x0 = 0, int nxl = 0, int* __restrict__ err = nullptr) {
     const long long lo = pbeg ? pbeg[blockIdx.y] : 0, hi = pbeg ? pend[blockIdx.y] : np;
     if (pbeg) phi += blockIdx.y * mesh_stride;
     for (long long p = lo + blockIdx.x * (long long)blockDim.x + threadIdx.x; p < hi;
@@ -385,7 +391,17 @@ __global__ void __launch_bounds__(256, 4) k_kick_drift_f32(const float* __restri
         canon_cell<POW2>(i, j, k, n);
         const float tx = __ldcs(ox + p), ty = __ldcs(oy + p), tz = __ldcs(oz + p);
         float gx, gy, gz;
-        force_at<ORDER, POW2>(phi, n, i, j, k, tx, ty, tz, gx, gy, gz);
+        if constexpr (SLAB) {
+            int li = (i & (n - 1)) - x0;
+            if (li < 0 || li >= nxl) {
+                atomicOr(err, ERRBIT_RANGE);
+                li = li < 0 ? 0 : nxl - 1;
+            }
+            force_at<ORDER, POW2, true>(phi, n, li + 2, j, k, tx, ty, tz, gx, gy, gz);
+            i = li + x0;  // the drift below starts from the (clamped) cell
+        } else {
+            force_at<ORDER, POW2>(phi, n, i, j, k, tx, ty, tz, gx, gy, gz);
+        }
         const float ux = __ldcs(vx + p) + gx * c_kick, uy = __ldcs(vy + p) + gy * c_kick,
                     uz = __ldcs(vz + p) + gz * c_kick;
         __stcs(vx + p, ux);
@@ -664,6 +680,28 @@ int kick_drift_f32(const Plan& p, const float* phi, uint32_t* cell, float* ox, f
             k_kick_drift_f32<2, true><<<g, kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz, np, ck, dt, p.ng);
         else
             k_kick_drift_f32<2, false><<<g, kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz, np, ck, dt, p.ng);
+    }
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+// Gather + kick + drift of the particles of one x-slab; phi is the slab's
+// buffer (plane 0 = x0 - 2).  Power-of-two meshes only.
+int slab_kick_drift_f32(const Plan& p, int x0, int nx, const float* phi, uint32_t* cell, float* ox, float* oy,
+                        float* oz, float* vx, float* vy, float* vz, int64_t np, double c_kick, double dt) {
+    if (np == 0) return PM_OK;
+    const unsigned g = grid_for(p, np, kThreads, 4);
+    const float ck = (float)c_kick;
+    {
+        Timed t(p, ST_KICK_DRIFT);
+        if (p.grad_order == 4)
+            k_kick_drift_f32<4, true, true><<<g, kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz, np, ck,
+                                                                          dt, p.ng, nullptr, nullptr, 0, x0, nx,
+                                                                          p.d_err);
+        else
+            k_kick_drift_f32<2, true, true><<<g, kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz, np, ck,
+                                                                          dt, p.ng, nullptr, nullptr, 0, x0, nx,
+                                                                          p.d_err);
     }
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;

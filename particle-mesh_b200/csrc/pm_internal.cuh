@@ -192,7 +192,7 @@ int deposit_f32_tiles_batch(Plan& p, const uint32_t* cell, const float* ox, cons
 int kick_drift_f32_batch(const Plan& p, const float* phi, uint32_t* cell, float* ox, float* oy, float* oz,
                          float* vx, float* vy, float* vz, const long long* pbeg, const long long* pend, int nbox,
                          int64_t np_total, double c_kick, double dt);
-int tile_scratch_ensure(Plan& p, int64_t np, int nbox);
+int tile_scratch_ensure(Plan& p, int64_t np, int nbox, long long min_nb = 0);
 // Fused deposit + z R2C (tiles.cu) and the rest of the fused Poisson solve
 // after it (fft.cu): y forward, x forward + Green + x inverse, y inverse, z C2R.
 bool zcol_supported(int ng);
@@ -208,6 +208,17 @@ int interp_f32(const Plan& p, const float* phi, const uint32_t* cell, const floa
                const float* oy, const float* oz, int64_t np, float* fx, float* fy, float* fz);
 int kick_drift_f32(const Plan& p, const float* phi, uint32_t* cell, float* ox, float* oy, float* oz,
                    float* vx, float* vy, float* vz, int64_t np, double c_kick, double dt);
+
+// x-slab decomposition (tiles.cu, fft.cu, particles.cu, slab.cu).
+int slab_deposit_zr2c_f32(Plan& p, int x0, int nx, const uint32_t* cell, const float* ox, const float* oy,
+                          const float* oz, int64_t np, float mass, float* mesh);
+int slab_rank_sort(Plan& p, int nranks, int nx, const uint32_t* cell, int64_t np, int64_t* counts);
+int slab_fft_forward_y_f32(const Plan& p, float* own, int nx);
+int slab_fft_xgreen_f32(const Plan& p, float* spec, double c_poisson, int nyl, int ky0);
+int slab_fft_backward_f32(const Plan& p, float* own, int nx);
+int slab_kick_drift_f32(const Plan& p, int x0, int nx, const float* phi, uint32_t* cell, float* ox, float* oy,
+                        float* oz, float* vx, float* vy, float* vz, int64_t np, double c_kick, double dt);
+int plan_create_internal(int ng, int precision, int green_kind, int grad_order, void* stream, pm_plan** out);
 
 // Adjoint kernels (adjoint.cu).
 int adjoint_gather_f64(const Plan& p, const double* x, const double* y, const double* z, const double* dbar,

@@ -1,0 +1,347 @@
+// x-slab decomposition of one periodic mesh over several ranks (one GPU
+// each): the reference's own parallel layout.  The reference splits the
+// particles and the mesh into cubes, sends each cube with its +1 ghost planes
+// to the owners of FFT x-slabs (src/decomp/slab/transpose_slab.cpp:3-39),
+// folds the ghosts there (reorder_slab.cpp:43-68), lets FFTW-MPI transpose
+// the spectrum (src/fft/fftw/fft.cpp:16, 96-97, FFTW_MPI_TRANSPOSED_OUT/IN),
+// and sends the potential back with -1/+2 ghost planes
+// (reorder_slab_back.cpp:37-49, transpose_slab_back.cpp:3-49).  Here the
+// particles live on the slab that owns their x plane, so:
+//
+//   deposit      the slab's particles, fused with the z R2C, into its own
+//                planes plus one ghost plane (the +1 corners of its last
+//                plane), which the next slab adds to its first plane;
+//   y forward    over the own planes, then rows packed [ky][x][kz] so that
+//                each destination's ky range is contiguous;
+//   (all-to-all) the global transpose;
+//   x + Green    rows unpacked to [ky][kx][kz], x forward, Green, x inverse
+//                along the middle axis, rows packed back [x owner][ky][x];
+//   (all-to-all) the transpose back;
+//   y inverse, z C2R over the own planes;
+//   (halo)       two planes from the previous slab, three from the next
+//                (the 4-point stencil reaches x - 2 .. x + 3);
+//   gather + kick + drift, then particles that left the slab migrate to
+//   their new owner (new: the reference never moves particles).
+//
+// The exchanges belong to the caller (NCCL through torch.distributed, or
+// copies between slabs emulated on one GPU); this file holds the per-slab
+// kernels and buffers.
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "pm_internal.cuh"
+
+namespace pmb {
+
+namespace {
+
+// Row permutations of a slab's share of the half spectrum (rows of H
+// complex, one warp per row, coalesced).  nx = ng / P own x planes, nyl =
+// ng / P ky planes after the transpose, P = ng / nx ranks.
+enum : int { ROWS_PACK_FWD = 0, ROWS_UNPACK_X = 1, ROWS_PACK_X = 2, ROWS_UNPACK_BACK = 3 };
+
+__device__ __forceinline__ long long slab_dst_row(long long row, int mode, int ng, int nx) {
+    const int nyl = nx;
+    switch (mode) {
+        case ROWS_PACK_FWD: {  // [x][ky] -> [ky][x]
+            const long long xl = row / ng, ky = row % ng;
+            return ky * nx + xl;
+        }
+        case ROWS_UNPACK_X: {  // [src][kyl][x] -> [kyl][src x0 + x]
+            const long long xl = row % nx, t = row / nx, kyl = t % nyl, src = t / nyl;
+            return kyl * ng + src * nx + xl;
+        }
+        case ROWS_PACK_X: {  // [kyl][kx] -> [owner of kx][kyl][kx - x0]
+            const long long kx = row % ng, kyl = row / ng;
+            return ((kx / nx) * nyl + kyl) * nx + kx % nx;
+        }
+        default: {  // [ky][x] -> [x][ky]
+            const long long xl = row % nx, ky = row / nx;
+            return xl * ng + ky;
+        }
+    }
+}
+
+__global__ void k_slab_rows(const float2* __restrict__ src, float2* __restrict__ dst, long long nrows, int h,
+                            int mode, int ng, int nx) {
+    const int lane = threadIdx.x & 31;
+    const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long row = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; row < nrows; row += warps) {
+        const float2* s = src + row * h;
+        float2* d = dst + slab_dst_row(row, mode, ng, nx) * h;
+        for (int e = lane; e < h; e += 32) d[e] = __ldcs(s + e);
+    }
+}
+
+// plane += ghost over one padded plane of ng (ng + 2) floats (float2 pairs).
+__global__ void k_fold_plane(float2* __restrict__ plane, const float2* __restrict__ ghost, long long n2) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n2; i += (long long)gridDim.x * blockDim.x) {
+        const float2 a = plane[i], b = ghost[i];
+        plane[i] = make_float2(a.x + b.x, a.y + b.y);
+    }
+}
+
+struct Words {
+    uint32_t* a[8];
+};
+
+// packed[i][w] = arrays[w][perm[i]]: the particles in destination order,
+// W 32-bit words each.
+__global__ void k_pack_words(const uint32_t* __restrict__ perm, long long n, Words src, int nw,
+                             uint32_t* __restrict__ packed) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const uint32_t p = __ldg(perm + i);
+        for (int w = 0; w < nw; ++w) packed[i * nw + w] = src.a[w][p];
+    }
+}
+
+// arrays[w][at + i] = packed[i][w].
+__global__ void k_unpack_words(const uint32_t* __restrict__ packed, long long n, Words dst, int nw, long long at) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        for (int w = 0; w < nw; ++w) dst.a[w][at + i] = __ldg(packed + i * nw + w);
+}
+
+}  // namespace
+
+struct Slab {
+    pm_plan* plan = nullptr;  // FP32 plan of the whole mesh: tables, stream, timers, binning scratch
+    int ng = 0, nranks = 1, rank = 0, nx = 0, x0 = 0, nyl = 0, ky0 = 0;
+    float* buf = nullptr;      // [nx + 6][ng][ng + 2]: planes 0-1 lower halo, 2..nx+1 own, nx+2.. ghost / upper halo
+    float2* send = nullptr;    // nx ng H complex
+    float2* recv = nullptr;    // nx ng H complex
+    size_t bytes = 0;
+    size_t plane_floats() const { return (size_t)ng * (ng + 2); }
+    float* own() const { return buf + 2 * plane_floats(); }
+    long long rows() const { return (long long)nx * ng; }
+};
+
+static int slab_rows(const Slab& s, const float2* src, float2* dst, int mode) {
+    const Plan& p = s.plan->p;
+    const int h = s.ng / 2 + 1;
+    const long long rows = s.rows();
+    k_slab_rows<<<grid_for(p, rows * 32, 256, 8), 256, 0, p.stream>>>(src, dst, rows, h, mode, s.ng, s.nx);
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+static void slab_release(Slab& s) {
+    if (s.buf) cudaFree(s.buf);
+    if (s.send) cudaFree(s.send);
+    if (s.recv) cudaFree(s.recv);
+    if (s.plan) pm_plan_destroy(s.plan);
+    s.buf = nullptr;
+    s.send = s.recv = nullptr;
+    s.plan = nullptr;
+}
+
+}  // namespace pmb
+
+struct pm_slab {
+    pmb::Slab s;
+};
+
+using namespace pmb;
+
+#define PM_TRY_S(expr)                \
+    do {                              \
+        int _rc = (expr);             \
+        if (_rc != PM_OK) return _rc; \
+    } while (0)
+
+static int slab_ok(const pm_slab* slab) {
+    if (!slab || !slab->s.plan) return fail(PM_ERR_ARG, "slab is NULL");
+    int cur = -1;
+    if (cudaGetDevice(&cur) != cudaSuccess) return fail(PM_ERR_CUDA, "cudaGetDevice failed");
+    if (cur != slab->s.plan->p.device) PMB_CUDA_CHECK(cudaSetDevice(slab->s.plan->p.device));
+    return PM_OK;
+}
+
+extern "C" {
+
+int pm_slab_create(int ng, int nranks, int rank, int green_kind, int grad_order, void* stream, pm_slab** out) {
+    if (!out) return fail(PM_ERR_ARG, "output pointer is NULL");
+    *out = nullptr;
+    if (!(ng >= 32 && ng <= 1024 && (ng & (ng - 1)) == 0))
+        return fail(PM_ERR_SIZE, "the slab path needs a power-of-two ng in [32, 1024]");
+    if (nranks < 1 || (nranks & (nranks - 1)) != 0 || ng % (4 * nranks) != 0)
+        return fail(PM_ERR_SIZE, "nranks must be a power of two with ng / nranks a multiple of 4");
+    if (rank < 0 || rank >= nranks) return fail(PM_ERR_ARG, "rank out of range");
+    pm_slab* slab = new (std::nothrow) pm_slab();
+    if (!slab) return fail(PM_ERR_NOMEM, "host allocation failed");
+    Slab& s = slab->s;
+    s.ng = ng;
+    s.nranks = nranks;
+    s.rank = rank;
+    s.nx = s.nyl = ng / nranks;
+    s.x0 = s.ky0 = rank * s.nx;
+    int rc = plan_create_internal(ng, PM_FP32, green_kind, grad_order, stream, &s.plan);
+    if (rc != PM_OK) {
+        delete slab;
+        return rc;
+    }
+    const size_t bufb = (size_t)(s.nx + 6) * s.plane_floats() * sizeof(float);
+    const size_t xfer = (size_t)s.rows() * (ng / 2 + 1) * sizeof(float2);
+    if (cudaMalloc(&s.buf, bufb) != cudaSuccess || cudaMalloc(&s.send, xfer) != cudaSuccess ||
+        cudaMalloc(&s.recv, xfer) != cudaSuccess || cudaMemset(s.buf, 0, bufb) != cudaSuccess) {
+        cudaGetLastError();
+        slab_release(s);
+        delete slab;
+        return fail(PM_ERR_NOMEM, "slab buffer allocation failed");
+    }
+    s.bytes = bufb + 2 * xfer;
+    *out = slab;
+    return PM_OK;
+}
+
+int pm_slab_destroy(pm_slab* slab) {
+    if (!slab) return PM_OK;
+    if (slab->s.plan) {
+        cudaSetDevice(slab->s.plan->p.device);
+        cudaStreamSynchronize(slab->s.plan->p.stream);
+    }
+    slab_release(slab->s);
+    delete slab;
+    return PM_OK;
+}
+
+int pm_slab_info(const pm_slab* slab, int* nx, int* x0, size_t* plane_floats, void** buf, void** send, void** recv,
+                 size_t* xfer_floats, size_t* device_bytes) {
+    if (!slab || !slab->s.plan) return fail(PM_ERR_ARG, "slab is NULL");
+    const Slab& s = slab->s;
+    if (nx) *nx = s.nx;
+    if (x0) *x0 = s.x0;
+    if (plane_floats) *plane_floats = s.plane_floats();
+    if (buf) *buf = s.buf;
+    if (send) *send = s.send;
+    if (recv) *recv = s.recv;
+    if (xfer_floats) *xfer_floats = (size_t)s.rows() * (s.ng + 2);
+    if (device_bytes) *device_bytes = s.bytes + s.plan->p.bytes;
+    return PM_OK;
+}
+
+int pm_slab_plan(pm_slab* slab, pm_plan** plan) {
+    if (!slab || !plan) return fail(PM_ERR_ARG, "NULL argument");
+    *plan = slab->s.plan;
+    return PM_OK;
+}
+
+int pm_slab_deposit_f32(pm_slab* slab, const uint32_t* cell, const float* ox, const float* oy, const float* oz,
+                        int64_t np, float mass) {
+    PM_TRY_S(slab_ok(slab));
+    if (np < 0) return fail(PM_ERR_ARG, "negative particle count");
+    if (np > 0 && (!cell || !ox || !oy || !oz)) return fail(PM_ERR_ARG, "NULL particle array");
+    Slab& s = slab->s;
+    return slab_deposit_zr2c_f32(s.plan->p, s.x0, s.nx, cell, ox, oy, oz, np, mass, s.own());
+}
+
+int pm_slab_fold_f32(pm_slab* slab, const float* ghost) {
+    PM_TRY_S(slab_ok(slab));
+    if (!ghost) return fail(PM_ERR_ARG, "ghost is NULL");
+    Slab& s = slab->s;
+    const Plan& p = s.plan->p;
+    const long long n2 = (long long)s.plane_floats() / 2;
+    {
+        Timed t(p, ST_DEPOSIT);
+        k_fold_plane<<<grid_for(p, n2, 256, 4), 256, 0, p.stream>>>(reinterpret_cast<float2*>(s.own()),
+                                                                    reinterpret_cast<const float2*>(ghost), n2);
+    }
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+int pm_slab_forward_f32(pm_slab* slab) {
+    PM_TRY_S(slab_ok(slab));
+    Slab& s = slab->s;
+    PM_TRY_S(slab_fft_forward_y_f32(s.plan->p, s.own(), s.nx));
+    Timed t(s.plan->p, ST_SORT);
+    return slab_rows(s, reinterpret_cast<const float2*>(s.own()), s.send, ROWS_PACK_FWD);
+}
+
+int pm_slab_xgreen_f32(pm_slab* slab, double c_poisson) {
+    PM_TRY_S(slab_ok(slab));
+    Slab& s = slab->s;
+    float2* x = reinterpret_cast<float2*>(s.own());  // the own planes are free between the transposes
+    {
+        Timed t(s.plan->p, ST_SORT);
+        PM_TRY_S(slab_rows(s, s.recv, x, ROWS_UNPACK_X));
+    }
+    PM_TRY_S(slab_fft_xgreen_f32(s.plan->p, s.own(), c_poisson, s.nyl, s.ky0));
+    Timed t(s.plan->p, ST_SORT);
+    return slab_rows(s, x, s.send, ROWS_PACK_X);
+}
+
+int pm_slab_backward_f32(pm_slab* slab) {
+    PM_TRY_S(slab_ok(slab));
+    Slab& s = slab->s;
+    {
+        Timed t(s.plan->p, ST_SORT);
+        PM_TRY_S(slab_rows(s, s.recv, reinterpret_cast<float2*>(s.own()), ROWS_UNPACK_BACK));
+    }
+    return slab_fft_backward_f32(s.plan->p, s.own(), s.nx);
+}
+
+int pm_slab_kick_drift_f32(pm_slab* slab, uint32_t* cell, float* ox, float* oy, float* oz, float* vx, float* vy,
+                           float* vz, int64_t np, double c_kick, double dt) {
+    PM_TRY_S(slab_ok(slab));
+    if (np < 0) return fail(PM_ERR_ARG, "negative particle count");
+    if (np > 0 && (!cell || !ox || !oy || !oz || !vx || !vy || !vz)) return fail(PM_ERR_ARG, "NULL particle array");
+    Slab& s = slab->s;
+    return slab_kick_drift_f32(s.plan->p, s.x0, s.nx, s.buf, cell, ox, oy, oz, vx, vy, vz, np, c_kick, dt);
+}
+
+int pm_slab_migrate_sort(pm_slab* slab, const uint32_t* cell, int64_t np, int64_t* counts) {
+    PM_TRY_S(slab_ok(slab));
+    if (np < 0 || !counts || (np > 0 && !cell)) return fail(PM_ERR_ARG, "bad migration arguments");
+    if (np > (int64_t)0xffffffffll) return fail(PM_ERR_SIZE, "a slab holds at most 2^32 - 1 particles");
+    Slab& s = slab->s;
+    return slab_rank_sort(s.plan->p, s.nranks, s.nx, cell, np, counts);
+}
+
+int pm_slab_migrate_pack(pm_slab* slab, void* const* arrays, int narrays, int64_t np, uint32_t* packed) {
+    PM_TRY_S(slab_ok(slab));
+    if (!arrays || narrays < 1 || narrays > 8 || np < 0 || (np > 0 && !packed))
+        return fail(PM_ERR_ARG, "bad pack arguments");
+    Words w{};
+    for (int a = 0; a < narrays; ++a) {
+        w.a[a] = static_cast<uint32_t*>(arrays[a]);
+        if (np > 0 && !w.a[a]) return fail(PM_ERR_ARG, "NULL particle array");
+    }
+    Slab& s = slab->s;
+    const Plan& p = s.plan->p;
+    if (np > s.plan->p.tiles.np_cap) return fail(PM_ERR_STATE, "pm_slab_migrate_sort must precede the pack");
+    if (np == 0) return PM_OK;
+    {
+        Timed t(p, ST_SORT);
+        k_pack_words<<<grid_for(p, np, 256, 4), 256, 0, p.stream>>>(p.tiles.perm, np, w, narrays, packed);
+    }
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+int pm_slab_migrate_unpack(pm_slab* slab, const uint32_t* packed, int64_t n, void* const* arrays, int narrays,
+                           int64_t at) {
+    PM_TRY_S(slab_ok(slab));
+    if (!arrays || narrays < 1 || narrays > 8 || n < 0 || at < 0 || (n > 0 && !packed))
+        return fail(PM_ERR_ARG, "bad unpack arguments");
+    Words w{};
+    for (int a = 0; a < narrays; ++a) {
+        w.a[a] = static_cast<uint32_t*>(arrays[a]);
+        if (n > 0 && !w.a[a]) return fail(PM_ERR_ARG, "NULL particle array");
+    }
+    if (n == 0) return PM_OK;
+    const Plan& p = slab->s.plan->p;
+    {
+        Timed t(p, ST_SORT);
+        k_unpack_words<<<grid_for(p, n, 256, 4), 256, 0, p.stream>>>(packed, n, w, narrays, at);
+    }
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+int pm_slab_check(pm_slab* slab) {
+    if (!slab || !slab->s.plan) return fail(PM_ERR_ARG, "slab is NULL");
+    return pm_plan_check(slab->s.plan);
+}
+
+}  // extern "C"

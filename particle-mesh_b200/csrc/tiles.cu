@@ -19,6 +19,8 @@
 // bucket counters; the exclusive scan is a three-kernel block scan.
 #include <algorithm>
 #include <mutex>
+#include <type_traits>
+#include <vector>
 
 #include "fft_engine.cuh"
 
@@ -64,7 +66,31 @@ __device__ __forceinline__ uint32_t column_bucket_of(uint32_t c, int ts_log, int
     return tile * 4u + ((i & m) == m ? 1u : 0u) + ((j & m) == m ? 2u : 0u);
 }
 
-enum : int { KEY_TILE3 = 0, KEY_MORTON = 1, KEY_COLUMN = 2 };
+// Bucket of a particle for the column tiles of one x-slab (planes
+// [x0, x0 + nxl) of the mesh): the column key of the slab-local x plane.  A
+// cell outside the slab (which the slab migration never leaves behind) is
+// clamped into it so that every bucket index stays in range.
+__device__ __forceinline__ uint32_t slab_column_bucket_of(uint32_t c, int nt, int x0, int nxl) {
+    int i, j, k;
+    unpack(c, i, j, k);
+    const int n = nt << 2;
+    if (j >= n) j %= n;
+    int li = i - x0;
+    if (li < 0 || li >= nxl) {
+        li = ((i % n) - x0 + n) % n;
+        if (li >= nxl) li = nxl - 1;
+    }
+    return ((uint32_t)(li >> 2) * nt + (uint32_t)(j >> 2)) * 4u + ((li & 3) == 3 ? 1u : 0u) + ((j & 3) == 3 ? 2u : 0u);
+}
+
+// Owner of a particle in an x-slab decomposition: (i mod n) >> log2(nx).
+__device__ __forceinline__ uint32_t slab_rank_of(uint32_t c, int nx_log, int n) {
+    int i = (int)(c >> 20);
+    if (i >= n) i %= n;
+    return (uint32_t)(i >> nx_log);
+}
+
+enum : int { KEY_TILE3 = 0, KEY_MORTON = 1, KEY_COLUMN = 2, KEY_SLABCOL = 3, KEY_RANK = 4 };
 
 // Morton (Z-order) index of a particle's tile, for the spatial sort.
 __device__ __forceinline__ uint32_t spread3(uint32_t v) {  // 10 bits -> every third bit
@@ -92,11 +118,16 @@ __device__ __forceinline__ uint32_t morton_tile(uint32_t c, int ts_log, int nt) 
 constexpr int kBinU = 4;  // chunks of 32 particles per warp and round in the binning kernels
 
 // Bucket key of particle p (0xffffffff past the end; no bucket has that key).
+// KEY_SLABCOL reads (x0, nxl) from (ts_log, xa), nt the column tiles per
+// axis; KEY_RANK reads log2 of the slab width from ts_log and the mesh size
+// from nt.
 template <int KEY>
 __device__ __forceinline__ uint32_t bin_key(const uint32_t* __restrict__ cell, long long p, long long hi, uint32_t kb,
-                                            int ts_log, int nt) {
+                                            int ts_log, int nt, int xa = 0) {
     if (p >= hi) return 0xffffffffu;
     const uint32_t c = __ldg(cell + p);
+    if (KEY == KEY_SLABCOL) return kb + slab_column_bucket_of(c, nt, ts_log, xa);
+    if (KEY == KEY_RANK) return kb + slab_rank_of(c, ts_log, nt);
     return kb + (KEY == KEY_MORTON ? morton_tile(c, ts_log, nt)
                                    : (KEY == KEY_COLUMN ? column_bucket_of(c, ts_log, nt) : bucket_of(c, ts_log, nt)));
 }
@@ -104,7 +135,7 @@ __device__ __forceinline__ uint32_t bin_key(const uint32_t* __restrict__ cell, l
 template <int KEY>
 __global__ void k_bucket_count(const uint32_t* __restrict__ cell, long long np, int ts_log, int nt,
                                uint32_t* __restrict__ count, const long long* __restrict__ pbeg = nullptr,
-                               const long long* __restrict__ pend = nullptr, long long nb_box = 0) {
+                               const long long* __restrict__ pend = nullptr, long long nb_box = 0, int xa = 0) {
     const int lane = threadIdx.x & 31;
     const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
@@ -114,7 +145,7 @@ __global__ void k_bucket_count(const uint32_t* __restrict__ cell, long long np, 
     for (long long base = lo + warp * 32 * kBinU; base < hi; base += nwarps * 32 * kBinU) {
         uint32_t key[kBinU];
 #pragma unroll
-        for (int u = 0; u < kBinU; ++u) key[u] = bin_key<KEY>(cell, base + u * 32 + lane, hi, kb, ts_log, nt);
+        for (int u = 0; u < kBinU; ++u) key[u] = bin_key<KEY>(cell, base + u * 32 + lane, hi, kb, ts_log, nt, xa);
 #pragma unroll
         for (int u = 0; u < kBinU; ++u) {
             const unsigned peers = __match_any_sync(0xffffffffu, key[u]);
@@ -128,7 +159,7 @@ template <int KEY>
 __global__ void k_bucket_scatter(const uint32_t* __restrict__ cell, long long np, int ts_log, int nt,
                                  uint32_t* __restrict__ cursor, uint32_t* __restrict__ perm,
                                  const long long* __restrict__ pbeg = nullptr,
-                                 const long long* __restrict__ pend = nullptr, long long nb_box = 0) {
+                                 const long long* __restrict__ pend = nullptr, long long nb_box = 0, int xa = 0) {
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
     const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
@@ -141,7 +172,7 @@ __global__ void k_bucket_scatter(const uint32_t* __restrict__ cell, long long np
         uint32_t key[kBinU], at[kBinU];
         unsigned peers[kBinU];
 #pragma unroll
-        for (int u = 0; u < kBinU; ++u) key[u] = bin_key<KEY>(cell, base + u * 32 + lane, hi, kb, ts_log, nt);
+        for (int u = 0; u < kBinU; ++u) key[u] = bin_key<KEY>(cell, base + u * 32 + lane, hi, kb, ts_log, nt, xa);
 #pragma unroll
         for (int u = 0; u < kBinU; ++u) {
             peers[u] = __match_any_sync(0xffffffffu, key[u]);
@@ -373,12 +404,17 @@ __device__ __forceinline__ void zcol_corners(uint32_t c, float fx, float fy, flo
 
 // Three blocks per SM (80 registers; 3 x 67.6 KB of rows at N = 1024): the
 // particle phase of one block overlaps the FFT and store phases of another.
-template <int N>
+// SLAB: the tile rows of one x-slab (blockIdx.x = tx * nt + ty, tx < nx/4 + 1):
+// no periodic x neighbour (tile row 0 takes no x - 1 halo; the previous
+// slab's face particles arrive through its ghost plane), and the tile rows
+// from ntx_own on -- the ghost row, whose plane 0 holds the +1 corners of the
+// slab's last plane -- carry no -1 background.
+template <int N, bool SLAB = false>
 __global__ void __launch_bounds__(zcol_threads<N>(), 3)
 k_deposit_zr2c(const uint32_t* __restrict__ cell, const float* __restrict__ ox, const float* __restrict__ oy,
                const float* __restrict__ oz, const uint32_t* __restrict__ perm, const uint32_t* __restrict__ off,
                float mass, float* __restrict__ mesh, const float2* __restrict__ tw, int nt, long long nb_box = 0,
-               long long mesh_stride = 0, const float* __restrict__ box_mass = nullptr) {
+               long long mesh_stride = 0, const float* __restrict__ box_mass = nullptr, int ntx_own = 0) {
     // a batch of boxes: box blockIdx.y has its own buckets, mesh and mass
     if (box_mass) mass = __ldg(box_mass + blockIdx.y);
     off += blockIdx.y * nb_box;
@@ -394,11 +430,16 @@ k_deposit_zr2c(const uint32_t* __restrict__ cell, const float* __restrict__ ox, 
     for (int c = threadIdx.x; c < kCTRows * RS; c += NTH) S[c] = make_float2(0.f, 0.f);
     if (threadIdx.x < kColRuns) {
         const int q = kColQ[threadIdx.x];
-        const int sx = (tx - (q & 1) + nt) % nt, sy = (ty - ((q >> 1) & 1) + nt) % nt;
-        const uint32_t b = (uint32_t)(sx * nt + sy) * 4u;
-        const uint32_t beg = __ldg(off + b + kColC0[threadIdx.x]);
-        rbeg[threadIdx.x] = beg;
-        rpre[threadIdx.x + 1] = __ldg(off + b + kColC1[threadIdx.x]) - beg;
+        const int sx = SLAB ? tx - (q & 1) : (tx - (q & 1) + nt) % nt, sy = (ty - ((q >> 1) & 1) + nt) % nt;
+        if (SLAB && sx < 0) {  // the slab's first tile row: no x - 1 neighbour here
+            rbeg[threadIdx.x] = 0;
+            rpre[threadIdx.x + 1] = 0;
+        } else {
+            const uint32_t b = (uint32_t)(sx * nt + sy) * 4u;
+            const uint32_t beg = __ldg(off + b + kColC0[threadIdx.x]);
+            rbeg[threadIdx.x] = beg;
+            rpre[threadIdx.x + 1] = __ldg(off + b + kColC1[threadIdx.x]) - beg;
+        }
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -455,8 +496,9 @@ k_deposit_zr2c(const uint32_t* __restrict__ cell, const float* __restrict__ ox, 
     // z R2C of the 16 rows (the z pass of the FFT, input already in shared memory)
     const int rrow = threadIdx.x / NT, tj = threadIdx.x % NT;
     float2* R = S + rrow * RS;
+    const float bg = (!SLAB || tx < ntx_own) ? 1.0f : 0.0f;  // the -1 background
     stockham_pass1<R1, R2, -1, true, float2>(
-        tj, [&](int j, int r) { const float2 v = R[I::in1(j, r)]; return make_float2(v.x - 1.0f, v.y - 1.0f); },
+        tj, [&](int j, int r) { const float2 v = R[I::in1(j, r)]; return make_float2(v.x - bg, v.y - bg); },
         [&](int j, int k, float2 v) { R[I::out1(j, k)] = v; });
     __syncthreads();
     stockham_pass2<R1, R2, -1, true, float2>(
@@ -508,7 +550,7 @@ int bucket_sort(const Plan& p, const uint32_t* cell, int64_t np, int ts_log, int
 
 }  // namespace
 
-int tile_scratch_ensure(Plan& p, int64_t np, int nbox) {
+int tile_scratch_ensure(Plan& p, int64_t np, int nbox, long long min_nb) {
     // the permutation and the bucket offsets are 32-bit particle indices
     if (np > (int64_t)0xffffffffll) return fail(PM_ERR_SIZE, "the FP32 binning holds at most 2^32 - 1 particles");
     const int ts = 1 << tile_log(p.ng), nt = p.ng / ts;
@@ -518,7 +560,7 @@ int tile_scratch_ensure(Plan& p, int64_t np, int nbox) {
     // fused deposit's column tiles x 4 classes
     const long long col = (long long)(p.ng / 4) * (p.ng / 4) * 4;
     const long long per = std::max(std::max((long long)nt * nt * nt * 8, (long long)nt2 * nt2 * nt2), col);
-    const long long nb = per * nbox;
+    const long long nb = std::max(per * nbox, min_nb);
     TileScratch& s = p.tiles;
     if (s.nb < nb) {
         for (uint32_t** q : {&s.count, &s.off, &s.cursor, &s.bsum}) {
@@ -620,6 +662,7 @@ bool zcol_supported(int ng) { return ng >= 32 && ng <= 1024 && (ng & (ng - 1)) =
 template <int N> static int zcol_prepare() {
     const int smem = kCTRows * z_row_stride<N>() * (int)sizeof(float2);
     PMB_CUDA_CHECK(cudaFuncSetAttribute(k_deposit_zr2c<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    PMB_CUDA_CHECK(cudaFuncSetAttribute(k_deposit_zr2c<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     return PM_OK;
 }
 
@@ -710,6 +753,87 @@ int deposit_zr2c_f32_batch(Plan& p, const uint32_t* cell, const float* ox, const
         }
     }
     PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+// ------------------------------------------------------ x-slab decomposition
+// Deposit of one x-slab (planes [x0, x0 + nx) of an ng^3 mesh) fused with the
+// z R2C, into `mesh` = the slab's first own plane: own planes 0..nx-1 receive
+// the z-transformed density contrast (background -1), planes nx..nx+3 the
+// ghost tile row, whose plane nx holds the z-transformed +1 corners of the
+// slab's last plane (background 0) -- the ghost plane the reference sends
+// with its cube (src/decomp/slab/transpose_slab.cpp:23-27) and folds into
+// the next slab (src/decomp/slab/reorder_slab.cpp:43-68).  Every particle
+// must lie in the slab.
+int slab_deposit_zr2c_f32(Plan& p, int x0, int nx, const uint32_t* cell, const float* ox, const float* oy,
+                          const float* oz, int64_t np, float mass, float* mesh) {
+    const int nt = p.ng / kCT, ntx = nx / kCT + 1;
+    const long long nb = (long long)ntx * nt * 4;
+    int rc = tile_scratch_ensure(p, np > 0 ? np : 1, 1, nb);
+    if (rc != PM_OK) return rc;
+    TileScratch& s = p.tiles;
+    const long long nscan = (nb + kScanThreads * kScanItems - 1) / (kScanThreads * kScanItems);
+    PMB_CUDA_CHECK(cudaMemsetAsync(s.count, 0, nb * sizeof(uint32_t), p.stream));
+    const unsigned g = grid_for(p, np, 256);
+    {
+        Timed t(p, ST_BIN, np > 0 ? 5 : 3);
+        if (np > 0)
+            k_bucket_count<KEY_SLABCOL><<<g, 256, 0, p.stream>>>(cell, np, x0, nt, s.count, nullptr, nullptr, 0, nx);
+        k_scan_local<<<(unsigned)nscan, kScanThreads, 0, p.stream>>>(s.count, nb, s.off, s.bsum);
+        k_scan_sums<<<1, kScanThreads, 0, p.stream>>>(s.bsum, (int)nscan, s.off + nb);
+        k_scan_add<<<(unsigned)nscan, kScanThreads, 0, p.stream>>>(s.off, s.cursor, nb, s.bsum);
+        if (np > 0)
+            k_bucket_scatter<KEY_SLABCOL><<<g, 256, 0, p.stream>>>(cell, np, x0, nt, s.cursor, s.perm, nullptr, nullptr,
+                                                                   0, nx);
+    }
+    const float2* tw = static_cast<const float2*>(p.tw);
+    {
+        Timed t(p, ST_DEPOSIT);
+        const unsigned blocks = (unsigned)(ntx * nt);
+        auto go = [&](auto nc) {
+            constexpr int N = decltype(nc)::value;
+            k_deposit_zr2c<N, true><<<blocks, zcol_threads<N>(), kCTRows * z_row_stride<N>() * sizeof(float2),
+                                      p.stream>>>(cell, ox, oy, oz, s.perm, s.off, mass, mesh, tw, nt, 0, 0, nullptr,
+                                                  nx / kCT);
+        };
+        switch (p.ng) {
+            case 32: go(std::integral_constant<int, 32>{}); break;
+            case 64: go(std::integral_constant<int, 64>{}); break;
+            case 128: go(std::integral_constant<int, 128>{}); break;
+            case 256: go(std::integral_constant<int, 256>{}); break;
+            case 512: go(std::integral_constant<int, 512>{}); break;
+            case 1024: go(std::integral_constant<int, 1024>{}); break;
+            default: return fail(PM_ERR_SIZE, "slab deposit needs a power-of-two ng in [32, 1024]");
+        }
+    }
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+// Counting sort of the particles by owning slab (x plane >> log2 nx): the
+// permutation in the plan's scratch, counts[r] (host) particles per rank r.
+int slab_rank_sort(Plan& p, int nranks, int nx, const uint32_t* cell, int64_t np, int64_t* counts) {
+    int nx_log = 0;
+    while ((1 << nx_log) < nx) ++nx_log;
+    const long long nb = nranks;
+    int rc = tile_scratch_ensure(p, np > 0 ? np : 1, 1, nb);
+    if (rc != PM_OK) return rc;
+    TileScratch& s = p.tiles;
+    PMB_CUDA_CHECK(cudaMemsetAsync(s.count, 0, nb * sizeof(uint32_t), p.stream));
+    const unsigned g = grid_for(p, np, 256);
+    {
+        Timed t(p, ST_SORT, np > 0 ? 5 : 3);
+        if (np > 0) k_bucket_count<KEY_RANK><<<g, 256, 0, p.stream>>>(cell, np, nx_log, p.ng, s.count);
+        k_scan_local<<<1, kScanThreads, 0, p.stream>>>(s.count, nb, s.off, s.bsum);
+        k_scan_sums<<<1, kScanThreads, 0, p.stream>>>(s.bsum, 1, s.off + nb);
+        k_scan_add<<<1, kScanThreads, 0, p.stream>>>(s.off, s.cursor, nb, s.bsum);
+        if (np > 0) k_bucket_scatter<KEY_RANK><<<g, 256, 0, p.stream>>>(cell, np, nx_log, p.ng, s.cursor, s.perm);
+    }
+    PMB_CUDA_CHECK(cudaGetLastError());
+    std::vector<uint32_t> off(nb + 1);
+    PMB_CUDA_CHECK(cudaMemcpyAsync(off.data(), s.off, (nb + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, p.stream));
+    PMB_CUDA_CHECK(cudaStreamSynchronize(p.stream));
+    for (long long r = 0; r < nb; ++r) counts[r] = (int64_t)off[r + 1] - (int64_t)off[r];
     return PM_OK;
 }
 
