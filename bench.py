@@ -22,8 +22,10 @@ over every particle; particle-updates/s = particles x steps / time.
   adjoint    adjoint step vs forward step at 128^3 (FP32 split path; FP64 check
              path under "fp64")
 
-Multi-GPU (torchrun): every rank advances its own box (seed + rank) with no
-collective on the data path; the timing is the max over ranks (weak scaling).
+Multi-GPU (torchrun): the configuration's one box is split into x-slabs, one
+per GPU (strong scaling; NCCL ghost fold, spectrum transposes, potential halo
+and particle migration every step), and the ensemble's boxes are dealt to the
+GPUs; every timing is the max over ranks.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -47,6 +49,9 @@ UNIT = "particle-updates/s"
 N_S, RMS, DT, SEED = -1.5, 1.0, 0.005, 1000
 CPU_SAMPLE = (256, 128)  # (mesh, particles per side): 1/64 of the workload
 ACC_STEPS = 50  # the mixed-precision configuration's run length
+# the ensemble autotuner's choices for B200, committed (pm_ensemble_create
+# reads it and measures only the shapes it lacks)
+TUNE_CACHE = os.path.join(ROOT, "particle-mesh_b200", "tune_b200.txt")
 
 
 def parse():
@@ -64,6 +69,8 @@ def parse():
     ap.add_argument("--skip-adjoint", action="store_true")
     ap.add_argument("--skip-accuracy", action="store_true")
     ap.add_argument("--ensemble-boxes", type=int, default=256)
+    ap.add_argument("--slab", action="store_true",
+                    help="run the x-slab decomposition at N = 1 too (at N > 1 it is the default)")
     return ap.parse_args()
 
 
@@ -262,6 +269,181 @@ def reference_arm(args):
     return 0
 
 
+# ------------------------------------------------------------- ensemble
+def ensemble_leg(pm, torch, args, world, rank, dev, stream, barrier, max_over_ranks):
+    """The batched-ensemble configuration: 256 boxes with mesh sizes drawn
+    from {32, 48, 64, 96, 128}, 20 KDK steps as one CUDA graph.  The box list
+    is the same on every rank; at N GPUs the boxes are dealt to the ranks
+    (largest first to the least loaded; independent boxes, no collective) and
+    the throughput counts every box over the slowest rank's time."""
+    import numpy as np
+    nb_ = args.ensemble_boxes
+    rng = np.random.default_rng(4242)
+    sizes = [int(v) for v in rng.choice([32, 48, 64, 96, 128], nb_)]
+    n_s = rng.uniform(-2.5, -1.0, nb_)
+    rms = rng.uniform(0.2, 1.0, nb_)
+    mine = pm.slab.deal_boxes([n ** 3 for n in sizes], world)[rank]
+    cells_, offs_, vels_ = [], [[], [], []], [[], [], []]
+    for b in mine:
+        ngb = sizes[b]
+        pb, vb_ = pm.zeldovich_ic(ngb, ngb, float(n_s[b]), float(rms[b]), 100000 + b, device=dev)
+        splitter = pm.Plan(ngb, "fp32", "spectral", 4, stream=stream, device=dev)
+        cb, ob = splitter.split(*pb)
+        cells_.append(cb)
+        for a in range(3):
+            offs_[a].append(ob[a])
+            vels_[a].append(vb_[a].float())
+        splitter.close()
+        del pb, vb_
+    ecell = torch.cat(cells_)
+    eoff = [torch.cat(t) for t in offs_]
+    evel = [torch.cat(t) for t in vels_]
+    del cells_, offs_, vels_
+    enp = [sizes[b] ** 3 for b in mine]
+    t0 = time.perf_counter()
+    ens = pm.Ensemble([sizes[b] for b in mine], enp, [1.0] * len(mine), "spectral", 4, autotune=True,
+                      tune_cache=TUNE_CACHE if os.path.exists(TUNE_CACHE) else None)
+    t_setup = time.perf_counter() - t0
+    cp = pm.unit_box_coefficients(0.01)[0]
+    esteps, edt = 20, 0.01
+    ens.run(ecell, eoff, evel, cp, edt, esteps)  # capture + first replay
+    torch.cuda.synchronize()
+    barrier()
+    reps = 3
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        ens.run(ecell, eoff, evel, cp, edt, esteps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    t_ens = max_over_ranks(e0.elapsed_time(e1)) / reps
+    info = ens.info()
+    total = int(sum(n ** 3 for n in sizes))
+    out = {"config": f"{nb_} boxes, mesh sizes drawn from {{32,48,64,96,128}}, particles = cells, "
+                     f"P(k)~k^n n~U[-2.5,-1], rms~U[0.2,1.0] cell, {esteps} KDK steps dt={edt}, FP32 split",
+           "particles": total, "value": total * esteps / (t_ens / 1e3),
+           "unit": UNIT, "ms_per_run": t_ens, "ms_per_step": t_ens / esteps,
+           "boxes_per_rank": len(mine), "graph_nodes": info["graph_nodes"], "classes": info["classes"],
+           "setup_s_incl_autotune": t_setup,
+           "note": "one CUDA graph per run of 20 KDK steps (21 force evaluations); batched kernels per "
+                   "mesh-size class, classes on parallel graph branches; boxes dealt to ranks"}
+    ens.close()
+    del ens, ecell, eoff, evel
+    torch.cuda.empty_cache()
+    return out
+
+
+# --------------------------------------------------- N GPUs: one slab each
+def ours_slab(args, pm, torch, dist, world, rank, dev, stream, barrier, max_over_ranks):
+    """The configuration's one box (512^3 particles on a 1024^3 mesh) split
+    over the N GPUs as x-slabs (strong scaling): per step the ghost-plane
+    fold, two all-to-all transposes of the spectrum, the potential halo and
+    the particle migration go over NCCL (slab.DistExchange)."""
+    S = pm.slab
+    ng, nrow = args.ng, args.nrow
+    np_ = nrow ** 3
+    mass = ng ** 3 / np_
+    cp, ck = pm.unit_box_coefficients(DT)
+    pos, vel = pm.zeldovich_ic(ng, nrow, N_S, RMS, rank_seed(0), device=dev)  # the one box, on every rank
+    splitter = pm.Plan(ng, "fp32", "spectral", 4, stream=stream, device=dev)
+    cell, off = splitter.split(*pos)
+    splitter.close()
+    v32 = [a.float() for a in vel]
+    ids = torch.arange(np_, dtype=torch.int32, device=dev)
+    del pos, vel
+    (part,) = S.distribute(cell, off, v32, ids, ng, world, [rank])
+    del cell, off, v32, ids
+    torch.cuda.empty_cache()
+    slab = S.Slab(ng, world, rank, "spectral", 4, stream=stream, device=dev)
+    ex = S.DistExchange()
+    sampler = ClockSampler(bus_id(torch, dev))
+    for _ in range(args.warmup):
+        S.step([slab], [part], ex, mass, cp, ck, DT)
+    slab.check()
+    slab.read_timing(reset=True)
+    slab.set_timing(True)
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        S.step([slab], [part], ex, mass, cp, ck, DT)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    barrier()
+    slab.set_timing(False)
+    t_ms = max_over_ranks(e0.elapsed_time(e1))
+    stages = slab.read_timing(reset=True)
+    launches = sum(n for _, n in stages.values())
+    slab.check()
+    value = np_ * args.steps / (t_ms / 1e3)
+    peak, peak_kind = measured_peaks()
+    per_stage = {s_: {"ms_per_step": ms / args.steps, "launches": n} for s_, (ms, n) in stages.items()}
+    dom = max(stages, key=lambda s_: stages[s_][0])
+    # algorithmic bytes of this rank's share: the single-box byte model scaled
+    # by the slab's share of the mesh and of the particles
+    share = 1.0 / world
+    dom_bytes = stage_bytes(dom, ng, np_, 4) * share if dom in ("deposit", "kick_drift", "bin") or \
+        dom.startswith("fft_") else None
+    dom_ms = stages[dom][0] / args.steps
+    roofline = {"bound": "hbm", "kernel": dom, "peak": peak, "unit": "GB/s",
+                "peak_source": f"{peak_kind} hbm_gbs (copy bandwidth)", "ms_per_launch": dom_ms,
+                "achieved": dom_bytes / (dom_ms / 1e3) / 1e9 if dom_bytes else None,
+                "frac": dom_bytes / (dom_ms / 1e3) / 1e9 / peak if dom_bytes else None, "traffic": None,
+                "note": "per rank; the byte model of one box times the slab's share"}
+    # ---- end to end: this rank's particle state from pinned host memory and
+    # back every step
+    host = torch.empty(part.words.shape, dtype=torch.int32, pin_memory=True)
+    host.copy_(part.words)
+    nbytes = part.n * 8 * 4
+
+    def e2e_step():
+        part.words[:, :part.n].copy_(host[:, :part.n], non_blocking=True)
+        S.step([slab], [part], ex, mass, cp, ck, DT)
+        host[:, :part.n].copy_(part.words[:, :part.n], non_blocking=True)
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    te = max_over_ranks(e0.elapsed_time(e1))
+    e2e = {"value": np_ * args.steps / (te / 1e3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
+           "d2h_bytes_per_step": nbytes, "ms_per_step": te / args.steps,
+           "path": "slab.step (pm_slab_* through the C ABI, NCCL exchanges); this rank's particle words copied "
+                   "from pinned host memory and back every step"}
+    ensemble = None
+    if not args.skip_ensemble:
+        slab.close()
+        del part, host
+        torch.cuda.empty_cache()
+        ensemble = ensemble_leg(pm, torch, args, world, rank, dev, stream, barrier, max_over_ranks)
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{nrow}^3 particles on {ng}^3 mesh, FP32 mesh/FFT/forces, split positions, "
+                                   f"spectral Poisson, 4-point gradient, KDK dt={DT}, Zel'dovich P(k)~k^{N_S} "
+                                   f"rms {RMS} cell",
+                       "particles_total": np_, "mesh": ng, "l2": "inputs larger than L2",
+                       "parallelism": f"slab{world}: x-slabs of {ng // world} planes, one per GPU; NCCL ghost "
+                                      f"fold, two all-to-all transposes, potential halo, particle migration"},
+            "stages": per_stage, "ensemble": ensemble, "e2e": e2e, "roofline": roofline, "cpu_baseline": None,
+            "clocks": clocks, "gpu_launches": launches}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 # -------------------------------------------------------------- GPU side
 def ours(args):
     import torch
@@ -290,6 +472,8 @@ def ours(args):
     mass = ng ** 3 / np_
     cp, ck = pm.unit_box_coefficients(DT)
     stream = torch.cuda.current_stream(dev)
+    if world > 1 or args.slab:
+        return ours_slab(args, pm, torch, dist, world, rank, dev, stream, barrier, max_over_ranks)
 
     pos, vel = pm.zeldovich_ic(ng, nrow, N_S, RMS, rank_seed(rank), device=dev)
     p32 = pm.Plan(ng, "fp32", "spectral", 4, stream=stream, device=dev)
@@ -523,55 +707,7 @@ def ours(args):
     # ---- batched ensemble: 256 boxes of mixed mesh sizes, 20 KDK steps per graph
     ensemble = None
     if not args.skip_ensemble:
-        import numpy as np
-        nb_ = args.ensemble_boxes
-        rng = np.random.default_rng(4242 + rank)
-        sizes = [int(v) for v in rng.choice([32, 48, 64, 96, 128], nb_)]
-        n_s = rng.uniform(-2.5, -1.0, nb_)
-        rms = rng.uniform(0.2, 1.0, nb_)
-        cells_, offs_, vels_ = [], [[], [], []], [[], [], []]
-        for b, ngb in enumerate(sizes):
-            pb, vb_ = pm.zeldovich_ic(ngb, ngb, float(n_s[b]), float(rms[b]), 100000 + 1000 * rank + b, device=dev)
-            splitter = pm.Plan(ngb, "fp32", "spectral", 4, stream=stream, device=dev)
-            cb, ob = splitter.split(*pb)
-            cells_.append(cb)
-            for a in range(3):
-                offs_[a].append(ob[a])
-                vels_[a].append(vb_[a].float())
-            splitter.close()
-            del pb, vb_
-        ecell = torch.cat(cells_)
-        eoff = [torch.cat(t) for t in offs_]
-        evel = [torch.cat(t) for t in vels_]
-        del cells_, offs_, vels_
-        enp = [n ** 3 for n in sizes]
-        t0 = time.perf_counter()
-        ens = pm.Ensemble(sizes, enp, [1.0] * nb_, "spectral", 4, autotune=True)
-        t_setup = time.perf_counter() - t0
-        esteps, edt = 20, 0.01
-        ens.run(ecell, eoff, evel, cp, edt, esteps)  # capture + first replay
-        torch.cuda.synchronize()
-        barrier()
-        reps = 3
-        e0.record(stream)
-        for _ in range(reps):
-            ens.run(ecell, eoff, evel, cp, edt, esteps)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        barrier()
-        t_ens = max_over_ranks(e0.elapsed_time(e1)) / reps
-        info = ens.info()
-        ensemble = {"config": f"{nb_} boxes, mesh sizes drawn from {{32,48,64,96,128}}, particles = cells, "
-                              f"P(k)~k^n n~U[-2.5,-1], rms~U[0.2,1.0] cell, {esteps} KDK steps dt={edt}, FP32 split",
-                    "particles": int(sum(enp)), "value": throughput(world, int(sum(enp)), esteps, t_ens),
-                    "unit": UNIT, "ms_per_run": t_ens, "ms_per_step": t_ens / esteps,
-                    "graph_nodes": info["graph_nodes"], "classes": info["classes"],
-                    "setup_s_incl_autotune": t_setup,
-                    "note": "one CUDA graph per run of 20 KDK steps (21 force evaluations); batched kernels per "
-                            "mesh-size class, classes on parallel graph branches"}
-        ens.close()
-        del ens, ecell, eoff, evel
-        torch.cuda.empty_cache()
+        ensemble = ensemble_leg(pm, torch, args, world, rank, dev, stream, barrier, max_over_ranks)
 
     # ---- end to end through the C ABI with host buffers
     e2e = None

@@ -140,6 +140,22 @@ class Slab:
     def check(self):
         check(self.lib.pm_slab_check(self._h))
 
+    def plan_handle(self):
+        """The slab's pm_plan (stage timers, stream)."""
+        h = ctypes.c_void_p()
+        check(self.lib.pm_slab_plan(self._h, ctypes.byref(h)))
+        return h
+
+    def set_timing(self, on: bool = True):
+        check(self.lib.pm_plan_set_timing(self.plan_handle(), 1 if on else 0))
+
+    def read_timing(self, reset: bool = True) -> dict:
+        """{stage: (milliseconds, launches)} of the slab's kernels since the last reset."""
+        ms = (ctypes.c_double * L.STAGE_COUNT)()
+        n = (ctypes.c_int64 * L.STAGE_COUNT)()
+        check(self.lib.pm_plan_read_timing(self.plan_handle(), ms, n, 1 if reset else 0))
+        return {self.lib.pm_stage_name(i).decode(): (ms[i], n[i]) for i in range(L.STAGE_COUNT) if n[i]}
+
     def device_bytes(self) -> int:
         nb = ctypes.c_size_t()
         check(self.lib.pm_slab_info(self._h, None, None, None, None, None, None, None, ctypes.byref(nb)))
@@ -311,6 +327,18 @@ def step(slabs, parts, exchange, mass: float, c_poisson: float, c_kick: float, d
     for s, q in zip(slabs, parts):
         s.kick_drift(q, c_kick, dt)
     exchange.migrate(slabs, parts)
+
+
+def deal_boxes(particles_per_box, nranks: int):
+    """Boxes of an ensemble dealt to ranks, largest first to the least loaded
+    rank (independent boxes: no exchange).  Returns one box list per rank."""
+    load = [0] * nranks
+    out = [[] for _ in range(nranks)]
+    for b in sorted(range(len(particles_per_box)), key=lambda b: (-particles_per_box[b], b)):
+        r = min(range(nranks), key=lambda r: (load[r], r))
+        out[r].append(b)
+        load[r] += particles_per_box[b]
+    return [sorted(o) for o in out]
 
 
 def distribute(cell, off, vel, ids, ng: int, nranks: int, ranks, cap_factor: float = 1.5, device=None):

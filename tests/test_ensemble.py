@@ -1,4 +1,4 @@
-"""Batched ensemble of boxes with mixed mesh sizes (32, 48, 64, 96): one CUDA
+"""Batched ensemble of boxes with mixed mesh sizes (32 to 128): one CUDA
 graph of a KDK run versus each box advanced alone with its own FP32 plan
 through the same schedule; the eager step versus the graph; the autotuner's
 cache file."""
@@ -53,16 +53,16 @@ def solo(pmpkg, sizes, cell, off, vel, cp, dt, steps):
 
 
 def test_ensemble_graph_matches_boxes_alone(pmpkg, tmp_path):
-    sizes = [32, 48, 64, 32, 96, 48]
-    seeds = [5, 6, 7, 8, 9, 10]
+    sizes = [32, 48, 64, 32, 96, 48, 128]
+    seeds = [5, 6, 7, 8, 9, 10, 11]
     cp, dt, steps = 4 * np.pi, 0.01, 3
     cell, off, vel = boxes_state(pmpkg, sizes, seeds)
     ref_c, ref_o, ref_v = solo(pmpkg, sizes, cell, off, vel, cp, dt, steps)
     cache = tmp_path / "tune.txt"
     ens = pmpkg.Ensemble(sizes, [n ** 3 for n in sizes], [1.0] * len(sizes), tune_cache=str(cache))
     info = ens.info()
-    assert sorted(c["ng"] for c in info["classes"]) == [32, 48, 64, 96]
-    assert cache.exists() and len(cache.read_text().splitlines()) == 4
+    assert sorted(c["ng"] for c in info["classes"]) == [32, 48, 64, 96, 128]
+    assert cache.exists() and len(cache.read_text().splitlines()) == 5
     c, o, v = cell.clone(), [t.clone() for t in off], [t.clone() for t in vel]
     ens.run(c, o, v, cp, dt, steps)
     torch.cuda.synchronize()
@@ -114,3 +114,29 @@ def test_fft_shapes_agree(pmpkg, ng):
         plan.set_fft_shape(12, 0)
     with pytest.raises(pmpkg.PMError):
         plan.set_fft_shape(0, 3)
+
+
+def test_dealt_boxes_match_the_whole_ensemble(pmpkg):
+    """Boxes dealt to two ranks (slab.deal_boxes, as bench.py --gpus 2 does):
+    each rank's ensemble of its own boxes gives those boxes the state the
+    whole ensemble gives them (independent boxes; FP32 rounding)."""
+    sizes = [32, 64, 48, 128, 32, 96, 64, 48]
+    seeds = list(range(20, 28))
+    cp, dt, steps = 4 * np.pi, 0.01, 2
+    cell, off, vel = boxes_state(pmpkg, sizes, seeds)
+    whole = pmpkg.Ensemble(sizes, [n ** 3 for n in sizes], [1.0] * len(sizes), autotune=False)
+    wc, wo, wv = cell.clone(), [t.clone() for t in off], [t.clone() for t in vel]
+    whole.run(wc, wo, wv, cp, dt, steps)
+    starts = np.cumsum([0] + [n ** 3 for n in sizes])
+    deal = pmpkg.slab.deal_boxes([n ** 3 for n in sizes], 2)
+    assert sorted(b for d in deal for b in d) == list(range(len(sizes)))
+    for mine in deal:
+        idx = torch.cat([torch.arange(int(starts[b]), int(starts[b + 1]), device=DEV) for b in mine])
+        c, o, v = cell[idx].clone(), [t[idx].clone() for t in off], [t[idx].clone() for t in vel]
+        ens = pmpkg.Ensemble([sizes[b] for b in mine], [sizes[b] ** 3 for b in mine], [1.0] * len(mine),
+                             autotune=False)
+        ens.run(c, o, v, cp, dt, steps)
+        torch.cuda.synchronize()
+        dv = max(float((a - b[idx]).abs().max()) for a, b in zip(v, wv))
+        assert dv < 1e-4 * max(float(t.abs().max()) for t in wv), dv
+        assert float((c != wc[idx]).float().mean()) < 1e-3

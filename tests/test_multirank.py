@@ -1,7 +1,7 @@
-"""Multi-GPU host logic on CPU ranks (gloo, world size 2): every rank runs its
-own box (distinct seeds), the timed region is the max over ranks, and the
-whole-job throughput counts every rank's particles.  No data-path
-collective exists to test: boxes are independent."""
+"""Multi-GPU host logic on CPU ranks (gloo, world size 2): the timed region is
+the max over ranks, the whole-job throughput counts every rank's particles,
+and the ensemble's boxes are dealt to the ranks (disjoint, complete,
+balanced).  The slab decomposition's exchanges are tested in test_slab.py."""
 import os
 import socket
 
@@ -21,14 +21,19 @@ def _free_port():
 def _rank(rank, world, port, q):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     import sys
-    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path[:0] = [root, os.path.join(root, "particle-mesh_b200")]
     import bench
     from datetime import timedelta
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
     local_ms = 100.0 + 50.0 * rank
     t = bench.reduce_max(local_ms, world, "cpu")
     v = bench.throughput(world, 1000, 10, t)
-    q.put((rank, t, v, bench.rank_seed(rank)))
+    from loader import load_package
+    S = load_package().slab
+    sizes = [n ** 3 for n in (32, 48, 64, 96, 128, 32, 64, 128, 96, 48, 48)]
+    mine = S.deal_boxes(sizes, world)[rank]
+    q.put((rank, t, v, bench.rank_seed(rank), mine, sum(sizes[b] for b in mine)))
     dist.barrier()
     dist.destroy_process_group()
 
@@ -45,6 +50,11 @@ def test_two_rank_timing_and_seeds():
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    assert all(t == pytest.approx(150.0) for _, t, _, _ in out)
-    assert all(v == pytest.approx(2 * 1000 * 10 / 0.150) for _, _, v, _ in out)
-    assert len({s for _, _, _, s in out}) == world
+    assert all(o[1] == pytest.approx(150.0) for o in out)
+    assert all(o[2] == pytest.approx(2 * 1000 * 10 / 0.150) for o in out)
+    assert len({o[3] for o in out}) == world
+    # ensemble boxes dealt to the ranks: disjoint, every box once, balanced
+    dealt = [b for o in out for b in o[4]]
+    assert sorted(dealt) == list(range(11))
+    loads = [o[5] for o in out]
+    assert max(loads) - min(loads) <= 128 ** 3
