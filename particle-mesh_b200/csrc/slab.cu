@@ -70,7 +70,16 @@ __global__ void k_slab_rows(const float2* __restrict__ src, float2* __restrict__
     for (long long row = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; row < nrows; row += warps) {
         const float2* s = src + row * h;
         float2* d = dst + slab_dst_row(row, mode, ng, nx) * h;
-        for (int e = lane; e < h; e += 32) d[e] = __ldcs(s + e);
+        // eight loads in flight per lane, then the stores
+        for (int e0 = lane; e0 < h; e0 += 32 * 8) {
+            float2 v[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                if (e0 + 32 * u < h) v[u] = __ldcs(s + e0 + 32 * u);
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                if (e0 + 32 * u < h) d[e0 + 32 * u] = v[u];
+        }
     }
 }
 

@@ -224,6 +224,8 @@ class LocalExchange:
 
     def migrate(self, slabs, parts):
         p = len(slabs)
+        if p == 1:  # one slab holds the whole periodic mesh: nothing leaves it
+            return
         groups = []
         for s, q in zip(slabs, parts):
             counts = s.migrate_sort(q)
@@ -287,13 +289,12 @@ class DistExchange:
     def migrate(self, slabs, parts):
         (s,), (q,) = slabs, parts
         p = s.nranks
+        if p == 1:  # one slab holds the whole periodic mesh: nothing leaves it
+            return
         dev = q.words.device
         counts = s.migrate_sort(q)
         packed = torch.empty((max(q.n, 1), WORDS), dtype=torch.int32, device=dev)
         s.migrate_pack(q, packed)
-        if p == 1:
-            s.migrate_unpack(packed, q.n, q, 0)
-            return
         send_c = torch.tensor(counts, dtype=torch.int64, device=dev)
         recv_c = torch.empty_like(send_c)
         self.dist.all_to_all_single(recv_c, send_c, group=self.group)
