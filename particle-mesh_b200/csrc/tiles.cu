@@ -372,28 +372,18 @@ template <int N> constexpr int zcol_threads() { return kCTRows * (N / 2) / Radix
 // i & 3 == 3 and only the a = 1 corners land here, in column 0), bit 1 the
 // y - 1 tile (likewise in y).  Two z cells per corner, FP32 shared atomics
 // into the padded complex rows (real index k at 2 zpad(k / 2) + k % 2).
-#ifndef PMB_DEP_V
-#define PMB_DEP_V 0
-#endif
 template <int N, int R1, int RS, int Q>
-__device__ __forceinline__ void zcol_corners(uint32_t c, float fx, float fy, float fz, float mass, float* Sf,
-                                             int half = -1) {
+__device__ __forceinline__ void zcol_corners(uint32_t c, float fx, float fy, float fz, float mass, float* Sf) {
     int i, j, k;
     unpack(c, i, j, k);
     if (k >= N) k %= N;
     const int k1 = (k + 1) & (N - 1);
     const int z0 = 2 * zpad<R1>(k >> 1) + (k & 1), z1 = 2 * zpad<R1>(k1 >> 1) + (k1 & 1);
     const float wz0 = mass * (1.0f - fz), wz1 = mass * fz;
-    const int zh = half ? z1 : z0;
-    const float wh = half ? wz1 : wz0;
     auto put = [&](int ci, int cj, float w) {
         float* row = Sf + (ci * kCT + cj) * (2 * RS);
-        if (PMB_DEP_V & 2) {
-            atomicAdd(row + zh, w * wh);
-        } else {
-            atomicAdd(row + z0, w * wz0);
-            atomicAdd(row + z1, w * wz1);
-        }
+        atomicAdd(row + z0, w * wz0);
+        atomicAdd(row + z1, w * wz1);
     };
     const int li = i & (kCT - 1), lj = j & (kCT - 1);
     if (Q == 0) {
@@ -420,7 +410,7 @@ __device__ __forceinline__ void zcol_corners(uint32_t c, float fx, float fy, flo
 // from ntx_own on -- the ghost row, whose plane 0 holds the +1 corners of the
 // slab's last plane -- carry no -1 background.
 template <int N, bool SLAB = false>
-__global__ void __launch_bounds__(zcol_threads<N>(), (PMB_DEP_V & 4) ? 2 : 3)
+__global__ void __launch_bounds__(zcol_threads<N>(), 3)
 k_deposit_zr2c(const uint32_t* __restrict__ cell, const float* __restrict__ ox, const float* __restrict__ oy,
                const float* __restrict__ oz, const uint32_t* __restrict__ perm, const uint32_t* __restrict__ off,
                float mass, float* __restrict__ mesh, const float2* __restrict__ tw, int nt, long long nb_box = 0,
@@ -463,16 +453,13 @@ k_deposit_zr2c(const uint32_t* __restrict__ cell, const float* __restrict__ ox, 
     const uint32_t p1 = rpre[1], p2 = rpre[2], p3 = rpre[3], p4 = rpre[4];
     const uint32_t d0 = rbeg[0], d1 = rbeg[1] - p1, d2 = rbeg[2] - p2, d3 = rbeg[3] - p3, d4 = rbeg[4] - p4;
     // four particles per thread per round, their loads issued together
-    // (variant 2: two lanes per particle, one z corner each)
     constexpr int U = 4;
-    constexpr int HS = (PMB_DEP_V & 2) ? 1 : 0;
-    const uint32_t items = total << HS;
-    for (uint32_t t0 = threadIdx.x; t0 < items; t0 += U * NTH) {
+    for (uint32_t t0 = threadIdx.x; t0 < total; t0 += U * NTH) {
         uint32_t pidx[U];
         int qq[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            const uint32_t t = (t0 + u * NTH) >> HS;
+            const uint32_t t = t0 + u * NTH;
             uint32_t d = d0;
             int q = 0;
             if (t >= p1) d = d1, q = 1;
@@ -496,12 +483,11 @@ k_deposit_zr2c(const uint32_t* __restrict__ cell, const float* __restrict__ ox, 
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             // q is uniform across a warp except at run boundaries
-            const int hf = HS ? (int)((t0 + u * NTH) & 1u) : -1;
             switch (qq[u]) {
-                case 0: zcol_corners<N, R1, RS, 0>(cc[u], fx[u], fy[u], fz[u], mass, Sf, hf); break;
-                case 1: zcol_corners<N, R1, RS, 1>(cc[u], fx[u], fy[u], fz[u], mass, Sf, hf); break;
-                case 2: zcol_corners<N, R1, RS, 2>(cc[u], fx[u], fy[u], fz[u], mass, Sf, hf); break;
-                case 3: zcol_corners<N, R1, RS, 3>(cc[u], fx[u], fy[u], fz[u], mass, Sf, hf); break;
+                case 0: zcol_corners<N, R1, RS, 0>(cc[u], fx[u], fy[u], fz[u], mass, Sf); break;
+                case 1: zcol_corners<N, R1, RS, 1>(cc[u], fx[u], fy[u], fz[u], mass, Sf); break;
+                case 2: zcol_corners<N, R1, RS, 2>(cc[u], fx[u], fy[u], fz[u], mass, Sf); break;
+                case 3: zcol_corners<N, R1, RS, 3>(cc[u], fx[u], fy[u], fz[u], mass, Sf); break;
                 default: break;
             }
         }
@@ -515,14 +501,11 @@ k_deposit_zr2c(const uint32_t* __restrict__ cell, const float* __restrict__ ox, 
         tj, [&](int j, int r) { const float2 v = R[I::in1(j, r)]; return make_float2(v.x - bg, v.y - bg); },
         [&](int j, int k, float2 v) { R[I::out1(j, k)] = v; });
     __syncthreads();
-    if constexpr ((PMB_DEP_V & 1) != 0 && R2 >= 16)
-        stockham_pass2<R1, R2, -1, true, float2>(
-            tj, [&](int j, int r) { return R[I::p2(j, r)]; }, [&](int j, int k, float2 v) { R[I::p2(j, k)] = v; },
-            pass2_twiddles<-1, true, 2>(tw, tj));
-    else
-        stockham_pass2<R1, R2, -1, true, float2>(
-            tj, [&](int j, int r) { return R[I::p2(j, r)]; }, [&](int j, int k, float2 v) { R[I::p2(j, k)] = v; },
-            [&](int e) { return twiddle<-1>(tw, 2 * e); });
+    // pass-2 twiddles from 10 table loads per thread (3.80 vs 4.27 ms at
+    // 1024^3 with 512^3 particles on B200)
+    stockham_pass2<R1, R2, -1, true, float2>(
+        tj, [&](int j, int r) { return R[I::p2(j, r)]; }, [&](int j, int k, float2 v) { R[I::p2(j, k)] = v; },
+        pass2_twiddles<-1, (R2 >= 16), 2>(tw, tj));
     __syncthreads();
     const int ci = rrow / kCT, cj = rrow % kCT;
     float2* crow = reinterpret_cast<float2*>(mesh + ((long long)(tx * kCT + ci) * N + (ty * kCT + cj)) * (N + 2));
