@@ -230,6 +230,7 @@ static int plan_create(int ng, int precision, int green_kind, int grad_order, vo
     }
     if (rc == PM_OK) rc = fft_prepare(p);
     if (rc == PM_OK && precision == PM_FP32) rc = deposit_zr2c_prepare(p);
+    if (rc == PM_OK && precision == PM_FP32 && tiled_gather_supported(ng)) rc = tiled_gather_prepare();
     if (rc == PM_OK) {
         p.timers = new (std::nothrow) StageTimers();
         if (!p.timers) rc = fail(PM_ERR_NOMEM, "host allocation failed");
@@ -568,6 +569,14 @@ int pm_step_f32(pm_plan* plan, uint32_t* cell, float* ox, float* oy, float* oz, 
     Plan& p = plan->p;
     PM_TRY(ensure_workspace(p, false));
     float* m = static_cast<float*>(p.mesh);
+    if (tiled_gather_supported(p.ng)) {
+        // binned by (column tile, class, z chunk): the deposit fused with the
+        // z FFT pass, and the gather from potential tiles staged in shared
+        // memory in the same bin order
+        PM_TRY(deposit_zr2c_f32(p, cell, ox, oy, oz, np, mass, m, tiled_gather_zcb(p.ng)));
+        PM_TRY(poisson_after_z_f32(p, m, c_poisson));
+        return kick_drift_tiles_f32(p, m, cell, ox, oy, oz, vx, vy, vz, np, c_kick, dt);
+    }
     if (zcol_supported(p.ng)) {  // deposit fused with the z FFT pass
         PM_TRY(deposit_zr2c_f32(p, cell, ox, oy, oz, np, mass, m));
         PM_TRY(poisson_after_z_f32(p, m, c_poisson));

@@ -315,13 +315,55 @@ __device__ __forceinline__ void canon_cell(int& i, int& j, int& k, int n) {
     }
 }
 
-template <int ORDER, bool POW2, bool XPLAIN = false>
-__device__ __forceinline__ void force_at(const float* __restrict__ phi, int n, int i, int j, int k,
-                                         float tx, float ty, float tz, float& gx, float& gy,
-                                         float& gz) {
-    using St = Stencil<ORDER, POW2, XPLAIN>;
+// The same 56 (or 32) values from a block's staged potential in shared
+// memory: rows of (x, y) on a square of side RW, z at padded index
+// zp(z) = z + z / 32 within a row of RL floats (lanes two cells apart in z
+// then fall on distinct banks).
+template <int ORDER, int RW, int RL> struct SmemStencil {
+    static constexpr int LO = ORDER == 4 ? -2 : -1, W = ORDER == 4 ? 6 : 4, C0 = -LO;
+    float Z[2][2][W], X[W][2][2], Y[2][W][2];
+    static __device__ __forceinline__ float D(const float* v, int s) {
+        return ORDER == 4 ? (8.0f * (v[s - 1] - v[s + 1]) - (v[s - 2] - v[s + 2])) * (1.0f / 12.0f)
+                          : (v[s - 1] - v[s + 1]) * 0.5f;
+    }
+    __device__ __forceinline__ SmemStencil(const float* __restrict__ S, int lx, int ly, int lz) {
+        int xo[W], yo[W], kc[W];
+#pragma unroll
+        for (int d = 0; d < W; ++d) {
+            xo[d] = (lx + LO + d) * (RW * RL);
+            yo[d] = (ly + LO + d) * RL;
+            const int z = lz + LO + d;
+            kc[d] = z + (z >> 5);
+        }
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+            for (int b = 0; b < 2; ++b)
+#pragma unroll
+                for (int c = 0; c < W; ++c) Z[a][b][c] = S[xo[C0 + a] + yo[C0 + b] + kc[c]];
+#pragma unroll
+        for (int d = 0; d < W; ++d)
+#pragma unroll
+            for (int b = 0; b < 2; ++b)
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    if (d == C0 || d == C0 + 1) {
+                        X[d][b][c] = Z[d - C0][b][C0 + c];
+                        Y[b][d][c] = Z[b][d - C0][C0 + c];
+                    } else {
+                        X[d][b][c] = S[xo[d] + yo[C0 + b] + kc[C0 + c]];
+                        Y[b][d][c] = S[xo[C0 + b] + yo[d] + kc[C0 + c]];
+                    }
+                }
+    }
+};
+
+// -grad phi interpolated at in-cell offsets (tx, ty, tz) from a stencil's
+// values (Stencil or SmemStencil).
+template <class St>
+__device__ __forceinline__ void force_from(const St& s, float tx, float ty, float tz, float& gx, float& gy,
+                                           float& gz) {
     constexpr int W = St::W, C0 = St::C0;
-    const St s(phi, n, i, j, k);
     const float w0[2] = {1.0f - tx, tx}, w1[2] = {1.0f - ty, ty}, w2[2] = {1.0f - tz, tz};
     gx = gy = gz = 0.0f;
 #pragma unroll
@@ -343,6 +385,14 @@ __device__ __forceinline__ void force_at(const float* __restrict__ phi, int n, i
 #pragma unroll
         for (int b = 0; b < 2; ++b)
             gz += w0[a] * w1[b] * (w2[0] * St::D(s.Z[a][b], C0) + w2[1] * St::D(s.Z[a][b], C0 + 1));
+}
+
+template <int ORDER, bool POW2, bool XPLAIN = false>
+__device__ __forceinline__ void force_at(const float* __restrict__ phi, int n, int i, int j, int k,
+                                         float tx, float ty, float tz, float& gx, float& gy,
+                                         float& gz) {
+    const Stencil<ORDER, POW2, XPLAIN> s(phi, n, i, j, k);
+    force_from(s, tx, ty, tz, gx, gy, gz);
 }
 
 template <int ORDER, bool POW2>
@@ -401,6 +451,97 @@ __global__ void __launch_bounds__(256, 4) k_kick_drift_f32(const float* __restri
             i = li + x0;  // the drift below starts from the (clamped) cell
         } else {
             force_at<ORDER, POW2>(phi, n, i, j, k, tx, ty, tz, gx, gy, gz);
+        }
+        const float ux = __ldcs(vx + p) + gx * c_kick, uy = __ldcs(vy + p) + gy * c_kick,
+                    uz = __ldcs(vz + p) + gz * c_kick;
+        __stcs(vx + p, ux);
+        __stcs(vy + p, uy);
+        __stcs(vz + p, uz);
+        if (dt != 0.0) {
+            int a, b, c;
+            float qa, qb, qc;
+            split1((double)i + (double)tx + (double)ux * dt, n, a, qa);
+            split1((double)j + (double)ty + (double)uy * dt, n, b, qb);
+            split1((double)k + (double)tz + (double)uz * dt, n, c, qc);
+            __stcs(cell + p, pack_cell(a, b, c));
+            __stcs(ox + p, qa);
+            __stcs(oy + p, qb);
+            __stcs(oz + p, qc);
+        }
+    }
+}
+
+// ---------------------------------------- tiled gather + kick + drift
+// The particles in the bin order of the fused deposit (column tile of 4 x 4
+// cells, face class, z chunk of 64 cells): one block per super-tile of 2 x 2
+// column tiles and one z chunk.  It stages in shared memory the potential
+// its particles' stencils reach -- 2 cells below to 2 above the 8 x 8
+// columns in x and y (13 x 13 rows), 2 below to 2 above the chunk in z --
+// with coalesced loads, then gathers every stencil from there: the neighbour
+// particles' re-reads of the potential are served once per block instead of
+// once per particle from L1/L2.  Particles are read and written through the
+// bin permutation.
+constexpr int kGS = 8, kGW = kGS + 5;  // super-tile side in cells; staged rows per axis
+constexpr int kGZC = 64, kGZ = kGZC + 5;  // z chunk; staged z values per row
+constexpr int kGRL = 72;                  // padded row: z + z / 32 < 72
+constexpr size_t kGSmem = (size_t)kGW * kGW * kGRL * sizeof(float);
+
+template <int ORDER>
+__global__ void __launch_bounds__(256, 4)
+k_kick_drift_tiles(const float* __restrict__ phi, uint32_t* __restrict__ cell, float* __restrict__ ox,
+                   float* __restrict__ oy, float* __restrict__ oz, float* __restrict__ vx, float* __restrict__ vy,
+                   float* __restrict__ vz, const uint32_t* __restrict__ perm, const uint32_t* __restrict__ off, int n,
+                   int zcb, float c_kick, double dt) {
+    extern __shared__ __align__(16) float S[];
+    __shared__ uint32_t rbeg[16], rpre[17];
+    const int nt = n >> 2, nst = nt >> 1, nzc = 1 << zcb, m = n - 1;
+    const int zc = (int)(blockIdx.x & (nzc - 1)), st = (int)(blockIdx.x >> zcb);
+    const int sx = st / nst, sy = st - sx * nst;
+    const int X0 = sx * kGS, Y0 = sy * kGS, Z0 = zc * kGZC;
+    if (threadIdx.x < 16) {  // the 2 x 2 tiles x 4 classes of this chunk
+        const int a = threadIdx.x >> 3, b = (threadIdx.x >> 2) & 1, cls = threadIdx.x & 3;
+        const uint32_t tile = (uint32_t)(2 * sx + a) * nt + (uint32_t)(2 * sy + b);
+        const uint32_t key = ((tile * 4u + cls) << zcb) + (uint32_t)zc;
+        const uint32_t beg = __ldg(off + key);
+        rbeg[threadIdx.x] = beg;
+        rpre[threadIdx.x + 1] = __ldg(off + key + 1) - beg;
+    }
+    const unsigned pz = (unsigned)n + 2u, plane = (unsigned)n * pz;
+#pragma unroll 4
+    for (int e = threadIdx.x; e < kGW * kGW * kGZ; e += 256) {
+        const int row = e / kGZ, z = e - row * kGZ;
+        const int rx = row / kGW, ry = row - rx * kGW;
+        const unsigned gx = (unsigned)((X0 - 2 + rx) & m), gy = (unsigned)((Y0 - 2 + ry) & m);
+        const unsigned gz = (unsigned)((Z0 - 2 + z) & m);
+        S[row * kGRL + z + (z >> 5)] = __ldg(phi + gx * plane + gy * pz + gz);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        rpre[0] = 0;
+        for (int r = 0; r < 16; ++r) rpre[r + 1] += rpre[r];
+    }
+    __syncthreads();
+    const uint32_t total = rpre[16];
+    for (uint32_t t = threadIdx.x; t < total; t += 256) {
+        int r = 0;  // range of t: binary search over the 16 prefix sums
+#pragma unroll
+        for (int h = 8; h >= 1; h >>= 1)
+            if (t >= rpre[r + h]) r += h;
+        const uint32_t p = __ldg(perm + rbeg[r] + (t - rpre[r]));
+        int i, j, k;
+        unpack_cell(__ldcs(cell + p), i, j, k);
+        i &= m;
+        j &= m;
+        k &= m;
+        // local coordinates in the staged block (clamped: memory stays in
+        // bounds even for a cell word inconsistent with its bucket)
+        const int lx = min(max(i - X0 + 2, 2), kGS + 1), ly = min(max(j - Y0 + 2, 2), kGS + 1);
+        const int lz = min(max(k - Z0 + 2, 2), kGZC + 1);
+        const float tx = __ldcs(ox + p), ty = __ldcs(oy + p), tz = __ldcs(oz + p);
+        float gx, gy, gz;
+        {
+            const SmemStencil<ORDER, kGW, kGRL> sst(S, lx, ly, lz);
+            force_from(sst, tx, ty, tz, gx, gy, gz);
         }
         const float ux = __ldcs(vx + p) + gx * c_kick, uy = __ldcs(vy + p) + gy * c_kick,
                     uz = __ldcs(vz + p) + gz * c_kick;
@@ -702,6 +843,41 @@ int slab_kick_drift_f32(const Plan& p, int x0, int nx, const float* phi, uint32_
             k_kick_drift_f32<2, true, true><<<g, kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz, np, ck,
                                                                           dt, p.ng, nullptr, nullptr, 0, x0, nx,
                                                                           p.d_err);
+    }
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+bool tiled_gather_supported(int ng) { return ng >= 256 && ng <= 1024 && (ng & (ng - 1)) == 0; }
+
+int tiled_gather_zcb(int ng) {
+    int b = 0;
+    while ((kGZC << b) < ng) ++b;
+    return b;
+}
+
+// One-time kernel attribute (48.7 KB of dynamic shared memory), set on the
+// plan's device when an FP32 plan is created.
+int tiled_gather_prepare() {
+    PMB_CUDA_CHECK(cudaFuncSetAttribute(k_kick_drift_tiles<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGSmem));
+    PMB_CUDA_CHECK(cudaFuncSetAttribute(k_kick_drift_tiles<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGSmem));
+    return PM_OK;
+}
+
+int kick_drift_tiles_f32(const Plan& p, const float* phi, uint32_t* cell, float* ox, float* oy, float* oz, float* vx,
+                         float* vy, float* vz, int64_t np, double c_kick, double dt) {
+    if (np == 0) return PM_OK;
+    if (!tiled_gather_supported(p.ng)) return fail(PM_ERR_SIZE, "tiled gather needs a power-of-two ng in [256, 1024]");
+    const int zcb = tiled_gather_zcb(p.ng);
+    const unsigned blocks = (unsigned)((p.ng / kGS) * (p.ng / kGS)) << zcb;
+    {
+        Timed t(p, ST_KICK_DRIFT);
+        if (p.grad_order == 4)
+            k_kick_drift_tiles<4><<<blocks, 256, kGSmem, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz, p.tiles.perm,
+                                                                     p.tiles.off, p.ng, zcb, (float)c_kick, dt);
+        else
+            k_kick_drift_tiles<2><<<blocks, 256, kGSmem, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz, p.tiles.perm,
+                                                                     p.tiles.off, p.ng, zcb, (float)c_kick, dt);
     }
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;

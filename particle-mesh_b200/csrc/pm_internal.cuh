@@ -198,7 +198,15 @@ int tile_scratch_ensure(Plan& p, int64_t np, int nbox, long long min_nb = 0);
 bool zcol_supported(int ng);
 int deposit_zr2c_prepare(const Plan& p);
 int deposit_zr2c_f32(Plan& p, const uint32_t* cell, const float* ox, const float* oy, const float* oz, int64_t np,
-                     float mass, float* mesh);
+                     float mass, float* mesh, int zcb = 0);
+// Gather + kick + drift in the bin order of the last deposit_zr2c_f32 with
+// z-chunk bits zcb (chunks of 64 cells, power-of-two ng >= 256), the
+// potential staged per block in shared memory (particles.cu).
+bool tiled_gather_supported(int ng);
+int tiled_gather_zcb(int ng);
+int tiled_gather_prepare();
+int kick_drift_tiles_f32(const Plan& p, const float* phi, uint32_t* cell, float* ox, float* oy, float* oz, float* vx,
+                         float* vy, float* vz, int64_t np, double c_kick, double dt);
 int poisson_after_z_f32(const Plan& p, float* mesh, double c_poisson, int nbox = 1);
 int deposit_zr2c_f32_batch(Plan& p, const uint32_t* cell, const float* ox, const float* oy, const float* oz,
                            const long long* pbeg, const long long* pend, int nbox, int64_t np_total,

@@ -54,8 +54,10 @@ __device__ __forceinline__ uint32_t bucket_of(uint32_t c, int ts_log, int nt) {
 
 // Bucket of a particle for the column tiles of the fused deposit + z FFT:
 // CT x CT cells in (x, y) and the whole z extent; class bits x-face (1),
-// y-face (2).  ts_log = log2 CT, nt = tiles per axis.
-__device__ __forceinline__ uint32_t column_bucket_of(uint32_t c, int ts_log, int nt) {
+// y-face (2).  ts_log = log2 CT, nt = tiles per axis.  zcb > 0 splits every
+// (tile, class) bucket into 2^zcb z chunks, z chunk fastest, so that the
+// classes of a tile still form one contiguous run of buckets.
+__device__ __forceinline__ uint32_t column_bucket_of(uint32_t c, int ts_log, int nt, int zcb = 0) {
     int i, j, k;
     unpack(c, i, j, k);
     const int n = nt << ts_log;
@@ -63,7 +65,11 @@ __device__ __forceinline__ uint32_t column_bucket_of(uint32_t c, int ts_log, int
     if (j >= n) j %= n;
     const int m = (1 << ts_log) - 1;
     const uint32_t tile = (uint32_t)(i >> ts_log) * nt + (uint32_t)(j >> ts_log);
-    return tile * 4u + ((i & m) == m ? 1u : 0u) + ((j & m) == m ? 2u : 0u);
+    const uint32_t b = tile * 4u + ((i & m) == m ? 1u : 0u) + ((j & m) == m ? 2u : 0u);
+    if (zcb == 0) return b;
+    if (k >= n) k %= n;
+    const int zsh = __ffs(n) - 1 - zcb;  // log2 of the chunk length
+    return (b << zcb) + (uint32_t)(k >> zsh);
 }
 
 // Bucket of a particle for the column tiles of one x-slab (planes
@@ -118,9 +124,9 @@ __device__ __forceinline__ uint32_t morton_tile(uint32_t c, int ts_log, int nt) 
 constexpr int kBinU = 4;  // chunks of 32 particles per warp and round in the binning kernels
 
 // Bucket key of particle p (0xffffffff past the end; no bucket has that key).
-// KEY_SLABCOL reads (x0, nxl) from (ts_log, xa), nt the column tiles per
-// axis; KEY_RANK reads log2 of the slab width from ts_log and the mesh size
-// from nt.
+// KEY_COLUMN reads the z-chunk bits from xa; KEY_SLABCOL reads (x0, nxl)
+// from (ts_log, xa), nt the column tiles per axis; KEY_RANK reads log2 of
+// the slab width from ts_log and the mesh size from nt.
 template <int KEY>
 __device__ __forceinline__ uint32_t bin_key(const uint32_t* __restrict__ cell, long long p, long long hi, uint32_t kb,
                                             int ts_log, int nt, int xa = 0) {
@@ -129,7 +135,7 @@ __device__ __forceinline__ uint32_t bin_key(const uint32_t* __restrict__ cell, l
     if (KEY == KEY_SLABCOL) return kb + slab_column_bucket_of(c, nt, ts_log, xa);
     if (KEY == KEY_RANK) return kb + slab_rank_of(c, ts_log, nt);
     return kb + (KEY == KEY_MORTON ? morton_tile(c, ts_log, nt)
-                                   : (KEY == KEY_COLUMN ? column_bucket_of(c, ts_log, nt) : bucket_of(c, ts_log, nt)));
+                                   : (KEY == KEY_COLUMN ? column_bucket_of(c, ts_log, nt, xa) : bucket_of(c, ts_log, nt)));
 }
 
 template <int KEY>
@@ -414,7 +420,8 @@ __global__ void __launch_bounds__(zcol_threads<N>(), 3)
 k_deposit_zr2c(const uint32_t* __restrict__ cell, const float* __restrict__ ox, const float* __restrict__ oy,
                const float* __restrict__ oz, const uint32_t* __restrict__ perm, const uint32_t* __restrict__ off,
                float mass, float* __restrict__ mesh, const float2* __restrict__ tw, int nt, long long nb_box = 0,
-               long long mesh_stride = 0, const float* __restrict__ box_mass = nullptr, int ntx_own = 0) {
+               long long mesh_stride = 0, const float* __restrict__ box_mass = nullptr, int ntx_own = 0,
+               int zcb = 0) {
     // a batch of boxes: box blockIdx.y has its own buckets, mesh and mass
     if (box_mass) mass = __ldg(box_mass + blockIdx.y);
     off += blockIdx.y * nb_box;
@@ -435,10 +442,11 @@ k_deposit_zr2c(const uint32_t* __restrict__ cell, const float* __restrict__ ox, 
             rbeg[threadIdx.x] = 0;
             rpre[threadIdx.x + 1] = 0;
         } else {
+            // (with z chunks, a class range of the tile spans its chunks)
             const uint32_t b = (uint32_t)(sx * nt + sy) * 4u;
-            const uint32_t beg = __ldg(off + b + kColC0[threadIdx.x]);
+            const uint32_t beg = __ldg(off + ((b + kColC0[threadIdx.x]) << zcb));
             rbeg[threadIdx.x] = beg;
-            rpre[threadIdx.x + 1] = __ldg(off + b + kColC1[threadIdx.x]) - beg;
+            rpre[threadIdx.x + 1] = __ldg(off + ((b + kColC1[threadIdx.x]) << zcb)) - beg;
         }
     }
     __syncthreads();
@@ -534,17 +542,19 @@ int tile_log(int n) { return n >= 16 ? 4 : 3; }  // 16^3 tiles (8^3 for the 8^3 
 
 // Counting sort of the bucket keys into perm / off (scratch of the plan).
 template <int KEY>
-int bucket_sort(const Plan& p, const uint32_t* cell, int64_t np, int ts_log, int nt, long long nb, TileScratch& s) {
+int bucket_sort(const Plan& p, const uint32_t* cell, int64_t np, int ts_log, int nt, long long nb, TileScratch& s,
+                int xa = 0) {
     const long long nscan = (nb + kScanThreads * kScanItems - 1) / (kScanThreads * kScanItems);
     PMB_CUDA_CHECK(cudaMemsetAsync(s.count, 0, nb * sizeof(uint32_t), p.stream));
     const unsigned g = grid_for(p, np, 256);
     {
         Timed t(p, ST_BIN, np > 0 ? 5 : 3);  // count, three scan kernels, scatter
-        if (np > 0) k_bucket_count<KEY><<<g, 256, 0, p.stream>>>(cell, np, ts_log, nt, s.count);
+        if (np > 0) k_bucket_count<KEY><<<g, 256, 0, p.stream>>>(cell, np, ts_log, nt, s.count, nullptr, nullptr, 0, xa);
         k_scan_local<<<(unsigned)nscan, kScanThreads, 0, p.stream>>>(s.count, nb, s.off, s.bsum);
         k_scan_sums<<<1, kScanThreads, 0, p.stream>>>(s.bsum, (int)nscan, s.off + nb);
         k_scan_add<<<(unsigned)nscan, kScanThreads, 0, p.stream>>>(s.off, s.cursor, nb, s.bsum);
-        if (np > 0) k_bucket_scatter<KEY><<<g, 256, 0, p.stream>>>(cell, np, ts_log, nt, s.cursor, s.perm);
+        if (np > 0)
+            k_bucket_scatter<KEY><<<g, 256, 0, p.stream>>>(cell, np, ts_log, nt, s.cursor, s.perm, nullptr, nullptr, 0, xa);
     }
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;
@@ -683,33 +693,34 @@ int deposit_zr2c_prepare(const Plan& p) {
 template <int N>
 static void launch_zcol(const Plan& p, unsigned blocks, const uint32_t* cell, const float* ox, const float* oy,
                         const float* oz, float mass, float* mesh, const float2* tw, int nt, int nbox = 1,
-                        long long nb_box = 0, const float* box_mass = nullptr) {
+                        long long nb_box = 0, const float* box_mass = nullptr, int zcb = 0) {
     k_deposit_zr2c<N><<<dim3(blocks, nbox), zcol_threads<N>(), kCTRows * z_row_stride<N>() * sizeof(float2),
                         p.stream>>>(cell, ox, oy, oz, p.tiles.perm, p.tiles.off, mass, mesh, tw, nt, nb_box,
-                                    (long long)mesh_elems(N), box_mass);
+                                    (long long)mesh_elems(N), box_mass, 0, zcb);
 }
 
 // Deposit + z R2C in one pass over the mesh (FP32, power-of-two ng >= 32):
 // mesh receives the z-transformed density contrast, ready for the y pass.
+// zcb > 0 bins by (column tile, class, z chunk) for the tiled gather.
 int deposit_zr2c_f32(Plan& p, const uint32_t* cell, const float* ox, const float* oy, const float* oz, int64_t np,
-                     float mass, float* mesh) {
+                     float mass, float* mesh, int zcb) {
     const int nt = p.ng / kCT, cl = 2;  // log2 kCT
-    const long long nb = (long long)nt * nt * 4;
-    int rc = tile_scratch_ensure(p, np > 0 ? np : 1, 1);
+    const long long nb = ((long long)nt * nt * 4) << zcb;
+    int rc = tile_scratch_ensure(p, np > 0 ? np : 1, 1, nb);
     if (rc != PM_OK) return rc;
-    rc = bucket_sort<KEY_COLUMN>(p, cell, np, cl, nt, nb, p.tiles);
+    rc = bucket_sort<KEY_COLUMN>(p, cell, np, cl, nt, nb, p.tiles, zcb);
     if (rc != PM_OK) return rc;
     const float2* tw = static_cast<const float2*>(p.tw);
     {
         Timed t(p, ST_DEPOSIT);
         const unsigned blocks = (unsigned)(nt * nt);
         switch (p.ng) {
-            case 32: launch_zcol<32>(p, blocks, cell, ox, oy, oz, mass, mesh, tw, nt); break;
-            case 64: launch_zcol<64>(p, blocks, cell, ox, oy, oz, mass, mesh, tw, nt); break;
-            case 128: launch_zcol<128>(p, blocks, cell, ox, oy, oz, mass, mesh, tw, nt); break;
-            case 256: launch_zcol<256>(p, blocks, cell, ox, oy, oz, mass, mesh, tw, nt); break;
-            case 512: launch_zcol<512>(p, blocks, cell, ox, oy, oz, mass, mesh, tw, nt); break;
-            case 1024: launch_zcol<1024>(p, blocks, cell, ox, oy, oz, mass, mesh, tw, nt); break;
+            case 32: launch_zcol<32>(p, blocks, cell, ox, oy, oz, mass, mesh, tw, nt, 1, 0, nullptr, zcb); break;
+            case 64: launch_zcol<64>(p, blocks, cell, ox, oy, oz, mass, mesh, tw, nt, 1, 0, nullptr, zcb); break;
+            case 128: launch_zcol<128>(p, blocks, cell, ox, oy, oz, mass, mesh, tw, nt, 1, 0, nullptr, zcb); break;
+            case 256: launch_zcol<256>(p, blocks, cell, ox, oy, oz, mass, mesh, tw, nt, 1, 0, nullptr, zcb); break;
+            case 512: launch_zcol<512>(p, blocks, cell, ox, oy, oz, mass, mesh, tw, nt, 1, 0, nullptr, zcb); break;
+            case 1024: launch_zcol<1024>(p, blocks, cell, ox, oy, oz, mass, mesh, tw, nt, 1, 0, nullptr, zcb); break;
             default: return fail(PM_ERR_SIZE, "fused deposit needs a power-of-two ng >= 32");
         }
     }
