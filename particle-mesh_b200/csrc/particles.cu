@@ -486,16 +486,13 @@ constexpr int kGZC = 64, kGZ = kGZC + 5;  // z chunk; staged z values per row
 constexpr int kGRL = 72;                  // padded row: z + z / 32 < 72
 constexpr size_t kGSmem = (size_t)kGW * kGW * kGRL * sizeof(float);
 
-template <int ORDER>
-__global__ void __launch_bounds__(256, 4)
-k_kick_drift_tiles(const float* __restrict__ phi, uint32_t* __restrict__ cell, float* __restrict__ ox,
-                   float* __restrict__ oy, float* __restrict__ oz, float* __restrict__ vx, float* __restrict__ vy,
-                   float* __restrict__ vz, const uint32_t* __restrict__ perm, const uint32_t* __restrict__ off, int n,
-                   int zcb, float c_kick, double dt) {
-    extern __shared__ __align__(16) float S[];
-    __shared__ uint32_t rbeg[16], rpre[17];
-    const int nt = n >> 2, nst = nt >> 1, nzc = 1 << zcb, m = n - 1;
-    const int zc = (int)(blockIdx.x & (nzc - 1)), st = (int)(blockIdx.x >> zcb);
+// Stages work item `item` (super-tile, z chunk) into buffer S: the 13 x 13
+// rows by cp.async (one warp per row, every copy in flight, no wait here) and
+// the 16 bucket ranges of its particles (rbeg, rlen) by plain loads.
+__device__ __forceinline__ void tiles_stage(const float* __restrict__ phi, const uint32_t* __restrict__ off, int n,
+                                            int zcb, int item, float* S, uint32_t* rbeg, uint32_t* rlen) {
+    const int nt = n >> 2, nst = nt >> 1, m = n - 1;
+    const int zc = item & ((1 << zcb) - 1), st = item >> zcb;
     const int sx = st / nst, sy = st - sx * nst;
     const int X0 = sx * kGS, Y0 = sy * kGS, Z0 = zc * kGZC;
     if (threadIdx.x < 16) {  // the 2 x 2 tiles x 4 classes of this chunk
@@ -504,25 +501,39 @@ k_kick_drift_tiles(const float* __restrict__ phi, uint32_t* __restrict__ cell, f
         const uint32_t key = ((tile * 4u + cls) << zcb) + (uint32_t)zc;
         const uint32_t beg = __ldg(off + key);
         rbeg[threadIdx.x] = beg;
-        rpre[threadIdx.x + 1] = __ldg(off + key + 1) - beg;
+        rlen[threadIdx.x] = __ldg(off + key + 1) - beg;
     }
     const unsigned pz = (unsigned)n + 2u, plane = (unsigned)n * pz;
-#pragma unroll 4
-    for (int e = threadIdx.x; e < kGW * kGW * kGZ; e += 256) {
-        const int row = e / kGZ, z = e - row * kGZ;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(S);
+    for (int row = warp; row < kGW * kGW; row += 8) {
         const int rx = row / kGW, ry = row - rx * kGW;
-        const unsigned gx = (unsigned)((X0 - 2 + rx) & m), gy = (unsigned)((Y0 - 2 + ry) & m);
-        const unsigned gz = (unsigned)((Z0 - 2 + z) & m);
-        S[row * kGRL + z + (z >> 5)] = __ldg(phi + gx * plane + gy * pz + gz);
+        const float* g = phi + (unsigned)((X0 - 2 + rx) & m) * plane + (unsigned)((Y0 - 2 + ry) & m) * pz;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            const int z = lane + 32 * q;
+            if (z < kGZ) {
+                const uint32_t dst = sbase + (uint32_t)(row * kGRL + z + (z >> 5)) * 4u;
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst), "l"(g + ((Z0 - 2 + z) & m)));
+            }
+        }
     }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        rpre[0] = 0;
-        for (int r = 0; r < 16; ++r) rpre[r + 1] += rpre[r];
-    }
-    __syncthreads();
+}
+
+// Gathers, kicks and drifts the particles of a staged item.  rpre holds the
+// prefix sums of the 16 range lengths.
+template <int ORDER>
+__device__ __forceinline__ void tiles_compute(const float* S, const uint32_t* rbeg, const uint32_t* rpre, int n,
+                                              int zcb, int item, uint32_t* __restrict__ cell, float* __restrict__ ox,
+                                              float* __restrict__ oy, float* __restrict__ oz, float* __restrict__ vx,
+                                              float* __restrict__ vy, float* __restrict__ vz,
+                                              const uint32_t* __restrict__ perm, float c_kick, double dt) {
+    const int nst = n >> 3, m = n - 1;
+    const int zc = item & ((1 << zcb) - 1), st = item >> zcb;
+    const int sx = st / nst, sy = st - sx * nst;
+    const int X0 = sx * kGS, Y0 = sy * kGS, Z0 = zc * kGZC;
     const uint32_t total = rpre[16];
-    for (uint32_t t = threadIdx.x; t < total; t += 256) {
+    for (uint32_t t = threadIdx.x; t < total; t += blockDim.x) {
         int r = 0;  // range of t: binary search over the 16 prefix sums
 #pragma unroll
         for (int h = 8; h >= 1; h >>= 1)
@@ -560,6 +571,61 @@ k_kick_drift_tiles(const float* __restrict__ phi, uint32_t* __restrict__ cell, f
             __stcs(oz + p, qc);
         }
     }
+}
+
+__device__ __forceinline__ void tiles_prefix(uint32_t* rpre, const uint32_t* rlen) {
+    if (threadIdx.x == 0) {
+        uint32_t acc = 0;
+        rpre[0] = 0;
+        for (int r = 0; r < 16; ++r) rpre[r + 1] = (acc += rlen[r]);
+    }
+}
+
+// One block per item: stage, wait, compute.
+template <int ORDER>
+__global__ void __launch_bounds__(256, 4)
+k_kick_drift_tiles(const float* __restrict__ phi, uint32_t* __restrict__ cell, float* __restrict__ ox,
+                   float* __restrict__ oy, float* __restrict__ oz, float* __restrict__ vx, float* __restrict__ vy,
+                   float* __restrict__ vz, const uint32_t* __restrict__ perm, const uint32_t* __restrict__ off, int n,
+                   int zcb, float c_kick, double dt) {
+    extern __shared__ __align__(16) float S[];
+    __shared__ uint32_t rbeg[16], rlen[16], rpre[17];
+    tiles_stage(phi, off, n, zcb, (int)blockIdx.x, S, rbeg, rlen);
+    asm volatile("cp.async.commit_group;\n" ::);
+    asm volatile("cp.async.wait_group 0;\n" ::);
+    __syncthreads();
+    tiles_prefix(rpre, rlen);
+    __syncthreads();
+    tiles_compute<ORDER>(S, rbeg, rpre, n, zcb, (int)blockIdx.x, cell, ox, oy, oz, vx, vy, vz, perm, c_kick, dt);
+}
+
+// Persistent blocks (two per SM) looping over the items with two buffers:
+// the copies of item k + 1 are in flight while item k is computed.
+template <int ORDER>
+__global__ void __launch_bounds__(256, 2)
+k_kick_drift_tiles_pipe(const float* __restrict__ phi, uint32_t* __restrict__ cell, float* __restrict__ ox,
+                        float* __restrict__ oy, float* __restrict__ oz, float* __restrict__ vx, float* __restrict__ vy,
+                        float* __restrict__ vz, const uint32_t* __restrict__ perm, const uint32_t* __restrict__ off,
+                        int n, int zcb, float c_kick, double dt, int nitems) {
+    extern __shared__ __align__(16) float S[];
+    __shared__ uint32_t rbeg[2][16], rlen[2][16], rpre[17];
+    constexpr int BUF = kGW * kGW * kGRL;
+    int item = (int)blockIdx.x, b = 0;
+    if (item < nitems) tiles_stage(phi, off, n, zcb, item, S, rbeg[0], rlen[0]);
+    asm volatile("cp.async.commit_group;\n" ::);
+    for (; item < nitems; item += (int)gridDim.x, b ^= 1) {
+        const int next = item + (int)gridDim.x;
+        if (next < nitems) tiles_stage(phi, off, n, zcb, next, S + (b ^ 1) * BUF, rbeg[b ^ 1], rlen[b ^ 1]);
+        asm volatile("cp.async.commit_group;\n" ::);
+        asm volatile("cp.async.wait_group 1;\n" ::);  // this item's copies have landed
+        __syncthreads();
+        tiles_prefix(rpre, rlen[b]);
+        __syncthreads();
+        tiles_compute<ORDER>(S + b * BUF, rbeg[b], rpre, n, zcb, item, cell, ox, oy, oz, vx, vy, vz, perm, c_kick,
+                             dt);
+        __syncthreads();  // buffer b is staged again two items on
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::);
 }
 
 // ----------------------------------------------------- FP32 adjoints
@@ -856,28 +922,51 @@ int tiled_gather_zcb(int ng) {
     return b;
 }
 
-// One-time kernel attribute (48.7 KB of dynamic shared memory), set on the
-// plan's device when an FP32 plan is created.
+// One-time kernel attributes (48.7 KB of dynamic shared memory, twice that
+// for the pipelined blocks), set on the plan's device when an FP32 plan is
+// created.
 int tiled_gather_prepare() {
     PMB_CUDA_CHECK(cudaFuncSetAttribute(k_kick_drift_tiles<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGSmem));
     PMB_CUDA_CHECK(cudaFuncSetAttribute(k_kick_drift_tiles<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGSmem));
+    PMB_CUDA_CHECK(cudaFuncSetAttribute(k_kick_drift_tiles_pipe<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)(2 * kGSmem)));
+    PMB_CUDA_CHECK(cudaFuncSetAttribute(k_kick_drift_tiles_pipe<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)(2 * kGSmem)));
     return PM_OK;
 }
+
+#ifndef PMB_GATHER_PIPE
+#define PMB_GATHER_PIPE 0
+#endif
 
 int kick_drift_tiles_f32(const Plan& p, const float* phi, uint32_t* cell, float* ox, float* oy, float* oz, float* vx,
                          float* vy, float* vz, int64_t np, double c_kick, double dt) {
     if (np == 0) return PM_OK;
     if (!tiled_gather_supported(p.ng)) return fail(PM_ERR_SIZE, "tiled gather needs a power-of-two ng in [256, 1024]");
     const int zcb = tiled_gather_zcb(p.ng);
-    const unsigned blocks = (unsigned)((p.ng / kGS) * (p.ng / kGS)) << zcb;
+    const int items = ((p.ng / kGS) * (p.ng / kGS)) << zcb;
+    const float ck = (float)c_kick;
     {
         Timed t(p, ST_KICK_DRIFT);
-        if (p.grad_order == 4)
-            k_kick_drift_tiles<4><<<blocks, 256, kGSmem, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz, p.tiles.perm,
-                                                                     p.tiles.off, p.ng, zcb, (float)c_kick, dt);
-        else
-            k_kick_drift_tiles<2><<<blocks, 256, kGSmem, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz, p.tiles.perm,
-                                                                     p.tiles.off, p.ng, zcb, (float)c_kick, dt);
+        if (PMB_GATHER_PIPE) {
+            const unsigned g = (unsigned)(2 * p.num_sms);
+            if (p.grad_order == 4)
+                k_kick_drift_tiles_pipe<4><<<g, 256, 2 * kGSmem, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz,
+                                                                             p.tiles.perm, p.tiles.off, p.ng, zcb, ck,
+                                                                             dt, items);
+            else
+                k_kick_drift_tiles_pipe<2><<<g, 256, 2 * kGSmem, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz,
+                                                                             p.tiles.perm, p.tiles.off, p.ng, zcb, ck,
+                                                                             dt, items);
+        } else if (p.grad_order == 4) {
+            k_kick_drift_tiles<4><<<(unsigned)items, 256, kGSmem, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz,
+                                                                              p.tiles.perm, p.tiles.off, p.ng, zcb, ck,
+                                                                              dt);
+        } else {
+            k_kick_drift_tiles<2><<<(unsigned)items, 256, kGSmem, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz,
+                                                                              p.tiles.perm, p.tiles.off, p.ng, zcb, ck,
+                                                                              dt);
+        }
     }
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;
