@@ -104,6 +104,20 @@ int pm_plan_set_timing(pm_plan* plan, int on);
  * smaller alternative, see pm_ensemble_info).  PM_ERR_ARG otherwise. */
 int pm_plan_set_fft_shape(pm_plan* plan, int tile_cols, int radix1);
 int pm_plan_read_timing(pm_plan* plan, double* ms, int64_t* launches, int reset);
+/* Gather of pm_step_f32 (new; no counterpart in the reference):
+ *   PM_GATHER_CACHED  one thread per particle in the caller's order, the 56
+ *                     potential values of its stencil read through L1 (the
+ *                     default; fastest when neighbouring array entries are
+ *                     neighbouring particles, e.g. Lagrangian or sorted order)
+ *   PM_GATHER_TILED   particles in the deposit's bin order (4 x 4-cell column
+ *                     tile, face class, 64-cell z chunk), each block's stencil
+ *                     region staged in shared memory: its cost does not depend
+ *                     on the particle order (FP32 plans, power-of-two ng in
+ *                     [256, 1024]; PM_ERR_SIZE otherwise).
+ * Both give the same forces up to FP32 rounding. */
+#define PM_GATHER_CACHED 0
+#define PM_GATHER_TILED 1
+int pm_plan_set_gather(pm_plan* plan, int mode);
 /* Name of stage i ("mesh_init", "deposit", "fft_z_r2c", ...), "" if out of range. */
 const char* pm_stage_name(int stage);
 

@@ -14,6 +14,7 @@ LIB_PATH = os.path.join(HERE, "libpm_b200.so")
 PM_OK, PM_ERR_ARG, PM_ERR_SIZE, PM_ERR_CUDA, PM_ERR_NOMEM, PM_ERR_RANGE, PM_ERR_STATE = range(7)
 PM_FP64, PM_FP32 = 0, 1
 PM_GREEN_DISCRETE, PM_GREEN_SPECTRAL = 0, 1
+PM_GATHER_CACHED, PM_GATHER_TILED = 0, 1
 
 _STATUS = {PM_ERR_ARG: "PM_ERR_ARG", PM_ERR_SIZE: "PM_ERR_SIZE", PM_ERR_CUDA: "PM_ERR_CUDA",
            PM_ERR_NOMEM: "PM_ERR_NOMEM", PM_ERR_RANGE: "PM_ERR_RANGE", PM_ERR_STATE: "PM_ERR_STATE"}
@@ -53,6 +54,7 @@ SIGNATURES = {
     "pm_kick_drift_f32": [_V, _V, _V, _V, _V, _V, _V, _V, _V, _L, _D, _D],
     "pm_step_f32": [_V, _V, _V, _V, _V, _V, _V, _V, _L, _F, _D, _D, _D],
     "pm_plan_set_fft_shape": [_V, _I, _I],
+    "pm_plan_set_gather": [_V, _I],
     "pm_reduce_f32": [_V, _V, _V, _V, _V, _L, _D, _V],
     "pm_reduce_f64": [_V, _V, _V, _V, _V, _L, _D, _V],
     "pm_adjoint_deposit_f32": [_V, _V, _V, _V, _V, _L, _F, _V, _V, _V, _V],

@@ -297,6 +297,15 @@ int pm_plan_set_fft_shape(pm_plan* plan, int tile_cols, int radix1) {
     return PM_OK;
 }
 
+int pm_plan_set_gather(pm_plan* plan, int mode) {
+    if (!plan) return fail(PM_ERR_ARG, "plan is NULL");
+    if (mode != PM_GATHER_CACHED && mode != PM_GATHER_TILED) return fail(PM_ERR_ARG, "unknown gather mode");
+    if (mode == PM_GATHER_TILED && (plan->p.precision != PM_FP32 || !tiled_gather_supported(plan->p.ng)))
+        return fail(PM_ERR_SIZE, "the tiled gather needs an FP32 plan of a power-of-two ng in [256, 1024]");
+    plan->p.gather = mode;
+    return PM_OK;
+}
+
 int pm_plan_set_timing(pm_plan* plan, int on) {
     if (!plan) return fail(PM_ERR_ARG, "plan is NULL");
     plan->p.timers->on = on != 0;
@@ -569,7 +578,7 @@ int pm_step_f32(pm_plan* plan, uint32_t* cell, float* ox, float* oy, float* oz, 
     Plan& p = plan->p;
     PM_TRY(ensure_workspace(p, false));
     float* m = static_cast<float*>(p.mesh);
-    if (tiled_gather_supported(p.ng)) {
+    if (p.gather == PM_GATHER_TILED && tiled_gather_supported(p.ng)) {
         // binned by (column tile, class, z chunk): the deposit fused with the
         // z FFT pass, and the gather from potential tiles staged in shared
         // memory in the same bin order

@@ -599,35 +599,6 @@ k_kick_drift_tiles(const float* __restrict__ phi, uint32_t* __restrict__ cell, f
     tiles_compute<ORDER>(S, rbeg, rpre, n, zcb, (int)blockIdx.x, cell, ox, oy, oz, vx, vy, vz, perm, c_kick, dt);
 }
 
-// Persistent blocks (two per SM) looping over the items with two buffers:
-// the copies of item k + 1 are in flight while item k is computed.
-template <int ORDER>
-__global__ void __launch_bounds__(256, 2)
-k_kick_drift_tiles_pipe(const float* __restrict__ phi, uint32_t* __restrict__ cell, float* __restrict__ ox,
-                        float* __restrict__ oy, float* __restrict__ oz, float* __restrict__ vx, float* __restrict__ vy,
-                        float* __restrict__ vz, const uint32_t* __restrict__ perm, const uint32_t* __restrict__ off,
-                        int n, int zcb, float c_kick, double dt, int nitems) {
-    extern __shared__ __align__(16) float S[];
-    __shared__ uint32_t rbeg[2][16], rlen[2][16], rpre[17];
-    constexpr int BUF = kGW * kGW * kGRL;
-    int item = (int)blockIdx.x, b = 0;
-    if (item < nitems) tiles_stage(phi, off, n, zcb, item, S, rbeg[0], rlen[0]);
-    asm volatile("cp.async.commit_group;\n" ::);
-    for (; item < nitems; item += (int)gridDim.x, b ^= 1) {
-        const int next = item + (int)gridDim.x;
-        if (next < nitems) tiles_stage(phi, off, n, zcb, next, S + (b ^ 1) * BUF, rbeg[b ^ 1], rlen[b ^ 1]);
-        asm volatile("cp.async.commit_group;\n" ::);
-        asm volatile("cp.async.wait_group 1;\n" ::);  // this item's copies have landed
-        __syncthreads();
-        tiles_prefix(rpre, rlen[b]);
-        __syncthreads();
-        tiles_compute<ORDER>(S + b * BUF, rbeg[b], rpre, n, zcb, item, cell, ox, oy, oz, vx, vy, vz, perm, c_kick,
-                             dt);
-        __syncthreads();  // buffer b is staged again two items on
-    }
-    asm volatile("cp.async.wait_group 0;\n" ::);
-}
-
 // ----------------------------------------------------- FP32 adjoints
 // The FP32 split-position counterparts of csrc/adjoint.cu (same algebra; no
 // counterpart in the reference).  With U(c) = scale_d dbar(c) +
@@ -922,22 +893,13 @@ int tiled_gather_zcb(int ng) {
     return b;
 }
 
-// One-time kernel attributes (48.7 KB of dynamic shared memory, twice that
-// for the pipelined blocks), set on the plan's device when an FP32 plan is
-// created.
+// One-time kernel attribute (48.7 KB of dynamic shared memory), set on the
+// plan's device when an FP32 plan is created.
 int tiled_gather_prepare() {
     PMB_CUDA_CHECK(cudaFuncSetAttribute(k_kick_drift_tiles<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGSmem));
     PMB_CUDA_CHECK(cudaFuncSetAttribute(k_kick_drift_tiles<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGSmem));
-    PMB_CUDA_CHECK(cudaFuncSetAttribute(k_kick_drift_tiles_pipe<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)(2 * kGSmem)));
-    PMB_CUDA_CHECK(cudaFuncSetAttribute(k_kick_drift_tiles_pipe<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)(2 * kGSmem)));
     return PM_OK;
 }
-
-#ifndef PMB_GATHER_PIPE
-#define PMB_GATHER_PIPE 0
-#endif
 
 int kick_drift_tiles_f32(const Plan& p, const float* phi, uint32_t* cell, float* ox, float* oy, float* oz, float* vx,
                          float* vy, float* vz, int64_t np, double c_kick, double dt) {
@@ -948,17 +910,7 @@ int kick_drift_tiles_f32(const Plan& p, const float* phi, uint32_t* cell, float*
     const float ck = (float)c_kick;
     {
         Timed t(p, ST_KICK_DRIFT);
-        if (PMB_GATHER_PIPE) {
-            const unsigned g = (unsigned)(2 * p.num_sms);
-            if (p.grad_order == 4)
-                k_kick_drift_tiles_pipe<4><<<g, 256, 2 * kGSmem, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz,
-                                                                             p.tiles.perm, p.tiles.off, p.ng, zcb, ck,
-                                                                             dt, items);
-            else
-                k_kick_drift_tiles_pipe<2><<<g, 256, 2 * kGSmem, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz,
-                                                                             p.tiles.perm, p.tiles.off, p.ng, zcb, ck,
-                                                                             dt, items);
-        } else if (p.grad_order == 4) {
+        if (p.grad_order == 4) {
             k_kick_drift_tiles<4><<<(unsigned)items, 256, kGSmem, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz,
                                                                               p.tiles.perm, p.tiles.off, p.ng, zcb, ck,
                                                                               dt);

@@ -129,6 +129,7 @@ struct Plan {
     TileScratch tiles;
     int tk = 0;  // column-tile width of the strided FFT passes (0: default)
     int rv = 0;  // strided-pass radix split: 0 the default, 1 the alternative (autotuned)
+    int gather = PM_GATHER_CACHED;  // gather of pm_step_f32 (pm_plan_set_gather)
 };
 
 // Brackets one kernel launch with the plan's stage timer.

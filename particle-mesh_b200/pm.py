@@ -123,6 +123,15 @@ class Plan:
         """Column-tile width and first radix of the strided FFT passes (0: default)."""
         check(self.lib.pm_plan_set_fft_shape(self._h, int(tile_cols), int(radix1)))
 
+    def set_gather(self, mode: str = "cached"):
+        """Gather of step_split: "cached" (per particle through L1, the
+        default) or "tiled" (bin order, shared-memory tiles; independent of
+        the particle order)."""
+        modes = {"cached": L.PM_GATHER_CACHED, "tiled": L.PM_GATHER_TILED}
+        if mode not in modes:
+            raise PMError(L.PM_ERR_ARG, f"unknown gather mode {mode!r}")
+        check(self.lib.pm_plan_set_gather(self._h, modes[mode]))
+
     def set_timing(self, on: bool = True):
         check(self.lib.pm_plan_set_timing(self._h, 1 if on else 0))
 
