@@ -73,8 +73,12 @@ typedef struct pm_plan pm_plan;
 
 /* ------------------------------------------------------------ plans */
 
-/* Creates a plan for an ng^3 mesh.  ng must be a power of two in [8, 1024];
- * FP32 plans also take the mixed-radix sizes 48 and 96.  grad_order is 2 (the reference's 2-point centred difference,
+/* Creates a plan for an ng^3 mesh.  ng is a power of two in [8, 1024] or one
+ * of the mixed-radix sizes 2^a 3^b 5^c 24, 40, 48, 80, 96, 120, 160, 192,
+ * 240, 320, 384, 480, 640, 768, 960 (radix 8/5/4/3/2 passes, the radix set of
+ * FFTE, src/fft/ffte1/factor.f:19-43), in both precisions; PM_ERR_SIZE
+ * otherwise.  The fused FP32 deposit + z FFT and the x-slab decomposition
+ * need a power of two.  grad_order is 2 (the reference's 2-point centred difference,
  * src/utils/utils.cpp:115-137) or 4.  stream may be NULL (legacy default
  * stream).  Replaces the setup of src/core/main.cpp:30-81 and the FFT
  * constructor src/fft/fftw/fft.cpp:3-59 (plans, Green's table). */

@@ -58,8 +58,13 @@ def build(force: bool = False, ptxas_v: bool = False, verbose: bool = False) -> 
         cc = nvcc()
         objs = []
 
+        headers = [d for d in deps if not d.endswith(".cu")]
+
         def compile_one(src):
             obj = os.path.join(BUILD, os.path.basename(src)[:-3] + ".o")
+            # an object is rebuilt when its source, a header or this recipe is newer
+            if not (force or ptxas_v) and not _stale(obj, [src] + headers):
+                return obj, ""
             cmd = [cc, *NVCC_FLAGS, "-I", os.path.join(ROOT, "include"), "-c", src, "-o", obj]
             if ptxas_v:
                 cmd += ["-Xptxas", "-v"]

@@ -22,6 +22,9 @@ namespace pmb {
 
 namespace {
 
+// Neighbour index c in [-n, 2n) wrapped into [0, n) (any mesh size).
+__device__ __forceinline__ int wrp(int c, int n) { return c < 0 ? c + n : (c >= n ? c - n : c); }
+
 __device__ __forceinline__ double wrapped(double v, double n) {
     if (v >= 0.0 && v < n) return v;
     double m = v - n * floor(v / n);
@@ -35,7 +38,6 @@ __global__ void k_deposit3_f64(const double* __restrict__ x, const double* __res
                                const double* __restrict__ uy, const double* __restrict__ uz, long long np,
                                double* __restrict__ ox, double* __restrict__ oy, double* __restrict__ oz, int n) {
     const double dn = (double)n;
-    const int msk = n - 1;
     for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np;
          p += (long long)gridDim.x * blockDim.x) {
         const double xp = wrapped(x[p], dn), yp = wrapped(y[p], dn), zp = wrapped(z[p], dn);
@@ -51,7 +53,7 @@ __global__ void k_deposit3_f64(const double* __restrict__ x, const double* __res
             for (int b = 0; b < 2; ++b)
 #pragma unroll
                 for (int c = 0; c < 2; ++c) {
-                    const long long o = ((long long)((i0 + a) & msk) * n + ((j0 + b) & msk)) * n + ((k0 + c) & msk);
+                    const long long o = ((long long)wrp(i0 + a, n) * n + wrp(j0 + b, n)) * n + wrp(k0 + c, n);
                     const double w = wx[a] * wy[b] * wz[c];
 #pragma unroll
                     for (int d = 0; d < 3; ++d) atomicAdd(out[d] + o, w * u[d]);
@@ -65,11 +67,10 @@ __global__ void k_deposit3_f64(const double* __restrict__ x, const double* __res
 template <int ORDER>
 __global__ void k_neg_divergence_f64(const double* __restrict__ ux, const double* __restrict__ uy,
                                      const double* __restrict__ uz, double* __restrict__ phibar, int n) {
-    const int msk = n - 1, sh = __ffs(n) - 1;
     const long long pz = n + 2;
     for (long long row = blockIdx.x; row < (long long)n * n; row += gridDim.x) {
-        const int i = (int)(row >> sh), j = (int)(row & msk);
-        auto R = [&](const double* g, int a, int b) { return g + ((long long)(a & msk) * n + (b & msk)) * n; };
+        const int i = (int)(row / n), j = (int)(row % n);
+        auto R = [&](const double* g, int a, int b) { return g + ((long long)wrp(a, n) * n + wrp(b, n)) * n; };
         const double *xm1 = R(ux, i - 1, j), *xp1 = R(ux, i + 1, j), *xm2 = R(ux, i - 2, j), *xp2 = R(ux, i + 2, j);
         const double *ym1 = R(uy, i, j - 1), *yp1 = R(uy, i, j + 1), *ym2 = R(uy, i, j - 2), *yp2 = R(uy, i, j + 2);
         const double* zc = R(uz, i, j);
@@ -79,7 +80,7 @@ __global__ void k_neg_divergence_f64(const double* __restrict__ ux, const double
                 out[k] = 0.0;
                 continue;
             }
-            const int km1 = (k - 1) & msk, kp1 = (k + 1) & msk, km2 = (k - 2) & msk, kp2 = (k + 2) & msk;
+            const int km1 = wrp(k - 1, n), kp1 = wrp(k + 1, n), km2 = wrp(k - 2, n), kp2 = wrp(k + 2, n);
             double g;
             if (ORDER == 4)
                 g = (8.0 * (xm1[k] - xp1[k]) - (xm2[k] - xp2[k])) / 12.0 +
@@ -97,7 +98,6 @@ __global__ void k_neg_divergence_f64(const double* __restrict__ ux, const double
 __device__ __forceinline__ void grad_gather(const double* __restrict__ g, long long pz, int n, int i0, int j0,
                                             int k0, double tx, double ty, double tz, double& gx, double& gy,
                                             double& gz) {
-    const int msk = n - 1;
     const double wx[2] = {1.0 - tx, tx}, wy[2] = {1.0 - ty, ty}, wz[2] = {1.0 - tz, tz};
     const double dw[2] = {-1.0, 1.0};
     gx = gy = gz = 0.0;
@@ -107,7 +107,7 @@ __device__ __forceinline__ void grad_gather(const double* __restrict__ g, long l
         for (int b = 0; b < 2; ++b)
 #pragma unroll
             for (int c = 0; c < 2; ++c) {
-                const double v = __ldg(g + ((long long)((i0 + a) & msk) * n + ((j0 + b) & msk)) * pz + ((k0 + c) & msk));
+                const double v = __ldg(g + ((long long)wrp(i0 + a, n) * n + wrp(j0 + b, n)) * pz + wrp(k0 + c, n));
                 gx += dw[a] * wy[b] * wz[c] * v;
                 gy += wx[a] * dw[b] * wz[c] * v;
                 gz += wx[a] * wy[b] * dw[c] * v;

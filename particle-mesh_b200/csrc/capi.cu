@@ -198,16 +198,13 @@ const char* pm_last_error(void) { return g_last_error.c_str(); }
 
 }  // extern "C"
 
-// allow_fp64_any: internal FP64 plans (initial conditions) may use the mixed-radix
-// sizes, whose FP64 particle kernels do not exist.
-static int plan_create(int ng, int precision, int green_kind, int grad_order, void* stream, pm_plan** out,
-                       bool allow_fp64_any) {
+static int plan_create(int ng, int precision, int green_kind, int grad_order, void* stream, pm_plan** out) {
     if (!out) return fail(PM_ERR_ARG, "output pointer is NULL");
     *out = nullptr;
     if (!fft_size_supported(ng))
-        return fail(PM_ERR_SIZE, "ng must be a power of two in [8, 1024], or 48 or 96 (FP32)");
-    if (precision == PM_FP64 && (ng & (ng - 1)) != 0 && !allow_fp64_any)
-        return fail(PM_ERR_SIZE, "FP64 plans need a power-of-two ng");
+        return fail(PM_ERR_SIZE,
+                    "ng must be a power of two in [8, 1024] or one of the mixed-radix sizes 24, 40, 48, 80, 96, 120, "
+                    "160, 192, 240, 320, 384, 480, 640, 768, 960");
     if (precision != PM_FP64 && precision != PM_FP32) return fail(PM_ERR_ARG, "unknown precision");
     if (green_kind != PM_GREEN_DISCRETE && green_kind != PM_GREEN_SPECTRAL) return fail(PM_ERR_ARG, "unknown green_kind");
     if (grad_order != 2 && grad_order != 4) return fail(PM_ERR_ARG, "grad_order must be 2 or 4");
@@ -247,14 +244,14 @@ static int plan_create(int ng, int precision, int green_kind, int grad_order, vo
 
 namespace pmb {
 int plan_create_internal(int ng, int precision, int green_kind, int grad_order, void* stream, pm_plan** out) {
-    return plan_create(ng, precision, green_kind, grad_order, stream, out, false);
+    return plan_create(ng, precision, green_kind, grad_order, stream, out);
 }
 }  // namespace pmb
 
 extern "C" {
 
 int pm_plan_create(int ng, int precision, int green_kind, int grad_order, void* stream, pm_plan** out) {
-    return plan_create(ng, precision, green_kind, grad_order, stream, out, false);
+    return plan_create(ng, precision, green_kind, grad_order, stream, out);
 }
 
 int pm_plan_destroy(pm_plan* plan) {
@@ -688,12 +685,12 @@ int pm_reduce_f64(pm_plan* plan, const double* mesh, const double* vx, const dou
 int pm_ic_zeldovich(int ng, int nrow, double n_s, double rms_cells, uint64_t seed,
                     double vel_factor, double* x, double* y, double* z, double* vx, double* vy,
                     double* vz, void* stream) {
-    if (!fft_size_supported(nrow)) return fail(PM_ERR_SIZE, "nrow must be a power of two in [8, 1024], or 48 or 96");
+    if (!fft_size_supported(nrow)) return fail(PM_ERR_SIZE, "nrow must be a mesh size pm_plan_create takes");
     if (ng < 1) return fail(PM_ERR_ARG, "ng must be positive");
     if (!(rms_cells >= 0.0) || !std::isfinite(n_s)) return fail(PM_ERR_ARG, "bad spectrum parameters");
     PM_TRY(check_np(1, {x, y, z, vx, vy, vz}));
     pm_plan* plan = nullptr;
-    PM_TRY(plan_create(nrow, PM_FP64, PM_GREEN_DISCRETE, 2, stream, &plan, true));
+    PM_TRY(plan_create(nrow, PM_FP64, PM_GREEN_DISCRETE, 2, stream, &plan));
     const int rc = ic_zeldovich(plan->p, n_s, rms_cells, seed, vel_factor, ng, x, y, z, vx, vy, vz);
     pm_plan_destroy(plan);
     return rc;

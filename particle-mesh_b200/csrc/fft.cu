@@ -289,9 +289,14 @@ __global__ void k_green(typename Cx<T>::t* __restrict__ spec, int n, const typen
     }
 }
 
-// ---------------------------------------------- 48 and 96: generic passes
+// ------------------------------- mixed-radix sizes (2^a 3^b 5^c): generic passes
 template <int N> constexpr int g_z_rows() { return 256 / GRadix<N / 2>::NT; }
-constexpr int kGTK = 16;  // columns per block of the generic strided passes
+// Columns per block of the generic strided passes: the widest of 16, 8, 4, 2
+// whose two ping-pong line buffers fit 96 KB (two blocks per SM).
+template <typename T, int N> constexpr int gtk() {
+    constexpr size_t c = 2 * sizeof(T);
+    return 2 * (size_t)N * 16 * c <= 98304 ? 16 : (2 * (size_t)N * 8 * c <= 98304 ? 8 : (2 * (size_t)N * 4 * c <= 98304 ? 4 : 2));
+}
 
 template <typename T, int N>
 __global__ void __launch_bounds__(256) k_fftg_z_r2c(T* __restrict__ mesh, long long nrows,
@@ -379,14 +384,24 @@ k_fftg_strided(typename Cx<T>::t* __restrict__ data, long long es, long long os,
         for (int e = ty; e < N; e += NT) base[e * es] = r[ix(e)];
 }
 
-template <typename T, int N, int TK = kGTK> struct LaunchG {
+template <typename T, int N, int TK = gtk<T, N>()> struct LaunchG {
     using C = typename Cx<T>::t;
     static constexpr int H = N / 2 + 1;
     static constexpr bool kTransposedX = false;
     static void xgreen_yinv_transposed(const Plan&, T*, T*, double) {}
     static size_t smem_z() { return (size_t)g_z_rows<N>() * 2 * (N / 2 + 1) * sizeof(C); }
     static size_t smem_s() { return (size_t)2 * N * TK * sizeof(C); }
-    static int prepare() { return PM_OK; }
+    static int prepare() {
+        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fftg_z_r2c<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_z()));
+        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fftg_z_c2r<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_z()));
+        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fftg_strided<T, N, -1, false, TK>,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
+        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fftg_strided<T, N, +1, false, TK>,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
+        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fftg_strided<T, N, -1, true, TK>,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
+        return PM_OK;
+    }
     static void z(const Plan& p, T* mesh, bool forward, int nbox = 1) {
         const long long rows = (long long)nbox * N * N;
         const unsigned grid = (unsigned)((rows + g_z_rows<N>() - 1) / g_z_rows<N>());
@@ -545,25 +560,45 @@ template <typename T, int N, int TK = tk_cols<T, N>(), int RV = 0> struct Launch
         case 8: { constexpr int N_ = 8; __VA_ARGS__; } break;        \
         case 16: { constexpr int N_ = 16; __VA_ARGS__; } break;      \
         case 32: { constexpr int N_ = 32; __VA_ARGS__; } break;      \
+        case 24: { constexpr int N_ = 24; __VA_ARGS__; } break;      \
+        case 40: { constexpr int N_ = 40; __VA_ARGS__; } break;      \
         case 48: { constexpr int N_ = 48; __VA_ARGS__; } break;      \
         case 64: { constexpr int N_ = 64; __VA_ARGS__; } break;      \
+        case 80: { constexpr int N_ = 80; __VA_ARGS__; } break;      \
         case 96: { constexpr int N_ = 96; __VA_ARGS__; } break;      \
+        case 120: { constexpr int N_ = 120; __VA_ARGS__; } break;    \
         case 128: { constexpr int N_ = 128; __VA_ARGS__; } break;    \
+        case 160: { constexpr int N_ = 160; __VA_ARGS__; } break;    \
+        case 192: { constexpr int N_ = 192; __VA_ARGS__; } break;    \
+        case 240: { constexpr int N_ = 240; __VA_ARGS__; } break;    \
         case 256: { constexpr int N_ = 256; __VA_ARGS__; } break;    \
+        case 320: { constexpr int N_ = 320; __VA_ARGS__; } break;    \
+        case 384: { constexpr int N_ = 384; __VA_ARGS__; } break;    \
+        case 480: { constexpr int N_ = 480; __VA_ARGS__; } break;    \
         case 512: { constexpr int N_ = 512; __VA_ARGS__; } break;    \
+        case 640: { constexpr int N_ = 640; __VA_ARGS__; } break;    \
+        case 768: { constexpr int N_ = 768; __VA_ARGS__; } break;    \
+        case 960: { constexpr int N_ = 960; __VA_ARGS__; } break;    \
         case 1024: { constexpr int N_ = 1024; __VA_ARGS__; } break;  \
         default: return fail(PM_ERR_SIZE, "mesh size not supported"); \
     }
 
+// Powers of two 8..1024 and the mixed-radix sizes 2^a 3^b 5^c (multiples of
+// 8, so that the FP32 deposit's 8^3 or 16^3 tiles divide the mesh).
 bool fft_size_supported(int ng) {
-    return (ng >= 8 && ng <= 1024 && (ng & (ng - 1)) == 0) || ng == 48 || ng == 96;
+    if (ng >= 8 && ng <= 1024 && (ng & (ng - 1)) == 0) return true;
+    switch (ng) {
+        case 24: case 40: case 48: case 80: case 96: case 120: case 160: case 192: case 240: case 320: case 384:
+        case 480: case 640: case 768: case 960: return true;
+        default: return false;
+    }
 }
 
 // Launcher of a mesh size: the two-pass power-of-two kernels, or the
-// generic mixed-radix ones for 48 and 96.
+// generic mixed-radix ones for the 2^a 3^b 5^c sizes.
 template <typename T, int N, int TK = 0, int RV = 0>
 using LaunchFor = typename std::conditional<
-    (N & (N - 1)) == 0, Launch<T, N, TK == 0 ? tk_cols<T, N>() : TK, RV>, LaunchG<T, N, TK == 0 ? kGTK : TK>>::type;
+    (N & (N - 1)) == 0, Launch<T, N, TK == 0 ? tk_cols<T, N>() : TK, RV>, LaunchG<T, N, TK == 0 ? gtk<T, N>() : TK>>::type;
 
 // Column-tile widths the autotuner may pick for small FP32 meshes (ng <= 128);
 // Plan::tk == 0 keeps the default width.
@@ -578,7 +613,7 @@ bool radix_variant_supported(int ng, int precision, int rv) {
 }
 
 // First radix of the strided passes' two-pass split (0 for the mixed-radix
-// 48 / 96 schedules).
+// mixed-radix schedules).
 int strided_radix1(int ng, int rv) {
     switch (ng) {
         case 8: return Radix<8>::R1;

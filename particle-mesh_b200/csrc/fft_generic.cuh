@@ -1,10 +1,17 @@
-// Mixed-radix (3 x 2^k) FFT passes for the mesh sizes 48 and 96 of the
-// batched-ensemble configuration.  A plain multi-pass Stockham schedule
-// (the same autosort recurrence as fft_engine.cuh) over ping-pong shared
-// buffers, with the radix list fixed per length:
-//   24 = 3 x 8,  48 = 3 x 4 x 4,  96 = 3 x 4 x 8.
-// The radix-3 butterfly is the one of FFTE (src/fft/ffte1/kernel.f:33-52, FFT3A):
-// X0 = a + (b + c), X1,2 = a - (b + c)/2 -/+ sign i sqrt(3)/2 (b - c).
+// Mixed-radix FFT passes for mesh sizes 2^a 3^b 5^c that are not powers of
+// two (24 to 960, multiples of 8).  A plain multi-pass Stockham schedule (the
+// same autosort recurrence as fft_engine.cuh) over ping-pong shared buffers.
+// The line length is factored into radices 8, 5, 4, 3, 2 -- the radix set of
+// the reference's FFTE (src/fft/ffte1/factor.f:19-43, kernel.f FFT2..FFT8) --
+// with the 5s and 3s first, then as many 8s as fit, then one 4 or 2.
+// The radix-3 and radix-5 butterflies are the published DFT identities that
+// FFTE's FFT3A / FFT5A (src/fft/ffte1/kernel.f) also evaluate:
+//   radix 3: X0 = a + (b + c), X1,2 = a - (b + c)/2 -/+ sign i sqrt(3)/2 (b - c);
+//   radix 5: with t1 = x1 + x4, t2 = x2 + x3, t3 = x1 - x4, t4 = x2 - x3,
+//            X0 = x0 + t1 + t2,
+//            X1,4 = x0 + c1 t1 + c2 t2 +/- sign i (s1 t3 + s2 t4),
+//            X2,3 = x0 + c2 t1 + c1 t2 +/- sign i (s2 t3 - s1 t4),
+//            c1 = cos 2pi/5, c2 = cos 4pi/5, s1 = sin 2pi/5, s2 = sin 4pi/5.
 #pragma once
 
 #include "fft_engine.cuh"
@@ -23,6 +30,20 @@ __device__ __forceinline__ void dft_nat(C* v) {
         v[0] = cadd(v[0], s);
         v[1] = cadd(m, t);
         v[2] = csub(m, t);
+    } else if constexpr (R == 5) {
+        constexpr T c1 = (T)0.30901699437494742410, c2 = (T)-0.80901699437494742410;
+        constexpr T s1 = (T)0.95105651629515357212, s2 = (T)0.58778525229247312917;
+        const C t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]), t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
+        const C a1 = cmake<C>(v[0].x + c1 * t1.x + c2 * t2.x, v[0].y + c1 * t1.y + c2 * t2.y);
+        const C a2 = cmake<C>(v[0].x + c2 * t1.x + c1 * t2.x, v[0].y + c2 * t1.y + c1 * t2.y);
+        const C b1 = cmake<C>(s1 * t3.x + s2 * t4.x, s1 * t3.y + s2 * t4.y);
+        const C b2 = cmake<C>(s2 * t3.x - s1 * t4.x, s2 * t3.y - s1 * t4.y);
+        const C ib1 = cmake<C>(-(T)DIR * b1.y, (T)DIR * b1.x), ib2 = cmake<C>(-(T)DIR * b2.y, (T)DIR * b2.x);
+        v[0] = cadd(v[0], cadd(t1, t2));
+        v[1] = cadd(a1, ib1);
+        v[4] = csub(a1, ib1);
+        v[2] = cadd(a2, ib2);
+        v[3] = csub(a2, ib2);
     } else {
         dft<R, DIR>(v);
         C t[R];
@@ -33,18 +54,33 @@ __device__ __forceinline__ void dft_nat(C* v) {
     }
 }
 
-template <int L> struct GRadix;
-template <> struct GRadix<24> {
-    static constexpr int P = 2, NT = 8;
-    static __host__ __device__ constexpr int R(int p) { return p == 0 ? 3 : 8; }
-};
-template <> struct GRadix<48> {
-    static constexpr int P = 3, NT = 16;
-    static __host__ __device__ constexpr int R(int p) { return p == 0 ? 3 : 4; }
-};
-template <> struct GRadix<96> {
-    static constexpr int P = 3, NT = 32;
-    static __host__ __device__ constexpr int R(int p) { return p == 0 ? 3 : (p == 1 ? 4 : 8); }
+// Radix schedule of a line of L = 2^a 3^b 5^c: all 5s, all 3s, then 8s while
+// they fit the power of two, then one 4 or 2 for what is left.  NT threads
+// per line: a power of two, about the butterflies of the widest pass.
+namespace gr {
+constexpr int pow_of(int L, int f) { return L % f == 0 ? 1 + pow_of(L / f, f) : 0; }
+constexpr int radix_at(int L, int p) {
+    const int n5 = pow_of(L, 5), n3 = pow_of(L, 3), n2 = pow_of(L, 2);
+    if (p < n5) return 5;
+    if (p < n5 + n3) return 3;
+    const int q = p - n5 - n3, n8 = n2 / 3, rest = n2 % 3;
+    if (q < n8) return 8;
+    return rest == 2 ? 4 : (rest == 1 ? 2 : 0);
+}
+constexpr int passes(int L) {
+    const int n2 = pow_of(L, 2);
+    return pow_of(L, 5) + pow_of(L, 3) + n2 / 3 + (n2 % 3 != 0 ? 1 : 0);
+}
+constexpr int threads(int L) {
+    int t = 1;
+    while (t * 2 <= L / 5 && t < 32) t *= 2;
+    return t;
+}
+}  // namespace gr
+
+template <int L> struct GRadix {
+    static constexpr int P = gr::passes(L), NT = gr::threads(L);
+    static __host__ __device__ constexpr int R(int p) { return gr::radix_at(L, p); }
 };
 
 // One Stockham pass of radix R after Ns: in -> out, butterflies j = tj,
@@ -80,6 +116,8 @@ __device__ __forceinline__ C* gfft(C* a, C* b, int tj, const IX& ix, const C* __
     for (int p = 0; p < G::P; ++p) {
         const int R = G::R(p);
         if (R == 3) gpass<L, 3, DIR>(in, out, Ns, tj, G::NT, ix, tw, tws);
+        else if (R == 5) gpass<L, 5, DIR>(in, out, Ns, tj, G::NT, ix, tw, tws);
+        else if (R == 2) gpass<L, 2, DIR>(in, out, Ns, tj, G::NT, ix, tw, tws);
         else if (R == 4) gpass<L, 4, DIR>(in, out, Ns, tj, G::NT, ix, tw, tws);
         else if (R == 8) gpass<L, 8, DIR>(in, out, Ns, tj, G::NT, ix, tw, tws);
         __syncthreads();

@@ -58,24 +58,32 @@ __global__ void k_mesh_init(T* __restrict__ mesh, int n, T val) {
     }
 }
 
+// Neighbour index c in [-n, 2n) wrapped into [0, n): a mask for power-of-
+// two meshes, one conditional otherwise (the mixed-radix sizes).
+template <bool POW2>
+__device__ __forceinline__ int wrap_near(int c, int n) {
+    if (POW2) return c & (n - 1);
+    return c < 0 ? c + n : (c >= n ? c - n : c);
+}
+
 // ------------------------------------------------------------------- FP64
 
 // CIC deposit, one thread per particle, 8 FP64 atomics into the periodic
 // mesh.  Same weights and operation order as cic_deposit
 // (include/utils/utils_inline.h:25-49); cell = floor(x) as static_cast<int>
 // in deposit_particles (src/utils/utils.cpp:85-97) for x >= 0.
+template <bool POW2>
 __global__ void k_deposit_f64(const double* __restrict__ x, const double* __restrict__ y,
                               const double* __restrict__ z, long long np, double mass,
                               double* __restrict__ mesh, int n, int* err) {
     const double dn = (double)n;
     const long long pz = n + 2;
-    const int msk = n - 1;
     for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np;
          p += (long long)gridDim.x * blockDim.x) {
         const double xp = sanitize(x[p], dn, err), yp = sanitize(y[p], dn, err), zp = sanitize(z[p], dn, err);
         const double fx = floor(xp), fy = floor(yp), fz = floor(zp);
         const int i0 = (int)fx, j0 = (int)fy, k0 = (int)fz;
-        const int i1 = (i0 + 1) & msk, j1 = (j0 + 1) & msk, k1 = (k0 + 1) & msk;
+        const int i1 = wrap_near<POW2>(i0 + 1, n), j1 = wrap_near<POW2>(j0 + 1, n), k1 = wrap_near<POW2>(k0 + 1, n);
         const double tx = xp - fx, ty = yp - fy, tz = zp - fz;
         const double sx0 = 1.0 - tx, sy0 = 1.0 - ty, sz0 = 1.0 - tz;
         const double sxy00 = sx0 * sy0, sxy10 = tx * sy0, sxy01 = sx0 * ty, sxy11 = tx * ty;
@@ -97,21 +105,22 @@ __global__ void k_deposit_f64(const double* __restrict__ x, const double* __rest
 // (i, j), threads along k, so the ten neighbour rows are addressed once.
 //   order 2: (phi[i-1] - phi[i+1]) / 2          (src/utils/utils.cpp:130-135)
 //   order 4: (8 (phi[i-1] - phi[i+1]) - (phi[i-2] - phi[i+2])) / 12
-template <int ORDER>
+template <int ORDER, bool POW2>
 __global__ void k_gradient_f64(const double* __restrict__ phi, double* __restrict__ fx,
                                double* __restrict__ fy, double* __restrict__ fz, int n) {
-    const int msk = n - 1, sh = __ffs(n) - 1;
     const long long pz = n + 2;
     for (long long row = blockIdx.x; row < (long long)n * n; row += gridDim.x) {
-        const int i = (int)(row >> sh), j = (int)(row & msk);
-        auto R = [&](int a, int b) { return phi + ((long long)(a & msk) * n + (b & msk)) * pz; };
+        const int i = (int)(row / n), j = (int)(row % n);
+        auto R = [&](int a, int b) {
+            return phi + ((long long)wrap_near<POW2>(a, n) * n + wrap_near<POW2>(b, n)) * pz;
+        };
         const double *c0 = R(i, j), *xm1 = R(i - 1, j), *xp1 = R(i + 1, j), *ym1 = R(i, j - 1), *yp1 = R(i, j + 1);
         const double *xm2 = R(i - 2, j), *xp2 = R(i + 2, j), *ym2 = R(i, j - 2), *yp2 = R(i, j + 2);
         const long long o = row * n;
         for (int k = threadIdx.x; k < n; k += blockDim.x) {
-            const int km1 = (k - 1) & msk, kp1 = (k + 1) & msk;
+            const int km1 = wrap_near<POW2>(k - 1, n), kp1 = wrap_near<POW2>(k + 1, n);
             if (ORDER == 4) {
-                const int km2 = (k - 2) & msk, kp2 = (k + 2) & msk;
+                const int km2 = wrap_near<POW2>(k - 2, n), kp2 = wrap_near<POW2>(k + 2, n);
                 fx[o + k] = (8.0 * (__ldg(xm1 + k) - __ldg(xp1 + k)) - (__ldg(xm2 + k) - __ldg(xp2 + k))) / 12.0;
                 fy[o + k] = (8.0 * (__ldg(ym1 + k) - __ldg(yp1 + k)) - (__ldg(ym2 + k) - __ldg(yp2 + k))) / 12.0;
                 fz[o + k] = (8.0 * (__ldg(c0 + km1) - __ldg(c0 + kp1)) - (__ldg(c0 + km2) - __ldg(c0 + kp2))) / 12.0;
@@ -140,6 +149,7 @@ __device__ __forceinline__ double trilerp(const double* __restrict__ f, long lon
 }
 
 // p += c_kick * W^T f (update_particles, src/utils/utils.cpp:141-170).
+template <bool POW2>
 __global__ void k_interp_kick_f64(const double* __restrict__ x, const double* __restrict__ y,
                                   const double* __restrict__ z, const double* __restrict__ fx,
                                   const double* __restrict__ fy, const double* __restrict__ fz,
@@ -147,13 +157,12 @@ __global__ void k_interp_kick_f64(const double* __restrict__ x, const double* __
                                   double* __restrict__ pzv, long long np, double c_kick, int n,
                                   int* err) {
     const double dn = (double)n;
-    const int msk = n - 1;
     for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np;
          p += (long long)gridDim.x * blockDim.x) {
         const double xp = sanitize(x[p], dn, err), yp = sanitize(y[p], dn, err), zp = sanitize(z[p], dn, err);
         const double flx = floor(xp), fly = floor(yp), flz = floor(zp);
         const int i0 = (int)flx, j0 = (int)fly, k0 = (int)flz;
-        const int i1 = (i0 + 1) & msk, j1 = (j0 + 1) & msk, k1 = (k0 + 1) & msk;
+        const int i1 = wrap_near<POW2>(i0 + 1, n), j1 = wrap_near<POW2>(j0 + 1, n), k1 = wrap_near<POW2>(k0 + 1, n);
         const double tx = xp - flx, ty = yp - fly, tz = zp - flz;
         const long long b00 = ((long long)i0 * n + j0) * n, b10 = ((long long)i1 * n + j0) * n;
         const long long b01 = ((long long)i0 * n + j1) * n, b11 = ((long long)i1 * n + j1) * n;
@@ -236,13 +245,6 @@ __global__ void k_join(const uint32_t* __restrict__ cell, const float* __restric
 // of the three components share their cells: each of the 32 (2-point) or 56
 // (4-point) distinct values is loaded once, from 12 or 20 mesh rows whose
 // offsets fit in 32 bits (ng <= 1024).
-// Stencil neighbour i + d (|d| <= 3) wrapped into [0, n): a mask for
-// power-of-two meshes, one conditional otherwise.
-template <bool POW2>
-__device__ __forceinline__ int wrap_near(int c, int n) {
-    if (POW2) return c & (n - 1);
-    return c < 0 ? c + n : (c >= n ? c - n : c);
-}
 
 // The potential values the 2- or 4-point centred differences need at the 8
 // CIC corners (i+a, j+b, k+c), each loaded once: the core rows (i+a, j+b)
@@ -753,25 +755,33 @@ int deposit_f64(const Plan& p, const double* x, const double* y, const double* z
         Timed t(p, ST_MESH_INIT);
         k_mesh_init<double><<<grid_for(p, (long long)mesh_elems(p.ng) / 2, kThreads), kThreads, 0, p.stream>>>(mesh, p.ng, -1.0);
     }
+    const bool pow2 = (p.ng & (p.ng - 1)) == 0;
     if (np > 0) {
-            Timed t(p, ST_DEPOSIT);
-            k_deposit_f64<<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(x, y, z, np, mass, mesh, p.ng, p.d_err);
-        }
+        Timed t(p, ST_DEPOSIT);
+        const unsigned g = grid_for(p, np, kThreads);
+        if (pow2)
+            k_deposit_f64<true><<<g, kThreads, 0, p.stream>>>(x, y, z, np, mass, mesh, p.ng, p.d_err);
+        else
+            k_deposit_f64<false><<<g, kThreads, 0, p.stream>>>(x, y, z, np, mass, mesh, p.ng, p.d_err);
+    }
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;
 }
 
 int gradient_f64(const Plan& p, const double* phi, double* fx, double* fy, double* fz) {
-    if (p.grad_order == 4)
-        {
-            Timed t(p, ST_GRADIENT);
-            k_gradient_f64<4><<<grid_for(p, (long long)p.ng * p.ng, 1), kThreads, 0, p.stream>>>(phi, fx, fy, fz, p.ng);
-        }
-    else
-        {
-            Timed t(p, ST_GRADIENT);
-            k_gradient_f64<2><<<grid_for(p, (long long)p.ng * p.ng, 1), kThreads, 0, p.stream>>>(phi, fx, fy, fz, p.ng);
-        }
+    const bool pow2 = (p.ng & (p.ng - 1)) == 0;
+    const unsigned g = grid_for(p, (long long)p.ng * p.ng, 1);
+    {
+        Timed t(p, ST_GRADIENT);
+        if (p.grad_order == 4 && pow2)
+            k_gradient_f64<4, true><<<g, kThreads, 0, p.stream>>>(phi, fx, fy, fz, p.ng);
+        else if (p.grad_order == 4)
+            k_gradient_f64<4, false><<<g, kThreads, 0, p.stream>>>(phi, fx, fy, fz, p.ng);
+        else if (pow2)
+            k_gradient_f64<2, true><<<g, kThreads, 0, p.stream>>>(phi, fx, fy, fz, p.ng);
+        else
+            k_gradient_f64<2, false><<<g, kThreads, 0, p.stream>>>(phi, fx, fy, fz, p.ng);
+    }
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;
 }
@@ -782,8 +792,13 @@ int interp_kick_f64(const Plan& p, const double* x, const double* y, const doubl
     if (np == 0) return PM_OK;
     {
         Timed t(p, ST_INTERP_KICK);
-        k_interp_kick_f64<<<grid_for(p, np, kThreads), kThreads, 0, p.stream>>>(x, y, z, fx, fy, fz, px, py, pz, np,
-                                                                          c_kick, p.ng, p.d_err);
+        const unsigned g = grid_for(p, np, kThreads);
+        if ((p.ng & (p.ng - 1)) == 0)
+            k_interp_kick_f64<true><<<g, kThreads, 0, p.stream>>>(x, y, z, fx, fy, fz, px, py, pz, np, c_kick, p.ng,
+                                                                  p.d_err);
+        else
+            k_interp_kick_f64<false><<<g, kThreads, 0, p.stream>>>(x, y, z, fx, fy, fz, px, py, pz, np, c_kick, p.ng,
+                                                                   p.d_err);
     }
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;

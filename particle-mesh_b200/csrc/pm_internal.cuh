@@ -48,7 +48,8 @@ template <> __device__ __forceinline__ float2 cscale<float2>(float2 a, float s) 
 #endif
 
 // Periodic wrap of a cell index into [0, n) for any n (the FP32 path also
-// serves meshes of 48 and 96 cells); one compare each way in the common case.
+// serves mixed-radix meshes such as 48 or 80 cells); one compare each way in the
+// common case.
 __host__ __device__ __forceinline__ int wrap_cell(int c, int n) {
     if (c < 0) c += n;
     else if (c >= n) c -= n;

@@ -538,7 +538,9 @@ __global__ void k_gather7(const uint32_t* __restrict__ perm, long long np, const
     }
 }
 
-int tile_log(int n) { return n >= 16 ? 4 : 3; }  // 16^3 tiles (8^3 for the 8^3 mesh)
+// 16^3 tiles where 16 divides the mesh, else 8^3 (the 8^3 mesh and the
+// mixed-radix sizes 24, 40, 120).
+int tile_log(int n) { return n % 16 == 0 ? 4 : 3; }
 
 // Counting sort of the bucket keys into perm / off (scratch of the plan).
 template <int KEY>

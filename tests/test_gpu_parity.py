@@ -606,7 +606,7 @@ def test_errors_are_reported(pmpkg):
         pmpkg.Plan(12, "fp64")
     assert e.value.code == 2  # PM_ERR_SIZE
     with pytest.raises(pmpkg.PMError) as e:
-        pmpkg.Plan(48, "fp64")  # mixed-radix sizes are FP32 only
+        pmpkg.Plan(36, "fp64")  # 36 = 4 x 9: not a supported mixed-radix size
     assert e.value.code == 2
     p32 = pmpkg.Plan(16, "fp32")
     with pytest.raises(pmpkg.PMError):
