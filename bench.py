@@ -318,6 +318,16 @@ def ensemble_leg(pm, torch, args, world, rank, dev, stream, barrier, max_over_ra
     torch.cuda.synchronize()
     barrier()
     t_ens = max_over_ranks(e0.elapsed_time(e1)) / reps
+    # the same run launched eagerly (no graph): the launch overhead the graph removes
+    ec, eo, ev = ecell.clone(), [t.clone() for t in eoff], [t.clone() for t in evel]
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for s_ in range(esteps + 1):
+        ens.step(ec, eo, ev, cp, (0.5 if s_ in (0, esteps) else 1.0) * edt, edt if s_ < esteps else 0.0)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_eager = max_over_ranks(e0.elapsed_time(e1))
+    del ec, eo, ev
     info = ens.info()
     total = int(sum(n ** 3 for n in sizes))
     out = {"config": f"{nb_} boxes, mesh sizes drawn from {{32,48,64,96,128}}, particles = cells, "
@@ -325,6 +335,11 @@ def ensemble_leg(pm, torch, args, world, rank, dev, stream, barrier, max_over_ra
            "particles": total, "value": total * esteps / (t_ens / 1e3),
            "unit": UNIT, "ms_per_run": t_ens, "ms_per_step": t_ens / esteps,
            "boxes_per_rank": len(mine), "graph_nodes": info["graph_nodes"], "classes": info["classes"],
+           "eager_ms_per_run": t_eager,
+           "launch_overhead_removed_by_graph": {"ms_per_run": t_eager - t_ens,
+                                                "share_of_eager": (t_eager - t_ens) / t_eager,
+                                                "us_per_node": (t_eager - t_ens) * 1e3 / max(1, info["graph_nodes"])},
+           "tune_cache": "committed" if os.path.exists(TUNE_CACHE) else "autotuned at creation",
            "setup_s_incl_autotune": t_setup,
            "note": "one CUDA graph per run of 20 KDK steps (21 force evaluations); batched kernels per "
                    "mesh-size class, classes on parallel graph branches; boxes dealt to ranks"}

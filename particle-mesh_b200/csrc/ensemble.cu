@@ -115,61 +115,6 @@ void write_cache(const char* path, const TuneCache& m) {
     std::fclose(f);
 }
 
-// Times the class's batched Poisson solve for each column-tile width and
-// radix split of the strided passes and keeps the fastest pair.
-int autotune_class(EnsembleClass& c, TuneCache& cache, bool measure) {
-    Plan& p = c.plan->p;
-    const std::string key = gpu_name() + " " + std::to_string(c.ng) + " " + std::to_string(p.green_kind) + " " +
-                            std::to_string(p.grad_order);
-    auto it = cache.find(key);
-    if (it != cache.end() && tk_variant_supported(c.ng, PM_FP32, it->second.first) &&
-        radix_variant_supported(c.ng, PM_FP32, it->second.second)) {
-        p.tk = it->second.first;
-        p.rv = it->second.second;
-        return PM_OK;
-    }
-    if (!measure || c.ng > 128) return PM_OK;
-    const int nbox = (int)c.boxes.size();
-    PMB_CUDA_CHECK(cudaMemsetAsync(c.mesh, 0, mesh_elems(c.ng) * nbox * sizeof(float), p.stream));
-    cudaEvent_t a, b;
-    PMB_CUDA_CHECK(cudaEventCreate(&a));
-    PMB_CUDA_CHECK(cudaEventCreate(&b));
-    float best = 1e30f;
-    int best_tk = 0, best_rv = 0;
-    for (int rv : {0, 1}) {
-        if (!radix_variant_supported(c.ng, PM_FP32, rv)) continue;
-        for (int tk : {0, 8, 16, 32}) {
-            if (!tk_variant_supported(c.ng, PM_FP32, tk)) continue;
-            p.tk = tk;
-            p.rv = rv;
-            int rc = PM_OK;
-            for (int r = 0; r < 2 && rc == PM_OK; ++r) rc = poisson_fused<float>(p, c.mesh, 1.0, nbox);
-            cudaEventRecord(a, p.stream);
-            for (int r = 0; r < 5 && rc == PM_OK; ++r) rc = poisson_fused<float>(p, c.mesh, 1.0, nbox);
-            cudaEventRecord(b, p.stream);
-            if (rc != PM_OK) {
-                cudaEventDestroy(a);
-                cudaEventDestroy(b);
-                return rc;
-            }
-            cudaEventSynchronize(b);
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, a, b);
-            if (ms < best) {
-                best = ms;
-                best_tk = tk;
-                best_rv = rv;
-            }
-        }
-    }
-    cudaEventDestroy(a);
-    cudaEventDestroy(b);
-    p.tk = best_tk;
-    p.rv = best_rv;
-    cache[key] = {best_tk, best_rv};
-    return PM_OK;
-}
-
 int enqueue_step(pm_ensemble* e, EnsembleClass& c, uint32_t* cell, float* ox, float* oy, float* oz, float* vx,
                  float* vy, float* vz, double c_poisson, double c_kick, double dt) {
     Plan& p = c.plan->p;
@@ -200,6 +145,94 @@ int fork_join(pm_ensemble* e, F body) {
         PMB_CUDA_CHECK(cudaEventRecord(c.done, c.plan->p.stream));
         PMB_CUDA_CHECK(cudaStreamWaitEvent(e->stream, c.done, 0));
     }
+    return PM_OK;
+}
+
+std::string tune_key(const EnsembleClass& c) {
+    const Plan& p = c.plan->p;
+    return gpu_name() + " " + std::to_string(c.ng) + " " + std::to_string(p.green_kind) + " " +
+           std::to_string(p.grad_order);
+}
+
+// Median time of `reps` runs of every class's batched Poisson solve, the
+// classes on their own streams forked from and joined to the ensemble
+// stream -- concurrently, as the captured graph runs them.
+int time_solves(pm_ensemble* e, int reps, cudaEvent_t a, cudaEvent_t b, float* out) {
+    std::vector<float> ts;
+    for (int r = 0; r < reps; ++r) {
+        PMB_CUDA_CHECK(cudaEventRecord(a, e->stream));
+        const int rc = fork_join(e, [](EnsembleClass& c) {
+            return poisson_fused<float>(c.plan->p, c.mesh, 1.0, (int)c.boxes.size());
+        });
+        if (rc != PM_OK) return rc;
+        PMB_CUDA_CHECK(cudaEventRecord(b, e->stream));
+        PMB_CUDA_CHECK(cudaEventSynchronize(b));
+        float ms = 0.f;
+        PMB_CUDA_CHECK(cudaEventElapsedTime(&ms, a, b));
+        ts.push_back(ms);
+    }
+    std::nth_element(ts.begin(), ts.begin() + ts.size() / 2, ts.end());
+    *out = ts[ts.size() / 2];
+    return PM_OK;
+}
+
+// Shapes of the strided FFT passes (column-tile width x radix split) per
+// class.  Classes found in the cache take the cached shape; the others (FP32
+// power-of-two or mixed-radix ng <= 128) are tuned by coordinate descent: two
+// rounds over the classes, each trying every candidate of one class while the
+// others keep their current shape, scored by the median of 21 concurrent
+// solves of all classes.  The shape changes only the strided passes, so the
+// solve is the part of the step that differs between candidates.
+int tune_shapes(pm_ensemble* e, TuneCache& cache, bool measure) {
+    std::vector<EnsembleClass*> todo;
+    for (auto& c : e->classes) {
+        Plan& p = c.plan->p;
+        auto it = cache.find(tune_key(c));
+        if (it != cache.end() && tk_variant_supported(c.ng, PM_FP32, it->second.first) &&
+            radix_variant_supported(c.ng, PM_FP32, it->second.second)) {
+            p.tk = it->second.first;
+            p.rv = it->second.second;
+        } else if (c.ng <= 128) {
+            todo.push_back(&c);
+        }
+    }
+    if (!measure || todo.empty()) return PM_OK;
+    for (auto& c : e->classes)
+        PMB_CUDA_CHECK(cudaMemsetAsync(c.mesh, 0, mesh_elems(c.ng) * c.boxes.size() * sizeof(float), c.plan->p.stream));
+    cudaEvent_t a, b;
+    PMB_CUDA_CHECK(cudaEventCreate(&a));
+    PMB_CUDA_CHECK(cudaEventCreate(&b));
+    float t = 0.f;
+    int rc = time_solves(e, 3, a, b, &t);  // warm-up
+    for (int round = 0; round < 2 && rc == PM_OK; ++round) {
+        for (EnsembleClass* c : todo) {
+            Plan& p = c->plan->p;
+            int best_tk = p.tk, best_rv = p.rv;
+            float best = 0.f;
+            rc = time_solves(e, 21, a, b, &best);
+            for (int rv : {0, 1}) {
+                if (rc != PM_OK || !radix_variant_supported(c->ng, PM_FP32, rv)) continue;
+                for (int tk : {0, 8, 16, 32}) {
+                    if (rc != PM_OK || !tk_variant_supported(c->ng, PM_FP32, tk) || (tk == best_tk && rv == best_rv))
+                        continue;
+                    p.tk = tk;
+                    p.rv = rv;
+                    rc = time_solves(e, 21, a, b, &t);
+                    if (rc == PM_OK && t < best) {
+                        best = t;
+                        best_tk = tk;
+                        best_rv = rv;
+                    }
+                }
+            }
+            p.tk = best_tk;
+            p.rv = best_rv;
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (rc != PM_OK) return rc;
+    for (EnsembleClass* c : todo) cache[tune_key(*c)] = {c->plan->p.tk, c->plan->p.rv};
     return PM_OK;
 }
 
@@ -283,10 +316,7 @@ int pm_ensemble_create(int nbox, const int* ng, const int64_t* np, const float* 
     if (rc == PM_OK) {
         auto cache = read_cache(tune_cache);
         const size_t before = cache.size();
-        for (auto& c : e->classes) {
-            rc = autotune_class(c, cache, autotune != 0);
-            if (rc != PM_OK) break;
-        }
+        rc = tune_shapes(e, cache, autotune != 0);
         if (rc == PM_OK && cache.size() != before) write_cache(tune_cache, cache);
         if (rc == PM_OK && cudaDeviceSynchronize() != cudaSuccess) rc = fail(PM_ERR_CUDA, "autotune failed");
     }
