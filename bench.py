@@ -69,6 +69,8 @@ def parse():
     ap.add_argument("--skip-adjoint", action="store_true")
     ap.add_argument("--skip-accuracy", action="store_true")
     ap.add_argument("--ensemble-boxes", type=int, default=256)
+    ap.add_argument("--gather", default="cached", choices=["cached", "tiled"],
+                    help="gather of the FP32 step (pm_plan_set_gather)")
     ap.add_argument("--slab", action="store_true",
                     help="run the x-slab decomposition at N = 1 too (at N > 1 it is the default)")
     return ap.parse_args()
@@ -492,6 +494,8 @@ def ours(args):
 
     pos, vel = pm.zeldovich_ic(ng, nrow, N_S, RMS, rank_seed(rank), device=dev)
     p32 = pm.Plan(ng, "fp32", "spectral", 4, stream=stream, device=dev)
+    if args.gather != "cached":
+        p32.set_gather(args.gather)
     cell, off = p32.split(*pos)
     v32 = [a.float() for a in vel]
     torch.cuda.synchronize()
@@ -792,6 +796,7 @@ def ours(args):
                        "particles_per_gpu": np_, "mesh": ng, "l2": "inputs larger than L2 (mesh 4.3 GB)",
                        "particle_order": "Lagrangian (lattice) order as generated; the deposit re-bins every "
                                          "step",
+                       "gather": args.gather,
                        "parallelism": f"{world} independent boxes, one per GPU"},
             "stages": per_stage, "fp64_detail": fp64, "accuracy_detail": accuracy, "fp64_256": c2,
             "adjoint": adjoint, "ensemble": ensemble,

@@ -54,26 +54,31 @@ __device__ __forceinline__ void dft_nat(C* v) {
     }
 }
 
-// Radix schedule of a line of L = 2^a 3^b 5^c: all 5s, all 3s, then 8s while
-// they fit the power of two, then one 4 or 2 for what is left.  NT threads
-// per line: a power of two, about the butterflies of the widest pass.
+// Radix schedule of a line of L = 2^a 3^b 5^c: all 5s, all 3s, then the
+// power of two as 8s with one 4 for a remainder of 4, or two 4s for a
+// remainder of 2 (a lone 2 only for a = 1).  NT threads per line: a power of
+// two near a third of the line, at most 32.
 namespace gr {
 constexpr int pow_of(int L, int f) { return L % f == 0 ? 1 + pow_of(L / f, f) : 0; }
+constexpr int n8(int a) { return a % 3 == 1 && a >= 4 ? (a - 4) / 3 : a / 3; }
+constexpr int n4(int a) { return a % 3 == 2 ? 1 : (a % 3 == 1 && a >= 4 ? 2 : 0); }
+constexpr int n2(int a) { return a == 1 ? 1 : 0; }
 constexpr int radix_at(int L, int p) {
-    const int n5 = pow_of(L, 5), n3 = pow_of(L, 3), n2 = pow_of(L, 2);
-    if (p < n5) return 5;
-    if (p < n5 + n3) return 3;
-    const int q = p - n5 - n3, n8 = n2 / 3, rest = n2 % 3;
-    if (q < n8) return 8;
-    return rest == 2 ? 4 : (rest == 1 ? 2 : 0);
+    const int a = pow_of(L, 2), f5 = pow_of(L, 5), f3 = pow_of(L, 3);
+    if (p < f5) return 5;
+    if (p < f5 + f3) return 3;
+    const int q = p - f5 - f3;
+    if (q < n8(a)) return 8;
+    if (q < n8(a) + n4(a)) return 4;
+    return 2;
 }
 constexpr int passes(int L) {
-    const int n2 = pow_of(L, 2);
-    return pow_of(L, 5) + pow_of(L, 3) + n2 / 3 + (n2 % 3 != 0 ? 1 : 0);
+    const int a = pow_of(L, 2);
+    return pow_of(L, 5) + pow_of(L, 3) + n8(a) + n4(a) + n2(a);
 }
 constexpr int threads(int L) {
     int t = 1;
-    while (t * 2 <= L / 5 && t < 32) t *= 2;
+    while (t * 2 <= L / 3 && t < 32) t *= 2;
     return t;
 }
 }  // namespace gr
