@@ -314,9 +314,11 @@ int pm_deposit_f32_noalloc(int ng, const uint32_t* cell, const float* ox, const 
  * the step covers the whole class in one launch, classes run concurrently on
  * their own streams.  mass[b] is box b's particle mass (host array, copied).
  * autotune != 0 picks, at creation, the shape of the strided FFT passes
- * (column-tile width x radix split) of every class with ng <= 128: all
- * classes' solves run concurrently, as in the run's graph, and each candidate
- * is scored by the median of 21 such runs, class by class for two rounds;
+ * (column-tile width x radix split) of every class with ng <= 128: whole
+ * steps of all classes run concurrently, as in the run's graph, on a lattice
+ * of particles in temporary device arrays (28 bytes per particle, freed
+ * before the call returns), and each candidate is scored by the median of 21
+ * such steps, class by class for two rounds;
  * tune_cache (may be NULL) is a
  * text file of earlier choices, read first and rewritten when new ones were
  * measured.  stream NULL: the ensemble uses its own stream (pm_ensemble_sync

@@ -154,15 +154,41 @@ std::string tune_key(const EnsembleClass& c) {
            std::to_string(p.grad_order);
 }
 
-// Median time of `reps` runs of every class's batched Poisson solve, the
-// classes on their own streams forked from and joined to the ensemble
-// stream -- concurrently, as the captured graph runs them.
-int time_solves(pm_ensemble* e, int reps, cudaEvent_t a, cudaEvent_t b, float* out) {
+// A lattice of particles per box for the tuner: particle i of a box of ng^3
+// cells sits in cell (i / ng^2, i / ng, i) mod ng with a fixed in-cell offset
+// (a hash of i spread over [0.25, 0.75)), at rest.
+__global__ void k_tune_lattice(uint32_t* __restrict__ cell, float* __restrict__ ox, float* __restrict__ oy,
+                               float* __restrict__ oz, float* __restrict__ vx, float* __restrict__ vy,
+                               float* __restrict__ vz, const long long* __restrict__ pbeg,
+                               const long long* __restrict__ pend, int ng) {
+    const long long lo = pbeg[blockIdx.y], hi = pend[blockIdx.y];
+    for (long long p = lo + blockIdx.x * (long long)blockDim.x + threadIdx.x; p < hi;
+         p += (long long)gridDim.x * blockDim.x) {
+        const long long i = p - lo;
+        const uint32_t x = (uint32_t)((i / ((long long)ng * ng)) % ng), y = (uint32_t)((i / ng) % ng),
+                       z = (uint32_t)(i % ng);
+        cell[p] = (x << 20) | (y << 10) | z;
+        uint32_t h = (uint32_t)i * 2654435761u;
+        ox[p] = 0.25f + 0.5f * (float)((h >> 8) & 1023u) / 1024.0f;
+        h = h * 2654435761u + 12345u;
+        oy[p] = 0.25f + 0.5f * (float)((h >> 8) & 1023u) / 1024.0f;
+        h = h * 2654435761u + 12345u;
+        oz[p] = 0.25f + 0.5f * (float)((h >> 8) & 1023u) / 1024.0f;
+        vx[p] = vy[p] = vz[p] = 0.0f;
+    }
+}
+
+// Median time of `reps` whole steps of every class (deposit, Poisson solve,
+// gather + kick + drift on the tuner's lattice particles; c_kick = 0 and a
+// tiny dt, so every rep does the same work), the classes on their own
+// streams forked from and joined to the ensemble stream -- concurrently, as
+// the captured graph runs them.
+int time_steps(pm_ensemble* e, uint32_t* cell, float* f[6], int reps, cudaEvent_t a, cudaEvent_t b, float* out) {
     std::vector<float> ts;
     for (int r = 0; r < reps; ++r) {
         PMB_CUDA_CHECK(cudaEventRecord(a, e->stream));
-        const int rc = fork_join(e, [](EnsembleClass& c) {
-            return poisson_fused<float>(c.plan->p, c.mesh, 1.0, (int)c.boxes.size());
+        const int rc = fork_join(e, [&](EnsembleClass& c) {
+            return enqueue_step(e, c, cell, f[0], f[1], f[2], f[3], f[4], f[5], 1.0, 0.0, 1e-6);
         });
         if (rc != PM_OK) return rc;
         PMB_CUDA_CHECK(cudaEventRecord(b, e->stream));
@@ -180,9 +206,10 @@ int time_solves(pm_ensemble* e, int reps, cudaEvent_t a, cudaEvent_t b, float* o
 // class.  Classes found in the cache take the cached shape; the others (FP32
 // power-of-two or mixed-radix ng <= 128) are tuned by coordinate descent: two
 // rounds over the classes, each trying every candidate of one class while the
-// others keep their current shape, scored by the median of 21 concurrent
-// solves of all classes.  The shape changes only the strided passes, so the
-// solve is the part of the step that differs between candidates.
+// others keep their current shape, scored by the median of 21 concurrent whole
+// steps of all classes on a lattice of particles (temporary device arrays of
+// the ensemble's particle count, freed before returning).  The shape of one
+// class changes the time of the others: their kernels share the SMs.
 int tune_shapes(pm_ensemble* e, TuneCache& cache, bool measure) {
     std::vector<EnsembleClass*> todo;
     for (auto& c : e->classes) {
@@ -197,19 +224,34 @@ int tune_shapes(pm_ensemble* e, TuneCache& cache, bool measure) {
         }
     }
     if (!measure || todo.empty()) return PM_OK;
-    for (auto& c : e->classes)
-        PMB_CUDA_CHECK(cudaMemsetAsync(c.mesh, 0, mesh_elems(c.ng) * c.boxes.size() * sizeof(float), c.plan->p.stream));
-    cudaEvent_t a, b;
-    PMB_CUDA_CHECK(cudaEventCreate(&a));
-    PMB_CUDA_CHECK(cudaEventCreate(&b));
+    const int64_t np = e->np_total > 0 ? e->np_total : 1;
+    uint32_t* cell = nullptr;
+    float* fbuf = nullptr;
+    if (cudaMalloc(&cell, (size_t)np * 4) != cudaSuccess || cudaMalloc(&fbuf, (size_t)np * 24) != cudaSuccess) {
+        cudaGetLastError();
+        if (cell) cudaFree(cell);
+        return fail(PM_ERR_NOMEM, "autotune: temporary particle arrays");
+    }
+    float* f[6];
+    for (int a = 0; a < 6; ++a) f[a] = fbuf + (size_t)a * np;
+    int rc = PM_OK;
+    for (auto& c : e->classes) {
+        const Plan& p = c.plan->p;
+        k_tune_lattice<<<dim3(grid_for(p, (long long)c.ng * c.ng * c.ng, 256, 2), (unsigned)c.boxes.size()), 256, 0,
+                         p.stream>>>(cell, f[0], f[1], f[2], f[3], f[4], f[5], c.d_pbeg, c.d_pend, c.ng);
+        if (cudaGetLastError() != cudaSuccess) rc = fail(PM_ERR_CUDA, "autotune: lattice fill");
+    }
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (rc == PM_OK && (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess))
+        rc = fail(PM_ERR_CUDA, "autotune: events");
     float t = 0.f;
-    int rc = time_solves(e, 3, a, b, &t);  // warm-up
+    if (rc == PM_OK) rc = time_steps(e, cell, f, 3, a, b, &t);  // warm-up
     for (int round = 0; round < 2 && rc == PM_OK; ++round) {
         for (EnsembleClass* c : todo) {
             Plan& p = c->plan->p;
             int best_tk = p.tk, best_rv = p.rv;
             float best = 0.f;
-            rc = time_solves(e, 21, a, b, &best);
+            rc = time_steps(e, cell, f, 21, a, b, &best);
             for (int rv : {0, 1}) {
                 if (rc != PM_OK || !radix_variant_supported(c->ng, PM_FP32, rv)) continue;
                 for (int tk : {0, 8, 16, 32}) {
@@ -217,7 +259,7 @@ int tune_shapes(pm_ensemble* e, TuneCache& cache, bool measure) {
                         continue;
                     p.tk = tk;
                     p.rv = rv;
-                    rc = time_solves(e, 21, a, b, &t);
+                    rc = time_steps(e, cell, f, 21, a, b, &t);
                     if (rc == PM_OK && t < best) {
                         best = t;
                         best_tk = tk;
@@ -229,8 +271,11 @@ int tune_shapes(pm_ensemble* e, TuneCache& cache, bool measure) {
             p.rv = best_rv;
         }
     }
-    cudaEventDestroy(a);
-    cudaEventDestroy(b);
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    cudaDeviceSynchronize();
+    cudaFree(cell);
+    cudaFree(fbuf);
     if (rc != PM_OK) return rc;
     for (EnsembleClass* c : todo) cache[tune_key(*c)] = {c->plan->p.tk, c->plan->p.rv};
     return PM_OK;

@@ -140,3 +140,39 @@ def test_dealt_boxes_match_the_whole_ensemble(pmpkg):
         dv = max(float((a - b[idx]).abs().max()) for a, b in zip(v, wv))
         assert dv < 1e-4 * max(float(t.abs().max()) for t in wv), dv
         assert float((c != wc[idx]).float().mean()) < 1e-3
+
+
+@pytest.mark.parametrize("ng", [32, 64, 128])
+def test_every_shape_gives_the_same_run(pmpkg, tmp_path, ng):
+    """A 10-step KDK run of an ensemble under every strided-pass shape the
+    autotuner may pick (forced through the cache file) ends in the state the
+    default shape gives: velocities within 1e-4 of their scale, cells equal
+    but for rounding at a face."""
+    sizes = [ng, ng, ng]
+    cell, off, vel = boxes_state(pmpkg, sizes, [31, 32, 33])
+    cp, dt, steps = 4 * np.pi, 0.01, 10
+    gpu = None
+    ref = None
+    default_r1 = {32: 4, 64: 8, 128: 8}[ng]
+    for tk in (0, 8, 16, 32):
+        for rv, r1 in ((0, default_r1), (1, {32: 2, 64: 4, 128: 4}[ng])):
+            cache = tmp_path / f"c{tk}_{rv}.txt"
+            if gpu is None:
+                probe = pmpkg.Ensemble([ng], [ng ** 3], [1.0], autotune=True, tune_cache=str(tmp_path / "probe.txt"))
+                gpu = (tmp_path / "probe.txt").read_text().split()[0]
+                probe.close()
+            cache.write_text(f"{gpu} {ng} 1 4 {tk} {rv}\n")
+            ens = pmpkg.Ensemble(sizes, [n ** 3 for n in sizes], [1.0] * 3, autotune=False, tune_cache=str(cache))
+            got = {c["ng"]: (c["tile_cols"], c["radix1"]) for c in ens.info()["classes"]}
+            assert got == {ng: (tk, r1)}
+            c, o, v = cell.clone(), [t.clone() for t in off], [t.clone() for t in vel]
+            ens.run(c, o, v, cp, dt, steps)
+            torch.cuda.synchronize()
+            ens.close()
+            if ref is None:
+                ref = (c, v)
+                continue
+            scale = max(float(t.abs().max()) for t in ref[1])
+            dv = max(float((a - b).abs().max()) for a, b in zip(v, ref[1]))
+            assert dv < 1e-4 * scale, (tk, r1, dv / scale)
+            assert float((c != ref[0]).float().mean()) < 1e-3, (tk, r1)
