@@ -202,6 +202,41 @@ template <int R1, int R2> struct ZIdx {  // z passes, unit stride, pad 1 per R1
     static __device__ __forceinline__ int out1(int j, int k) { return j * (R1 + 1) + k; }
     static __device__ __forceinline__ int p2(int j, int r) { return j + r * (R1 + 1); }
 };
+// Post-processing of the z R2C from the registers of pass 2.  Thread tj of
+// a row (R1 threads per row, lanes tj of one aligned group of R1 in a warp)
+// holds Z[tj + R1 k] in X[k]; output m = tj + R1 k needs Z[M - m], which is
+// X[R2 - 1 - k] of lane R1 - tj (or, for tj = 0, its own X[(R2 - k) mod R2]),
+// fetched with one shuffle per element.  Writes the M + 1 spectrum entries
+//   X[m] = E + W_N^m O,  E = (Z[m] + conj Z[M-m]) / 2,  O = -i (Z[m] - conj Z[M-m]) / 2
+// (Z[M] taken as Z[0]); for fixed k the R1 lanes write consecutive entries.
+template <int R1, int R2, typename C>
+__device__ __forceinline__ void r2c_post(const C (&X)[R2], int tj, bool active, C* __restrict__ crow,
+                                         const C* __restrict__ tw) {
+    using T = decltype(C::x);
+    constexpr int M = R1 * R2;
+    const int partner = (R1 - tj) & (R1 - 1);
+#pragma unroll
+    for (int k = 0; k < R2; ++k) {
+        const C q = X[R2 - 1 - k];
+        C p;
+        p.x = __shfl_sync(0xffffffffu, q.x, partner, R1);
+        p.y = __shfl_sync(0xffffffffu, q.y, partner, R1);
+        const C zc = cconj(tj == 0 ? X[(R2 - k) & (R2 - 1)] : p);
+        const C zk = X[k];
+        const C e = cscale(cadd(zk, zc), (T)0.5);
+        const C d = csub(zk, zc);
+        const C o = cmake<C>((T)0.5 * d.y, (T)-0.5 * d.x);  // -i d / 2
+        const int m = tj + R1 * k;
+        if (active) crow[m] = cadd(e, cmul(twiddle<-1>(tw, m), o));
+    }
+    if (active && tj == 0) {  // m = M: Z[M] = Z[0], W_N^M = -1
+        const C zk = X[0], zc = cconj(X[0]);
+        const C e = cscale(cadd(zk, zc), (T)0.5);
+        const C d = csub(zk, zc);
+        crow[M] = cmake<C>(e.x - (T)0.5 * d.y, e.y + (T)0.5 * d.x);
+    }
+}
+
 // Complex entries per padded z row (M + 1 values of the half spectrum).
 template <int N> constexpr int z_row_stride() { return (N / 2 + 1) + (N / 2 + 1) / Radix<N / 2>::R1 + 1; }
 

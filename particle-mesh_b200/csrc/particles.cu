@@ -424,7 +424,7 @@ __global__ void __launch_bounds__(256, 4) k_interp_f32(const float* __restrict__
 // below and three above (buffer plane = x - x0 + 2); a particle outside the
 // slab is recorded in *err and clamped into it.
 template <int ORDER, bool POW2, bool SLAB = false>
-__global__ void __launch_bounds__(256, 4) k_kick_drift_f32(const float* __restrict__ phi, uint32_t* __restrict__ cell,
+__global__ void __launch_bounds__(256, SLAB ? 3 : 4) k_kick_drift_f32(const float* __restrict__ phi, uint32_t* __restrict__ cell,
                                  float* __restrict__ ox, float* __restrict__ oy, float* __restrict__ oz,
                                  float* __restrict__ vx, float* __restrict__ vy, float* __restrict__ vz,
                                  long long np, float c_kick, double dt, int n,
