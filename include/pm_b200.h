@@ -410,6 +410,79 @@ int pm_slab_migrate_unpack(pm_slab* slab, const uint32_t* packed, int64_t n, voi
                            int64_t at);
 int pm_slab_check(pm_slab* slab);
 
+/* ------------------------------------- pencil decomposition (FP32, new)
+ * The decomposition the reference's Makefile names (DECOMP_CHOICES "pencil",
+ * Makefile:1) but does not contain; it lifts the slab path's limit of one
+ * x plane block per rank.  px x py ranks, rank r = rx py + ry owning the
+ * pencil x in [rx nx, (rx + 1) nx), y in [ry ny, (ry + 1) ny), all z, with
+ * nx = ng / px, ny = ng / py, and the particles whose cell lies there.  ng a
+ * power of two in [32, 1024]; px, py powers of two with nx, ny >= 4.  The
+ * half spectrum's H = ng / 2 + 1 kz planes are split into py chunks
+ * [kb(c), kb(c + 1)), kb(c) = floor(c H / py), hc(c) = kb(c + 1) - kb(c); the
+ * ky axis into px chunks of nx.  A y group is the py ranks of one rx, an x
+ * group the px ranks of one ry.  Buffers (complex = 2 floats):
+ *   halo  [nx + 5][ny + 5][ng + 2] floats, row (x - x0 + 2, y - y0 + 2)
+ *   send, recv  xfer_floats floats each
+ * One step, on every rank in the same order:
+ *
+ *   pm_pencil_deposit_f32    CIC deposit into the halo buffer's own rows and
+ *                            the +1 ghost rows x = nx, y = ny
+ *   exchange A               ghost rows to the neighbours: the x ghost
+ *                            (buffer rows (nx + 2, 2 .. ny + 1)) to rank
+ *                            (rx + 1, ry), the y ghost ((2 .. nx + 1, ny + 2))
+ *                            to (rx, ry + 1), the corner (nx + 2, ny + 2) to
+ *                            (rx + 1, ry + 1); ng + 2 floats per row
+ *   pm_pencil_fold_f32       add the received x ghost, y ghost and corner
+ *   pm_pencil_forward_f32    z R2C; kz chunk c ([nx][ny][hc(c)]) packed into
+ *                            send at complex offset nx ny kb(c)
+ *   exchange B (y group)     chunk c to group member c, into recv block s
+ *                            (complex offset s nx ny hc(ry)) from member s
+ *   pm_pencil_yfwd_f32       y forward; ky chunk d ([nx][nx][hc(ry)]) packed
+ *                            into send block d
+ *   exchange C (x group)     block d to member d, into recv block s
+ *   pm_pencil_xgreen_f32     x forward, Green, x inverse; send = recv
+ *   exchange C again
+ *   pm_pencil_yinv_f32       y inverse; y block d ([nx][ny][hc(ry)]) into
+ *                            send block d (complex offset d nx ny hc(ry))
+ *   exchange B reversed      block d to member d, into recv at complex
+ *                            offset nx ny kb(s) from member s (hc(s) wide)
+ *   pm_pencil_backward_f32   z C2R: the potential in the own rows of halo
+ *   exchange D               potential halo: x rows first (own y rows),
+ *                            buffer x rows nx, nx + 1 to (rx + 1, ry)'s 0, 1
+ *                            and 2, 3, 4 to (rx - 1, ry)'s nx + 2 .. nx + 4;
+ *                            then y rows over all nx + 5 x rows likewise
+ *   pm_pencil_kick_drift_f32 gradient + gather + kick + drift
+ *   pm_pencil_migrate_sort / _pack / _unpack   as for the slabs, by owner
+ *                            rank rx py + ry
+ */
+typedef struct pm_pencil pm_pencil;
+int pm_pencil_create(int ng, int px, int py, int rank, int green_kind, int grad_order, void* stream,
+                     pm_pencil** pencil);
+int pm_pencil_destroy(pm_pencil* pencil);
+/* Geometry and device buffers; any output may be NULL. */
+int pm_pencil_info(const pm_pencil* pencil, int* nx, int* ny, int* x0, int* y0, void** halo, void** send,
+                   void** recv, size_t* xfer_floats, size_t* device_bytes);
+int pm_pencil_plan(pm_pencil* pencil, pm_plan** plan);
+int pm_pencil_deposit_f32(pm_pencil* pencil, const uint32_t* cell, const float* ox, const float* oy,
+                          const float* oz, int64_t np, float mass);
+/* xghost: ny rows, yghost: nx rows, corner: 1 row of ng + 2 floats each. */
+int pm_pencil_fold_f32(pm_pencil* pencil, const float* xghost, const float* yghost, const float* corner);
+int pm_pencil_forward_f32(pm_pencil* pencil);
+int pm_pencil_yfwd_f32(pm_pencil* pencil);
+int pm_pencil_xgreen_f32(pm_pencil* pencil, double c_poisson);
+int pm_pencil_yinv_f32(pm_pencil* pencil);
+int pm_pencil_backward_f32(pm_pencil* pencil);
+/* A particle whose cell is outside the pencil is clamped into it and
+ * reported by pm_pencil_check (PM_ERR_RANGE). */
+int pm_pencil_kick_drift_f32(pm_pencil* pencil, uint32_t* cell, float* ox, float* oy, float* oz, float* vx,
+                             float* vy, float* vz, int64_t np, double c_kick, double dt);
+/* counts: host array of px py; waits for the pencil's stream. */
+int pm_pencil_migrate_sort(pm_pencil* pencil, const uint32_t* cell, int64_t np, int64_t* counts);
+int pm_pencil_migrate_pack(pm_pencil* pencil, void* const* arrays, int narrays, int64_t np, uint32_t* packed);
+int pm_pencil_migrate_unpack(pm_pencil* pencil, const uint32_t* packed, int64_t n, void* const* arrays,
+                             int narrays, int64_t at);
+int pm_pencil_check(pm_pencil* pencil);
+
 /* ---------------------------------------------- initial conditions (new)
  * Zel'dovich particles on an nrow^3 lattice q = (i + 1/2) ng/nrow from a
  * Gaussian random field with P(k) ~ k^n_s, scaled to an rms 3D displacement

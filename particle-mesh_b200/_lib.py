@@ -82,6 +82,22 @@ SIGNATURES = {
     "pm_slab_migrate_pack": [_V, _V, _I, _L, _V],
     "pm_slab_migrate_unpack": [_V, _V, _L, _V, _I, _L],
     "pm_slab_check": [_V],
+    "pm_pencil_create": [_I, _I, _I, _I, _I, _I, _V, ctypes.POINTER(_V)],
+    "pm_pencil_destroy": [_V],
+    "pm_pencil_info": [_V, _V, _V, _V, _V, _V, _V, _V, _V, _V],
+    "pm_pencil_plan": [_V, ctypes.POINTER(_V)],
+    "pm_pencil_deposit_f32": [_V, _V, _V, _V, _V, _L, _F],
+    "pm_pencil_fold_f32": [_V, _V, _V, _V],
+    "pm_pencil_forward_f32": [_V],
+    "pm_pencil_yfwd_f32": [_V],
+    "pm_pencil_xgreen_f32": [_V, _D],
+    "pm_pencil_yinv_f32": [_V],
+    "pm_pencil_backward_f32": [_V],
+    "pm_pencil_kick_drift_f32": [_V, _V, _V, _V, _V, _V, _V, _V, _L, _D, _D],
+    "pm_pencil_migrate_sort": [_V, _V, _L, _V],
+    "pm_pencil_migrate_pack": [_V, _V, _I, _L, _V],
+    "pm_pencil_migrate_unpack": [_V, _V, _L, _V, _I, _L],
+    "pm_pencil_check": [_V],
 }
 
 _lib = None

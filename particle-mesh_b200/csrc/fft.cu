@@ -448,6 +448,8 @@ template <typename T, int N, int TK = tk_cols<T, N>(), int RV = 0> struct Launch
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_x_green<T, N, TK, RV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_x_green<T, N, TK, RV, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, +1, TK, RV, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
+        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, -1, TK, RV, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
+        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, +1, TK, RV, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_x_green<T, N, TK, RV, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         return PM_OK;
     }
@@ -478,6 +480,21 @@ template <typename T, int N, int TK = tk_cols<T, N>(), int RV = 0> struct Launch
                 d, H, (long long)N * H, 0, H, tw, d);
     }
     // x forward + Green + x inverse over `planes` ky planes [ky - ky0][kx][kz]
+    // lines of N complex at runtime element stride es: `planes` planes at
+    // stride os, ncols columns (consecutive) per plane; every plane < N
+    static void strided_rt(const Plan& p, T* data, long long es, long long os, int planes, int ncols, int dir,
+                           int stage) {
+        C* d = reinterpret_cast<C*>(data);
+        const dim3 grid((ncols + TK - 1) / TK, planes);
+        const C* tw = static_cast<const C*>(p.tw);
+        Timed t(p, stage);
+        if (dir < 0)
+            k_fft_strided<T, N, -1, TK, RV, -1><<<grid, strided_threads<N, TK, RV>(), smem_s(), p.stream>>>(
+                d, es, os, 0, ncols, tw, d);
+        else
+            k_fft_strided<T, N, +1, TK, RV, -1><<<grid, strided_threads<N, TK, RV>(), smem_s(), p.stream>>>(
+                d, es, os, 0, ncols, tw, d);
+    }
     static void xgreen_slab(const Plan& p, T* spec, double cg, int planes, int ky0) {
         C* d = reinterpret_cast<C*>(spec);
         const dim3 grid((H + TK - 1) / TK, planes);
@@ -766,6 +783,72 @@ int slab_fft_backward_f32(const Plan& p, float* own, int nx) {
         L_::y_planes(p, own, +1, nx);
         L_::z_rows(p, own, false, (long long)nx * N_);
     });
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+// ---------------------------------------------- pencil decomposition
+// The FFT passes of one pencil (x range nx, y range ny, all z) of a
+// power-of-two FP32 mesh, on the pencil's buffers between the transposes:
+//   y stage  [nx][ng][hc]  y lines (element stride hc), one kz chunk of hc
+//   x stage  [ng][yc][hc]  x lines (element stride yc hc), yc ky planes
+// and the Green multiply of the x stage at global (kx, ky0 + y, kz0 + kz).
+__global__ void k_green_pencil(float2* __restrict__ spec, int ng, int yc, int hc, int ky0, int kz0,
+                               const float2* __restrict__ tw, const float* __restrict__ g1d, double cg, int kind) {
+    const long long n = (long long)ng * yc * hc;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const int kz = (int)(e % hc);
+        const long long t = e / hc;
+        const int ky = (int)(t % yc), kx = (int)(t / yc);
+        spec[e] = cscale(spec[e], green_value<float>(kx, ky0 + ky, kz0 + kz, kind, cg, tw, g1d));
+    }
+}
+
+// dst block [a][b][c] (strides da, db, 1) <- src block (strides sa, sb, 1),
+// complex elements; one thread per element of the c axis, coalesced.
+__global__ void k_copy3(const float2* __restrict__ src, long long sa, long long sb, float2* __restrict__ dst,
+                        long long da, long long db, int A, int B, int Cn) {
+    const long long rows = (long long)A * B;
+    for (long long r = blockIdx.y; r < rows; r += gridDim.y) {
+        const long long a = r / B, b = r % B;
+        const float2* s = src + a * sa + b * sb;
+        float2* d = dst + a * da + b * db;
+        for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < Cn; c += gridDim.x * blockDim.x) d[c] = s[c];
+    }
+}
+
+int pencil_copy3(const Plan& p, const float2* src, long long sa, long long sb, float2* dst, long long da,
+                 long long db, int A, int B, int C) {
+    if ((long long)A * B * C == 0) return PM_OK;
+    const unsigned gx = (unsigned)((C + 255) / 256);
+    const long long rows = (long long)A * B;
+    const unsigned gy = (unsigned)(rows < 65535 ? rows : 65535);
+    k_copy3<<<dim3(gx, gy), 256, 0, p.stream>>>(src, sa, sb, dst, da, db, A, B, C);
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+int pencil_fft_lines_f32(const Plan& p, float* data, long long es, long long os, int planes, int ncols, int dir,
+                         int stage) {
+    PMB_SLAB_LAUNCH(p, L_::strided_rt(p, data, es, os, planes, ncols, dir, stage));
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+int pencil_green_f32(const Plan& p, float* spec, int yc, int hc, int ky0, int kz0, double c_poisson) {
+    const long long n = (long long)p.ng * yc * hc;
+    {
+        Timed t(p, ST_GREEN);
+        k_green_pencil<<<grid_for(p, n, 256, 8), 256, 0, p.stream>>>(
+            reinterpret_cast<float2*>(spec), p.ng, yc, hc, ky0, kz0, static_cast<const float2*>(p.tw),
+            static_cast<const float*>(p.g1d), green_scale(p, c_poisson), p.green_kind);
+    }
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+int pencil_z_f32(const Plan& p, float* rows, long long nrows, bool forward) {
+    PMB_SLAB_LAUNCH(p, L_::z_rows(p, rows, forward, nrows));
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;
 }

@@ -251,18 +251,20 @@ __global__ void k_join(const uint32_t* __restrict__ cell, const float* __restric
 // over the whole z stencil, and the x and y stencil rows at columns k, k+1.
 // XPLAIN: the x planes are not periodic -- phi is one slab of a decomposed
 // mesh with its halo planes, and i already indexes the buffer's planes.
-template <int ORDER, bool POW2, bool XPLAIN = false> struct Stencil {
+// YPLAIN likewise for y: phi is one pencil with its halo rows, `yrows` rows
+// per x plane, and j indexes the buffer's rows.
+template <int ORDER, bool POW2, bool XPLAIN = false, bool YPLAIN = false> struct Stencil {
     static constexpr int LO = ORDER == 4 ? -2 : -1, W = ORDER == 4 ? 6 : 4;  // offsets LO..LO+W-1
     static constexpr int C0 = -LO;                                            // slot of offset 0
     float Z[2][2][W], X[W][2][2], Y[2][W][2];
 
-    __device__ __forceinline__ Stencil(const float* __restrict__ phi, int n, int i, int j, int k) {
-        const unsigned pz = (unsigned)n + 2u, plane = (unsigned)n * pz;
+    __device__ __forceinline__ Stencil(const float* __restrict__ phi, int n, int i, int j, int k, int yrows = 0) {
+        const unsigned pz = (unsigned)n + 2u, plane = (unsigned)(YPLAIN ? yrows : n) * pz;
         unsigned xo[W], yo[W], kc[W];
 #pragma unroll
         for (int d = 0; d < W; ++d) {
             xo[d] = (unsigned)(XPLAIN ? i + LO + d : wrap_near<POW2>(i + LO + d, n)) * plane;
-            yo[d] = (unsigned)wrap_near<POW2>(j + LO + d, n) * pz;
+            yo[d] = (unsigned)(YPLAIN ? j + LO + d : wrap_near<POW2>(j + LO + d, n)) * pz;
             kc[d] = (unsigned)wrap_near<POW2>(k + LO + d, n);
         }
 #pragma unroll
@@ -601,6 +603,100 @@ k_kick_drift_tiles(const float* __restrict__ phi, uint32_t* __restrict__ cell, f
     tiles_compute<ORDER>(S, rbeg, rpre, n, zcb, (int)blockIdx.x, cell, ox, oy, oz, vx, vy, vz, perm, c_kick, dt);
 }
 
+// ------------------------------------------------ pencil decomposition
+// One pencil (x in [x0, x0 + nx), y in [y0, y0 + ny), all z) with its halo
+// rows: buffer [nx + 5][ny + 5][n + 2], row (x - x0 + 2, y - y0 + 2).
+// Every row to 0, the own rows' cells to -1 (the density contrast's
+// background); padding 0.
+__global__ void k_pencil_init(float* __restrict__ buf, int nx, int ny, int n) {
+    const long long pz = n + 2, rows = (long long)(nx + 5) * (ny + 5);
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < rows * pz;
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long r = e / pz;
+        const int z = (int)(e - r * pz), xl = (int)(r / (ny + 5)), yl = (int)(r % (ny + 5));
+        const bool own = xl >= 2 && xl < nx + 2 && yl >= 2 && yl < ny + 2;
+        buf[e] = (own && z < n) ? -1.0f : 0.0f;
+    }
+}
+
+// CIC deposit of the pencil's particles into its buffer with shared-nothing
+// FP32 atomics: the +1 corners of the last x plane / y row land in the ghost
+// rows x = nx (buffer row nx + 2) and y = ny, which the neighbours fold.  A
+// cell outside the pencil is recorded in *err and clamped into it.
+__global__ void k_pencil_deposit(const uint32_t* __restrict__ cell, const float* __restrict__ ox,
+                                 const float* __restrict__ oy, const float* __restrict__ oz, long long np, float mass,
+                                 float* __restrict__ buf, int x0, int y0, int nx, int ny, int n, int* err) {
+    const long long pz = n + 2, yr = ny + 5;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np;
+         p += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        unpack_cell(__ldg(cell + p), i, j, k);
+        int li = (i & (n - 1)) - x0, lj = (j & (n - 1)) - y0;
+        k &= n - 1;
+        if (li < 0 || li >= nx || lj < 0 || lj >= ny) {
+            atomicOr(err, ERRBIT_RANGE);
+            li = min(max(li, 0), nx - 1);
+            lj = min(max(lj, 0), ny - 1);
+        }
+        const float fx = __ldg(ox + p), fy = __ldg(oy + p), fz = __ldg(oz + p);
+        const float wx[2] = {1.0f - fx, fx}, wy[2] = {1.0f - fy, fy}, wz[2] = {mass * (1.0f - fz), mass * fz};
+        const int kk[2] = {k, (k + 1) & (n - 1)};
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+            for (int b = 0; b < 2; ++b) {
+                float* row = buf + ((long long)(li + 2 + a) * yr + (lj + 2 + b)) * pz;
+                const float w = wx[a] * wy[b];
+#pragma unroll
+                for (int c = 0; c < 2; ++c) atomicAdd(row + kk[c], w * wz[c]);
+            }
+    }
+}
+
+// Gather + kick + drift of the pencil's particles from its buffer (potential
+// with two halo planes / rows below and three above in x and y).
+template <int ORDER>
+__global__ void __launch_bounds__(256, 3)
+k_pencil_kick_drift(const float* __restrict__ buf, uint32_t* __restrict__ cell, float* __restrict__ ox,
+                    float* __restrict__ oy, float* __restrict__ oz, float* __restrict__ vx, float* __restrict__ vy,
+                    float* __restrict__ vz, long long np, float c_kick, double dt, int n, int x0, int y0, int nx,
+                    int ny, int* err) {
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np;
+         p += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        unpack_cell(__ldcs(cell + p), i, j, k);
+        int li = (i & (n - 1)) - x0, lj = (j & (n - 1)) - y0;
+        k &= n - 1;
+        if (li < 0 || li >= nx || lj < 0 || lj >= ny) {
+            atomicOr(err, ERRBIT_RANGE);
+            li = min(max(li, 0), nx - 1);
+            lj = min(max(lj, 0), ny - 1);
+        }
+        const float tx = __ldcs(ox + p), ty = __ldcs(oy + p), tz = __ldcs(oz + p);
+        float gx, gy, gz;
+        {
+            const Stencil<ORDER, true, true, true> st(buf, n, li + 2, lj + 2, k, ny + 5);
+            force_from(st, tx, ty, tz, gx, gy, gz);
+        }
+        const float ux = __ldcs(vx + p) + gx * c_kick, uy = __ldcs(vy + p) + gy * c_kick,
+                    uz = __ldcs(vz + p) + gz * c_kick;
+        __stcs(vx + p, ux);
+        __stcs(vy + p, uy);
+        __stcs(vz + p, uz);
+        if (dt != 0.0) {
+            int a, b, c;
+            float qa, qb, qc;
+            split1((double)(li + x0) + (double)tx + (double)ux * dt, n, a, qa);
+            split1((double)(lj + y0) + (double)ty + (double)uy * dt, n, b, qb);
+            split1((double)k + (double)tz + (double)uz * dt, n, c, qc);
+            __stcs(cell + p, pack_cell(a, b, c));
+            __stcs(ox + p, qa);
+            __stcs(oy + p, qb);
+            __stcs(oz + p, qc);
+        }
+    }
+}
+
 // ----------------------------------------------------- FP32 adjoints
 // The FP32 split-position counterparts of csrc/adjoint.cu (same algebra; no
 // counterpart in the reference).  With U(c) = scale_d dbar(c) +
@@ -895,6 +991,40 @@ int slab_kick_drift_f32(const Plan& p, int x0, int nx, const float* phi, uint32_
             k_kick_drift_f32<2, true, true><<<g, kThreads, 0, p.stream>>>(phi, cell, ox, oy, oz, vx, vy, vz, np, ck,
                                                                           dt, p.ng, nullptr, nullptr, 0, x0, nx,
                                                                           p.d_err);
+    }
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+int pencil_deposit_f32(const Plan& p, int x0, int y0, int nx, int ny, const uint32_t* cell, const float* ox,
+                       const float* oy, const float* oz, int64_t np, float mass, float* buf) {
+    const long long n = (long long)(nx + 5) * (ny + 5) * (p.ng + 2);
+    {
+        Timed t(p, ST_MESH_INIT);
+        k_pencil_init<<<grid_for(p, n, kThreads, 8), kThreads, 0, p.stream>>>(buf, nx, ny, p.ng);
+    }
+    if (np > 0) {
+        Timed t(p, ST_DEPOSIT);
+        k_pencil_deposit<<<grid_for(p, np, kThreads, 8), kThreads, 0, p.stream>>>(cell, ox, oy, oz, np, mass, buf, x0,
+                                                                                  y0, nx, ny, p.ng, p.d_err);
+    }
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+int pencil_kick_drift_f32(const Plan& p, int x0, int y0, int nx, int ny, const float* buf, uint32_t* cell, float* ox,
+                          float* oy, float* oz, float* vx, float* vy, float* vz, int64_t np, double c_kick,
+                          double dt) {
+    if (np == 0) return PM_OK;
+    const unsigned g = grid_for(p, np, kThreads, 3);
+    {
+        Timed t(p, ST_KICK_DRIFT);
+        if (p.grad_order == 4)
+            k_pencil_kick_drift<4><<<g, kThreads, 0, p.stream>>>(buf, cell, ox, oy, oz, vx, vy, vz, np, (float)c_kick,
+                                                                 dt, p.ng, x0, y0, nx, ny, p.d_err);
+        else
+            k_pencil_kick_drift<2><<<g, kThreads, 0, p.stream>>>(buf, cell, ox, oy, oz, vx, vy, vz, np, (float)c_kick,
+                                                                 dt, p.ng, x0, y0, nx, ny, p.d_err);
     }
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;

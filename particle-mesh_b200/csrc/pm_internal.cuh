@@ -229,6 +229,19 @@ int slab_fft_backward_f32(const Plan& p, float* own, int nx);
 int slab_kick_drift_f32(const Plan& p, int x0, int nx, const float* phi, uint32_t* cell, float* ox, float* oy,
                         float* oz, float* vx, float* vy, float* vz, int64_t np, double c_kick, double dt);
 int plan_create_internal(int ng, int precision, int green_kind, int grad_order, void* stream, pm_plan** out);
+// pencil decomposition (tiles.cu, fft.cu, particles.cu, slab.cu)
+int pencil_rank_sort(Plan& p, int px, int py, int nx, int ny, const uint32_t* cell, int64_t np, int64_t* counts);
+int pencil_copy3(const Plan& p, const float2* src, long long sa, long long sb, float2* dst, long long da, long long db,
+                 int A, int B, int C);
+int pencil_fft_lines_f32(const Plan& p, float* data, long long es, long long os, int planes, int ncols, int dir,
+                         int stage);
+int pencil_green_f32(const Plan& p, float* spec, int yc, int hc, int ky0, int kz0, double c_poisson);
+int pencil_z_f32(const Plan& p, float* rows, long long nrows, bool forward);
+int pencil_deposit_f32(const Plan& p, int x0, int y0, int nx, int ny, const uint32_t* cell, const float* ox,
+                       const float* oy, const float* oz, int64_t np, float mass, float* buf);
+int pencil_kick_drift_f32(const Plan& p, int x0, int y0, int nx, int ny, const float* buf, uint32_t* cell, float* ox,
+                          float* oy, float* oz, float* vx, float* vy, float* vz, int64_t np, double c_kick,
+                          double dt);
 
 // Adjoint kernels (adjoint.cu).
 int adjoint_gather_f64(const Plan& p, const double* x, const double* y, const double* z, const double* dbar,

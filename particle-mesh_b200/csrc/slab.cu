@@ -144,10 +144,53 @@ static void slab_release(Slab& s) {
     s.plan = nullptr;
 }
 
+// One rank's pencil of a Px x Py decomposition: x in [x0, x0 + nx), y in
+// [y0, y0 + ny), all z.  The spectrum is split into Py kz chunks
+// [kb(c), kb(c + 1)), kb(c) = c H / Py (H = ng/2 + 1), for the y stage and
+// into Px ky chunks of yc = ng / Px for the x stage.
+struct Pencil {
+    pm_plan* plan = nullptr;
+    int ng = 0, px = 1, py = 1, rank = 0, rx = 0, ry = 0, nx = 0, ny = 0, x0 = 0, y0 = 0, yc = 0, h = 0;
+    float* halo = nullptr;  // [nx + 5][ny + 5][ng + 2]
+    float2* own = nullptr;  // [nx][ny][h]
+    float2* work = nullptr;  // [nx][ng][hc] (y stage)
+    float2* send = nullptr;
+    float2* recv = nullptr;
+    long long xfer = 0;  // complex entries of each of work / send / recv
+    size_t bytes = 0;
+    int kb(int c) const { return (int)((long long)c * h / py); }
+    int hc(int c) const { return kb(c + 1) - kb(c); }
+    long long yoff(int c) const { return (long long)nx * ny * kb(c); }  // y-stage block c at nx ny kb(c)
+    float2* halo_c() const { return reinterpret_cast<float2*>(halo); }
+    long long hrow(int xl, int yl) const { return ((long long)xl * (ny + 5) + yl) * h; }  // complex offset
+};
+
+static void pencil_release(Pencil& q) {
+    for (void* b : {(void*)q.halo, (void*)q.own, (void*)q.work, (void*)q.send, (void*)q.recv})
+        if (b) cudaFree(b);
+    if (q.plan) pm_plan_destroy(q.plan);
+    q = Pencil{};
+}
+
+namespace {
+__global__ void k_add_rows(float* __restrict__ dst, long long dstride, const float* __restrict__ src, int nrows,
+                           int rowlen) {
+    const long long n = (long long)nrows * rowlen;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const long long r = e / rowlen, c = e - r * rowlen;
+        dst[r * dstride + c] += src[e];
+    }
+}
+}  // namespace
+
 }  // namespace pmb
 
 struct pm_slab {
     pmb::Slab s;
+};
+
+struct pm_pencil {
+    pmb::Pencil q;
 };
 
 using namespace pmb;
@@ -351,6 +394,274 @@ int pm_slab_migrate_unpack(pm_slab* slab, const uint32_t* packed, int64_t n, voi
 int pm_slab_check(pm_slab* slab) {
     if (!slab || !slab->s.plan) return fail(PM_ERR_ARG, "slab is NULL");
     return pm_plan_check(slab->s.plan);
+}
+
+// ------------------------------------------------------------- pencils
+
+static int pencil_ok(const pm_pencil* pen) {
+    if (!pen || !pen->q.plan) return fail(PM_ERR_ARG, "pencil is NULL");
+    int cur = -1;
+    if (cudaGetDevice(&cur) != cudaSuccess) return fail(PM_ERR_CUDA, "cudaGetDevice failed");
+    if (cur != pen->q.plan->p.device) PMB_CUDA_CHECK(cudaSetDevice(pen->q.plan->p.device));
+    return PM_OK;
+}
+
+int pm_pencil_create(int ng, int px, int py, int rank, int green_kind, int grad_order, void* stream,
+                     pm_pencil** out) {
+    if (!out) return fail(PM_ERR_ARG, "output pointer is NULL");
+    *out = nullptr;
+    if (!(ng >= 32 && ng <= 1024 && (ng & (ng - 1)) == 0))
+        return fail(PM_ERR_SIZE, "the pencil path needs a power-of-two ng in [32, 1024]");
+    auto pow2 = [](int v) { return v >= 1 && (v & (v - 1)) == 0; };
+    if (!pow2(px) || !pow2(py) || ng / px < 4 || ng / py < 4)
+        return fail(PM_ERR_SIZE, "px and py must be powers of two with ng / px and ng / py at least 4");
+    if (py > ng / 2 + 1) return fail(PM_ERR_SIZE, "py exceeds the kz planes of the half spectrum");
+    if (rank < 0 || rank >= px * py) return fail(PM_ERR_ARG, "rank out of range");
+    pm_pencil* pen = new (std::nothrow) pm_pencil();
+    if (!pen) return fail(PM_ERR_NOMEM, "host allocation failed");
+    Pencil& q = pen->q;
+    q.ng = ng;
+    q.px = px;
+    q.py = py;
+    q.rank = rank;
+    q.rx = rank / py;
+    q.ry = rank % py;
+    q.nx = ng / px;
+    q.ny = ng / py;
+    q.x0 = q.rx * q.nx;
+    q.y0 = q.ry * q.ny;
+    q.yc = ng / px;
+    q.h = ng / 2 + 1;
+    int rc = plan_create_internal(ng, PM_FP32, green_kind, grad_order, stream, &q.plan);
+    if (rc != PM_OK) {
+        delete pen;
+        return rc;
+    }
+    const int hcmax = (q.h + py - 1) / py;
+    q.xfer = (long long)q.nx * ng * hcmax;
+    const size_t haloB = (size_t)(q.nx + 5) * (q.ny + 5) * (ng + 2) * sizeof(float);
+    const size_t ownB = (size_t)q.nx * q.ny * q.h * sizeof(float2), xB = (size_t)q.xfer * sizeof(float2);
+    if (cudaMalloc(&q.halo, haloB) != cudaSuccess || cudaMalloc(&q.own, ownB) != cudaSuccess ||
+        cudaMalloc(&q.work, xB) != cudaSuccess || cudaMalloc(&q.send, xB) != cudaSuccess ||
+        cudaMalloc(&q.recv, xB) != cudaSuccess || cudaMemset(q.halo, 0, haloB) != cudaSuccess) {
+        cudaGetLastError();
+        pencil_release(q);
+        delete pen;
+        return fail(PM_ERR_NOMEM, "pencil buffer allocation failed");
+    }
+    q.bytes = haloB + ownB + 3 * xB;
+    *out = pen;
+    return PM_OK;
+}
+
+int pm_pencil_destroy(pm_pencil* pen) {
+    if (!pen) return PM_OK;
+    if (pen->q.plan) {
+        cudaSetDevice(pen->q.plan->p.device);
+        cudaStreamSynchronize(pen->q.plan->p.stream);
+    }
+    pencil_release(pen->q);
+    delete pen;
+    return PM_OK;
+}
+
+int pm_pencil_info(const pm_pencil* pen, int* nx, int* ny, int* x0, int* y0, void** halo, void** send, void** recv,
+                   size_t* xfer_floats, size_t* device_bytes) {
+    if (!pen || !pen->q.plan) return fail(PM_ERR_ARG, "pencil is NULL");
+    const Pencil& q = pen->q;
+    if (nx) *nx = q.nx;
+    if (ny) *ny = q.ny;
+    if (x0) *x0 = q.x0;
+    if (y0) *y0 = q.y0;
+    if (halo) *halo = q.halo;
+    if (send) *send = q.send;
+    if (recv) *recv = q.recv;
+    if (xfer_floats) *xfer_floats = (size_t)q.xfer * 2;
+    if (device_bytes) *device_bytes = q.bytes + q.plan->p.bytes;
+    return PM_OK;
+}
+
+int pm_pencil_plan(pm_pencil* pen, pm_plan** plan) {
+    if (!pen || !plan) return fail(PM_ERR_ARG, "NULL argument");
+    *plan = pen->q.plan;
+    return PM_OK;
+}
+
+int pm_pencil_deposit_f32(pm_pencil* pen, const uint32_t* cell, const float* ox, const float* oy, const float* oz,
+                          int64_t np, float mass) {
+    PM_TRY_S(pencil_ok(pen));
+    if (np < 0) return fail(PM_ERR_ARG, "negative particle count");
+    if (np > 0 && (!cell || !ox || !oy || !oz)) return fail(PM_ERR_ARG, "NULL particle array");
+    Pencil& q = pen->q;
+    return pencil_deposit_f32(q.plan->p, q.x0, q.y0, q.nx, q.ny, cell, ox, oy, oz, np, mass, q.halo);
+}
+
+int pm_pencil_fold_f32(pm_pencil* pen, const float* xghost, const float* yghost, const float* corner) {
+    PM_TRY_S(pencil_ok(pen));
+    if (!xghost || !yghost || !corner) return fail(PM_ERR_ARG, "NULL ghost rows");
+    Pencil& q = pen->q;
+    const Plan& p = q.plan->p;
+    const int rl = q.ng + 2;
+    const long long row = rl, plane = (long long)(q.ny + 5) * rl;
+    {
+        Timed t(p, ST_DEPOSIT, 3);
+        // x ghost: rows (2, 2..ny+1); y ghost: rows (2..nx+1, 2); corner: (2, 2)
+        k_add_rows<<<grid_for(p, (long long)q.ny * rl, 256, 2), 256, 0, p.stream>>>(q.halo + 2 * plane + 2 * row, row,
+                                                                                   xghost, q.ny, rl);
+        k_add_rows<<<grid_for(p, (long long)q.nx * rl, 256, 2), 256, 0, p.stream>>>(q.halo + 2 * plane + 2 * row,
+                                                                                   plane, yghost, q.nx, rl);
+        k_add_rows<<<grid_for(p, rl, 256, 2), 256, 0, p.stream>>>(q.halo + 2 * plane + 2 * row, row, corner, 1, rl);
+    }
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+int pm_pencil_forward_f32(pm_pencil* pen) {
+    PM_TRY_S(pencil_ok(pen));
+    Pencil& q = pen->q;
+    const Plan& p = q.plan->p;
+    const long long H = q.h, ny = q.ny, nx = q.nx;
+    {
+        Timed t(p, ST_SORT);
+        PM_TRY_S(pencil_copy3(p, q.halo_c() + q.hrow(2, 2), (ny + 5) * H, H, q.own, ny * H, H, q.nx, q.ny, q.h));
+    }
+    PM_TRY_S(pencil_z_f32(p, reinterpret_cast<float*>(q.own), nx * ny, true));
+    Timed t(p, ST_SORT);
+    for (int c = 0; c < q.py; ++c)
+        PM_TRY_S(pencil_copy3(p, q.own + q.kb(c), ny * H, H, q.send + q.yoff(c), ny * q.hc(c), q.hc(c), q.nx, q.ny,
+                              q.hc(c)));
+    return PM_OK;
+}
+
+int pm_pencil_yfwd_f32(pm_pencil* pen) {
+    PM_TRY_S(pencil_ok(pen));
+    Pencil& q = pen->q;
+    const Plan& p = q.plan->p;
+    const long long hc = q.hc(q.ry), ng = q.ng, nx = q.nx, ny = q.ny, yc = q.yc;
+    {
+        Timed t(p, ST_SORT);
+        for (int s = 0; s < q.py; ++s)  // [src][nx][ny][hc] -> [nx][ng][hc]
+            PM_TRY_S(pencil_copy3(p, q.recv + (long long)s * nx * ny * hc, ny * hc, hc, q.work + (long long)s * ny * hc,
+                                  ng * hc, hc, q.nx, q.ny, (int)hc));
+    }
+    PM_TRY_S(pencil_fft_lines_f32(p, reinterpret_cast<float*>(q.work), hc, ng * hc, q.nx, (int)hc, -1, ST_FFT_Y_FWD));
+    Timed t(p, ST_SORT);
+    for (int d = 0; d < q.px; ++d)  // ky chunk d: [nx][yc][hc]
+        PM_TRY_S(pencil_copy3(p, q.work + (long long)d * yc * hc, ng * hc, hc, q.send + (long long)d * nx * yc * hc,
+                              yc * hc, hc, q.nx, q.yc, (int)hc));
+    return PM_OK;
+}
+
+int pm_pencil_xgreen_f32(pm_pencil* pen, double c_poisson) {
+    PM_TRY_S(pencil_ok(pen));
+    Pencil& q = pen->q;
+    const Plan& p = q.plan->p;
+    const long long hc = q.hc(q.ry), yc = q.yc;
+    float* x = reinterpret_cast<float*>(q.recv);  // [src x block][nx][yc][hc] = [ng][yc][hc]
+    PM_TRY_S(pencil_fft_lines_f32(p, x, yc * hc, hc, q.yc, (int)hc, -1, ST_FFT_X_FWD));
+    PM_TRY_S(pencil_green_f32(p, x, q.yc, (int)hc, q.rx * q.yc, q.kb(q.ry), c_poisson));
+    PM_TRY_S(pencil_fft_lines_f32(p, x, yc * hc, hc, q.yc, (int)hc, +1, ST_FFT_X_INV));
+    PMB_CUDA_CHECK(cudaMemcpyAsync(q.send, q.recv, (size_t)q.ng * yc * hc * sizeof(float2), cudaMemcpyDeviceToDevice,
+                                   p.stream));
+    return PM_OK;
+}
+
+int pm_pencil_yinv_f32(pm_pencil* pen) {
+    PM_TRY_S(pencil_ok(pen));
+    Pencil& q = pen->q;
+    const Plan& p = q.plan->p;
+    const long long hc = q.hc(q.ry), ng = q.ng, nx = q.nx, ny = q.ny, yc = q.yc;
+    {
+        Timed t(p, ST_SORT);
+        for (int s = 0; s < q.px; ++s)  // [src ky chunk][nx][yc][hc] -> [nx][ng][hc]
+            PM_TRY_S(pencil_copy3(p, q.recv + (long long)s * nx * yc * hc, yc * hc, hc, q.work + (long long)s * yc * hc,
+                                  ng * hc, hc, q.nx, q.yc, (int)hc));
+    }
+    PM_TRY_S(pencil_fft_lines_f32(p, reinterpret_cast<float*>(q.work), hc, ng * hc, q.nx, (int)hc, +1, ST_FFT_Y_INV));
+    Timed t(p, ST_SORT);
+    for (int d = 0; d < q.py; ++d)  // y block d: [nx][ny][hc]
+        PM_TRY_S(pencil_copy3(p, q.work + (long long)d * ny * hc, ng * hc, hc, q.send + (long long)d * nx * ny * hc,
+                              ny * hc, hc, q.nx, q.ny, (int)hc));
+    return PM_OK;
+}
+
+int pm_pencil_backward_f32(pm_pencil* pen) {
+    PM_TRY_S(pencil_ok(pen));
+    Pencil& q = pen->q;
+    const Plan& p = q.plan->p;
+    const long long H = q.h, nx = q.nx, ny = q.ny;
+    {
+        Timed t(p, ST_SORT);
+        for (int s = 0; s < q.py; ++s)  // [src kz chunk][nx][ny][hc(src)] -> own [nx][ny][H]
+            PM_TRY_S(pencil_copy3(p, q.recv + q.yoff(s), ny * q.hc(s), q.hc(s), q.own + q.kb(s), ny * H, H, q.nx, q.ny,
+                                  q.hc(s)));
+    }
+    PM_TRY_S(pencil_z_f32(p, reinterpret_cast<float*>(q.own), nx * ny, false));
+    Timed t(p, ST_SORT);
+    return pencil_copy3(p, q.own, ny * H, H, q.halo_c() + q.hrow(2, 2), (ny + 5) * H, H, q.nx, q.ny, q.h);
+}
+
+int pm_pencil_kick_drift_f32(pm_pencil* pen, uint32_t* cell, float* ox, float* oy, float* oz, float* vx, float* vy,
+                             float* vz, int64_t np, double c_kick, double dt) {
+    PM_TRY_S(pencil_ok(pen));
+    if (np < 0) return fail(PM_ERR_ARG, "negative particle count");
+    if (np > 0 && (!cell || !ox || !oy || !oz || !vx || !vy || !vz)) return fail(PM_ERR_ARG, "NULL particle array");
+    Pencil& q = pen->q;
+    return pencil_kick_drift_f32(q.plan->p, q.x0, q.y0, q.nx, q.ny, q.halo, cell, ox, oy, oz, vx, vy, vz, np, c_kick,
+                                 dt);
+}
+
+int pm_pencil_migrate_sort(pm_pencil* pen, const uint32_t* cell, int64_t np, int64_t* counts) {
+    PM_TRY_S(pencil_ok(pen));
+    if (np < 0 || !counts || (np > 0 && !cell)) return fail(PM_ERR_ARG, "bad migration arguments");
+    if (np > (int64_t)0xffffffffll) return fail(PM_ERR_SIZE, "a pencil holds at most 2^32 - 1 particles");
+    Pencil& q = pen->q;
+    return pencil_rank_sort(q.plan->p, q.px, q.py, q.nx, q.ny, cell, np, counts);
+}
+
+int pm_pencil_migrate_pack(pm_pencil* pen, void* const* arrays, int narrays, int64_t np, uint32_t* packed) {
+    PM_TRY_S(pencil_ok(pen));
+    if (!arrays || narrays < 1 || narrays > 8 || np < 0 || (np > 0 && !packed))
+        return fail(PM_ERR_ARG, "bad pack arguments");
+    Words w{};
+    for (int a = 0; a < narrays; ++a) {
+        w.a[a] = static_cast<uint32_t*>(arrays[a]);
+        if (np > 0 && !w.a[a]) return fail(PM_ERR_ARG, "NULL particle array");
+    }
+    const Plan& p = pen->q.plan->p;
+    if (np > p.tiles.np_cap) return fail(PM_ERR_STATE, "pm_pencil_migrate_sort must precede the pack");
+    if (np == 0) return PM_OK;
+    {
+        Timed t(p, ST_SORT);
+        k_pack_words<<<grid_for(p, np, 256, 4), 256, 0, p.stream>>>(p.tiles.perm, np, w, narrays, packed);
+    }
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+int pm_pencil_migrate_unpack(pm_pencil* pen, const uint32_t* packed, int64_t n, void* const* arrays, int narrays,
+                             int64_t at) {
+    PM_TRY_S(pencil_ok(pen));
+    if (!arrays || narrays < 1 || narrays > 8 || n < 0 || at < 0 || (n > 0 && !packed))
+        return fail(PM_ERR_ARG, "bad unpack arguments");
+    Words w{};
+    for (int a = 0; a < narrays; ++a) {
+        w.a[a] = static_cast<uint32_t*>(arrays[a]);
+        if (n > 0 && !w.a[a]) return fail(PM_ERR_ARG, "NULL particle array");
+    }
+    if (n == 0) return PM_OK;
+    const Plan& p = pen->q.plan->p;
+    {
+        Timed t(p, ST_SORT);
+        k_unpack_words<<<grid_for(p, n, 256, 4), 256, 0, p.stream>>>(packed, n, w, narrays, at);
+    }
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+int pm_pencil_check(pm_pencil* pen) {
+    if (!pen || !pen->q.plan) return fail(PM_ERR_ARG, "pencil is NULL");
+    return pm_plan_check(pen->q.plan);
 }
 
 }  // extern "C"

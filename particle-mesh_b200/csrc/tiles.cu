@@ -96,7 +96,17 @@ __device__ __forceinline__ uint32_t slab_rank_of(uint32_t c, int nx_log, int n) 
     return (uint32_t)(i >> nx_log);
 }
 
-enum : int { KEY_TILE3 = 0, KEY_MORTON = 1, KEY_COLUMN = 2, KEY_SLABCOL = 3, KEY_RANK = 4 };
+// Owner of a particle in a pencil decomposition (Px x Py ranks, rank =
+// px * Py + py): ((i mod n) >> log2 nx) << log2 Py | ((j mod n) >> log2 ny);
+// yp packs log2 ny (low byte) and log2 Py (next byte).
+__device__ __forceinline__ uint32_t pencil_rank_of(uint32_t c, int nx_log, int n, int yp) {
+    int i = (int)(c >> 20), j = (int)((c >> 10) & 1023u);
+    if (i >= n) i %= n;
+    if (j >= n) j %= n;
+    return ((uint32_t)(i >> nx_log) << ((yp >> 8) & 255)) | (uint32_t)(j >> (yp & 255));
+}
+
+enum : int { KEY_TILE3 = 0, KEY_MORTON = 1, KEY_COLUMN = 2, KEY_SLABCOL = 3, KEY_RANK = 4, KEY_PENCIL = 5 };
 
 // Morton (Z-order) index of a particle's tile, for the spatial sort.
 __device__ __forceinline__ uint32_t spread3(uint32_t v) {  // 10 bits -> every third bit
@@ -134,6 +144,7 @@ __device__ __forceinline__ uint32_t bin_key(const uint32_t* __restrict__ cell, l
     const uint32_t c = __ldg(cell + p);
     if (KEY == KEY_SLABCOL) return kb + slab_column_bucket_of(c, nt, ts_log, xa);
     if (KEY == KEY_RANK) return kb + slab_rank_of(c, ts_log, nt);
+    if (KEY == KEY_PENCIL) return kb + pencil_rank_of(c, ts_log, nt, xa);
     return kb + (KEY == KEY_MORTON ? morton_tile(c, ts_log, nt)
                                    : (KEY == KEY_COLUMN ? column_bucket_of(c, ts_log, nt, xa) : bucket_of(c, ts_log, nt)));
 }
@@ -838,6 +849,40 @@ int slab_rank_sort(Plan& p, int nranks, int nx, const uint32_t* cell, int64_t np
         k_scan_sums<<<1, kScanThreads, 0, p.stream>>>(s.bsum, 1, s.off + nb);
         k_scan_add<<<1, kScanThreads, 0, p.stream>>>(s.off, s.cursor, nb, s.bsum);
         if (np > 0) k_bucket_scatter<KEY_RANK><<<g, 256, 0, p.stream>>>(cell, np, nx_log, p.ng, s.cursor, s.perm);
+    }
+    PMB_CUDA_CHECK(cudaGetLastError());
+    std::vector<uint32_t> off(nb + 1);
+    PMB_CUDA_CHECK(cudaMemcpyAsync(off.data(), s.off, (nb + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, p.stream));
+    PMB_CUDA_CHECK(cudaStreamSynchronize(p.stream));
+    for (long long r = 0; r < nb; ++r) counts[r] = (int64_t)off[r + 1] - (int64_t)off[r];
+    return PM_OK;
+}
+
+// Counting sort of the particles by owning pencil: the permutation in the
+// plan's scratch, counts[r] (host) particles per rank r = px * Py + py.
+int pencil_rank_sort(Plan& p, int px, int py, int nx, int ny, const uint32_t* cell, int64_t np, int64_t* counts) {
+    auto lg = [](int v) {
+        int l = 0;
+        while ((1 << l) < v) ++l;
+        return l;
+    };
+    const int nx_log = lg(nx), yp = lg(ny) | (lg(py) << 8);
+    const long long nb = (long long)px * py;
+    int rc = tile_scratch_ensure(p, np > 0 ? np : 1, 1, nb);
+    if (rc != PM_OK) return rc;
+    TileScratch& s = p.tiles;
+    PMB_CUDA_CHECK(cudaMemsetAsync(s.count, 0, nb * sizeof(uint32_t), p.stream));
+    const unsigned g = grid_for(p, np, 256);
+    {
+        Timed t(p, ST_SORT, np > 0 ? 5 : 3);
+        if (np > 0)
+            k_bucket_count<KEY_PENCIL><<<g, 256, 0, p.stream>>>(cell, np, nx_log, p.ng, s.count, nullptr, nullptr, 0, yp);
+        k_scan_local<<<1, kScanThreads, 0, p.stream>>>(s.count, nb, s.off, s.bsum);
+        k_scan_sums<<<1, kScanThreads, 0, p.stream>>>(s.bsum, 1, s.off + nb);
+        k_scan_add<<<1, kScanThreads, 0, p.stream>>>(s.off, s.cursor, nb, s.bsum);
+        if (np > 0)
+            k_bucket_scatter<KEY_PENCIL><<<g, 256, 0, p.stream>>>(cell, np, nx_log, p.ng, s.cursor, s.perm, nullptr,
+                                                                  nullptr, 0, yp);
     }
     PMB_CUDA_CHECK(cudaGetLastError());
     std::vector<uint32_t> off(nb + 1);
