@@ -25,7 +25,8 @@ over every particle; particle-updates/s = particles x steps / time.
 Multi-GPU (torchrun): the configuration's one box is split into x-slabs, one
 per GPU (strong scaling; NCCL ghost fold, spectrum transposes, potential halo
 and particle migration every step), and the ensemble's boxes are dealt to the
-GPUs; every timing is the max over ranks.
+GPUs; every timing is the max over ranks.  --pencil splits it into px x py
+pencils instead (x and y; two sub-group transposes).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -73,6 +74,8 @@ def parse():
                     help="gather of the FP32 step (pm_plan_set_gather)")
     ap.add_argument("--slab", action="store_true",
                     help="run the x-slab decomposition at N = 1 too (at N > 1 it is the default)")
+    ap.add_argument("--pencil", action="store_true",
+                    help="run the pencil decomposition instead (px x py = N pencils, px >= py; 1 x 1 at N = 1)")
     return ap.parse_args()
 
 
@@ -351,13 +354,24 @@ def ensemble_leg(pm, torch, args, world, rank, dev, stream, barrier, max_over_ra
     return out
 
 
+def pencil_grid(world: int):
+    """px x py = world, px the larger power-of-two factor."""
+    px = 1
+    while px * px < world:
+        px *= 2
+    return px, world // px
+
+
 # --------------------------------------------------- N GPUs: one slab each
 def ours_slab(args, pm, torch, dist, world, rank, dev, stream, barrier, max_over_ranks):
     """The configuration's one box (512^3 particles on a 1024^3 mesh) split
     over the N GPUs as x-slabs (strong scaling): per step the ghost-plane
     fold, two all-to-all transposes of the spectrum, the potential halo and
-    the particle migration go over NCCL (slab.DistExchange)."""
+    the particle migration go over NCCL (slab.DistExchange).  With --pencil,
+    px x py pencils (pencil.DistExchange: row / column sub-groups)."""
     S = pm.slab
+    P = pm.pencil
+    px, py = pencil_grid(world)
     ng, nrow = args.ng, args.nrow
     np_ = nrow ** 3
     mass = ng ** 3 / np_
@@ -369,14 +383,23 @@ def ours_slab(args, pm, torch, dist, world, rank, dev, stream, barrier, max_over
     v32 = [a.float() for a in vel]
     ids = torch.arange(np_, dtype=torch.int32, device=dev)
     del pos, vel
-    (part,) = S.distribute(cell, off, v32, ids, ng, world, [rank])
+    if args.pencil:
+        (part,) = P.distribute(cell, off, v32, ids, ng, px, py, [rank])
+    else:
+        (part,) = S.distribute(cell, off, v32, ids, ng, world, [rank])
     del cell, off, v32, ids
     torch.cuda.empty_cache()
-    slab = S.Slab(ng, world, rank, "spectral", 4, stream=stream, device=dev)
-    ex = S.DistExchange()
+    if args.pencil:
+        slab = P.Pencil(ng, px, py, rank, "spectral", 4, stream=stream, device=dev)
+        ex = P.DistExchange(px, py) if world > 1 else P.LocalExchange()
+        step_fn = P.step
+    else:
+        slab = S.Slab(ng, world, rank, "spectral", 4, stream=stream, device=dev)
+        ex = S.DistExchange()
+        step_fn = S.step
     sampler = ClockSampler(bus_id(torch, dev))
     for _ in range(args.warmup):
-        S.step([slab], [part], ex, mass, cp, ck, DT)
+        step_fn([slab], [part], ex, mass, cp, ck, DT)
     slab.check()
     slab.read_timing(reset=True)
     slab.set_timing(True)
@@ -385,7 +408,7 @@ def ours_slab(args, pm, torch, dist, world, rank, dev, stream, barrier, max_over
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
-        S.step([slab], [part], ex, mass, cp, ck, DT)
+        step_fn([slab], [part], ex, mass, cp, ck, DT)
     e1.record(stream)
     torch.cuda.synchronize()
     clocks = sampler.stop()
@@ -409,7 +432,8 @@ def ours_slab(args, pm, torch, dist, world, rank, dev, stream, barrier, max_over
                 "peak_source": f"{peak_kind} hbm_gbs (copy bandwidth)", "ms_per_launch": dom_ms,
                 "achieved": dom_bytes / (dom_ms / 1e3) / 1e9 if dom_bytes else None,
                 "frac": dom_bytes / (dom_ms / 1e3) / 1e9 / peak if dom_bytes else None, "traffic": None,
-                "note": "per rank; the byte model of one box times the slab's share"}
+                "note": f"per rank; the byte model of one box times the {'pencil' if args.pencil else 'slab'}'s "
+                        "share"}
     # ---- end to end: this rank's particle state from pinned host memory and
     # back every step
     host = torch.empty(part.words.shape, dtype=torch.int32, pin_memory=True)
@@ -417,9 +441,13 @@ def ours_slab(args, pm, torch, dist, world, rank, dev, stream, barrier, max_over
     nbytes = part.n * 8 * 4
 
     def e2e_step():
-        part.words[:, :part.n].copy_(host[:, :part.n], non_blocking=True)
-        S.step([slab], [part], ex, mass, cp, ck, DT)
-        host[:, :part.n].copy_(part.words[:, :part.n], non_blocking=True)
+        # one contiguous copy per particle word (a strided view of pinned
+        # memory would be staged through pageable memory)
+        for w in range(part.words.shape[0]):
+            part.words[w, :part.n].copy_(host[w, :part.n], non_blocking=True)
+        step_fn([slab], [part], ex, mass, cp, ck, DT)
+        for w in range(part.words.shape[0]):
+            host[w, :part.n].copy_(part.words[w, :part.n], non_blocking=True)
 
     for _ in range(max(1, args.warmup)):
         e2e_step()
@@ -434,8 +462,9 @@ def ours_slab(args, pm, torch, dist, world, rank, dev, stream, barrier, max_over
     te = max_over_ranks(e0.elapsed_time(e1))
     e2e = {"value": np_ * args.steps / (te / 1e3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
            "d2h_bytes_per_step": nbytes, "ms_per_step": te / args.steps,
-           "path": "slab.step (pm_slab_* through the C ABI, NCCL exchanges); this rank's particle words copied "
-                   "from pinned host memory and back every step"}
+           "path": f"{'pencil' if args.pencil else 'slab'}.step (pm_{'pencil' if args.pencil else 'slab'}_* "
+                   "through the C ABI, NCCL exchanges); this rank's particle words copied from pinned host memory "
+                   "and back every step"}
     ensemble = None
     if not args.skip_ensemble:
         slab.close()
@@ -453,8 +482,11 @@ def ours_slab(args, pm, torch, dist, world, rank, dev, stream, barrier, max_over
                                    f"spectral Poisson, 4-point gradient, KDK dt={DT}, Zel'dovich P(k)~k^{N_S} "
                                    f"rms {RMS} cell",
                        "particles_total": np_, "mesh": ng, "l2": "inputs larger than L2",
-                       "parallelism": f"slab{world}: x-slabs of {ng // world} planes, one per GPU; NCCL ghost "
-                                      f"fold, two all-to-all transposes, potential halo, particle migration"},
+                       "parallelism": (f"pencil{px}x{py}: pencils of {ng // px} x {ng // py} columns, one per "
+                                       f"GPU; ghost rows, two y-group and two x-group all-to-all transposes, "
+                                       f"two-axis potential halo, particle migration" if args.pencil else
+                                       f"slab{world}: x-slabs of {ng // world} planes, one per GPU; NCCL ghost "
+                                       f"fold, two all-to-all transposes, potential halo, particle migration")},
             "stages": per_stage, "ensemble": ensemble, "e2e": e2e, "roofline": roofline, "cpu_baseline": None,
             "clocks": clocks, "gpu_launches": launches}
     print(json.dumps(line), flush=True)
@@ -489,7 +521,7 @@ def ours(args):
     mass = ng ** 3 / np_
     cp, ck = pm.unit_box_coefficients(DT)
     stream = torch.cuda.current_stream(dev)
-    if world > 1 or args.slab:
+    if world > 1 or args.slab or args.pencil:
         return ours_slab(args, pm, torch, dist, world, rank, dev, stream, barrier, max_over_ranks)
 
     pos, vel = pm.zeldovich_ic(ng, nrow, N_S, RMS, rank_seed(rank), device=dev)

@@ -161,12 +161,20 @@ k_fft_strided(typename Cx<T>::t* __restrict__ data, long long es_, long long os_
     // AX = 2: lines read along the outer axis of `data` (element stride N H,
     // plane stride H: y lines of the transposed spectrum [ky][kx][kz]) and
     // written along the middle axis of `out` (element stride H, plane stride
-    // N H: the spectrum [kx][y][kz]); every other AX works in place.
+    // N H: the spectrum [kx][y][kz]).
+    // AX = 3: y lines of the planes [x][y][kz] of `data` written into `out`
+    // at the runtime strides es_ (element) and os_ (plane): the x-slab's y
+    // forward pass storing straight into its transpose buffer.
+    // AX = 4: lines read from `data` at the runtime strides es_, os_ and
+    // written along the middle axis of `out` (stride H, planes N H): the
+    // x-slab's y inverse pass reading straight from its transpose buffer.
+    // AX = 0, 1, -1 work in place.
     constexpr long long H = N / 2 + 1;
     constexpr bool OUTER = AX == 0 || AX == 2;
-    const long long es = AX == 1 ? H : (OUTER ? (long long)N * H : es_);
-    const long long os = AX == 1 ? (long long)N * H : (OUTER ? H : os_);
-    const long long oes = AX == 2 ? H : es, oos = AX == 2 ? (long long)N * H : os;
+    constexpr bool MID_IN = AX == 1 || AX == 3, MID_OUT = AX == 2 || AX == 4;
+    const long long es = MID_IN ? H : (OUTER ? (long long)N * H : es_);
+    const long long os = MID_IN ? (long long)N * H : (OUTER ? H : os_);
+    const long long oes = MID_OUT ? H : (AX == 3 ? es_ : es), oos = MID_OUT ? (long long)N * H : (AX == 3 ? os_ : os);
     extern __shared__ __align__(16) unsigned char smraw[];
     C* S = reinterpret_cast<C*>(smraw);
     const int tx = threadIdx.x % TK, ty = threadIdx.x / TK;
@@ -175,7 +183,7 @@ k_fft_strided(typename Cx<T>::t* __restrict__ data, long long es_, long long os_
     // plane blockIdx.y % N of box blockIdx.y / N (boxes of a batch at stride bs)
     const long long box = blockIdx.y / N, plane = blockIdx.y % N;
     C* base = data + box * bs + plane * os + (active ? col : 0);
-    C* obase = AX == 2 ? out + box * bs + plane * oos + (active ? col : 0) : base;
+    C* obase = AX >= 2 ? out + box * bs + plane * oos + (active ? col : 0) : base;
 
     using I = SIdx<R1, R2, TK>;
     const long long es1 = es * R2, oes2 = oes * R1;
@@ -219,19 +227,22 @@ __device__ __forceinline__ T green_value(int kx, int ky, int kz, int kind, doubl
 // written to `out` in the transposed layout [ky][kx][kz] (element stride H),
 // so that neither this pass nor the next one both reads and writes lines
 // whose elements lie N H apart; otherwise in place.
-// SLABX: the x lines of one slab's share of the spectrum after the global
-// transpose, laid out [ky - ky0][kx][kz] (element stride H, plane stride N H,
-// in place), plane blockIdx.y holding ky = ky0 + blockIdx.y.
+// SLABX: the x lines of one x-slab's share of the spectrum straight from the
+// transpose buffer `data` into the one to send back, `out`: plane blockIdx.y
+// holds ky = ky0 + blockIdx.y, and element kx of a line lies at
+// (kx >> nxl) nx^2 H + (kx & (nx - 1)) H from the plane's start
+// blockIdx.y nx H (nx = 2^nxl planes per slab; rank kx / nx's block of
+// [ky][x][kz] rows), in both buffers.
 template <typename T, int N, int TK, int RV = 0, bool XT = false, bool SLABX = false>
 __global__ void __launch_bounds__(strided_threads<N, TK, RV>(), 2)
 k_fft_x_green(typename Cx<T>::t* __restrict__ data, long long es_, long long os_, long long bs, int ncols,
               const typename Cx<T>::t* __restrict__ tw, const T* __restrict__ g1d, double cg, int kind,
-              typename Cx<T>::t* out, int ky0 = 0) {
+              typename Cx<T>::t* out, int ky0 = 0, int nxl = 0) {
     using C = typename Cx<T>::t;
     constexpr int R1 = RadixV<N, RV>::R1, R2 = RadixV<N, RV>::R2;
     // x lines of the padded spectrum: compile-time strides (es_ = N H and
     // os_ = H are what every caller passes)
-    constexpr long long es = SLABX ? N / 2 + 1 : (long long)N * (N / 2 + 1), os = SLABX ? (long long)N * (N / 2 + 1) : N / 2 + 1;
+    constexpr long long es = (long long)N * (N / 2 + 1), os = N / 2 + 1;
     constexpr long long oes = XT ? os : es, oos = XT ? es : os;
     // FP32: pass-2 twiddles from 10 table loads per thread (2.97 vs 3.10 ms)
     constexpr bool kSplitTw = R2 >= 16 && sizeof(T) == 4;
@@ -243,15 +254,24 @@ k_fft_x_green(typename Cx<T>::t* __restrict__ data, long long es_, long long os_
     const int col = blockIdx.x * TK + tx;
     const bool active = col < ncols;
     const int ky = SLABX ? ky0 + (int)blockIdx.y : (int)(blockIdx.y % N);
-    C* base = SLABX ? data + (long long)blockIdx.y * os + (active ? col : 0)
+    constexpr int H = N / 2 + 1;
+    // (SLABX offsets fit 32 bits: nx^2 H * (N / nx) <= N^2 H < 2^31)
+    const int nmask = (1 << nxl) - 1, sstride = (1 << (2 * nxl)) * H;
+    auto soff = [&](int n) { return (n >> nxl) * sstride + (n & nmask) * H; };
+    C* base = SLABX ? data + (long long)blockIdx.y * ((long long)H << nxl) + (active ? col : 0)
                     : data + (long long)(blockIdx.y / N) * bs + (long long)ky * os + (active ? col : 0);
-    C* obase = XT ? out + (long long)(blockIdx.y / N) * bs + (long long)ky * oos + (active ? col : 0) : base;
+    C* obase = SLABX ? out + (long long)blockIdx.y * ((long long)H << nxl) + (active ? col : 0)
+                     : (XT ? out + (long long)(blockIdx.y / N) * bs + (long long)ky * oos + (active ? col : 0) : base);
 
     using I = SIdx<R1, R2, TK>;
     const long long es1 = es * R2, oes2 = oes * R1;
     auto p2ld = [&](int j, int r) { return S[I::p2(j, r, tx)]; };
     stockham_pass1<R1, R2, -1, false, C>(
-        ty, [&](int j, int r) { return active ? base[j * es + r * es1] : cmake<C>(0, 0); },
+        ty,
+        [&](int j, int r) {
+            if (!active) return cmake<C>(0, 0);
+            return SLABX ? base[soff(j + r * R2)] : base[j * es + r * es1];
+        },
         [&](int j, int k, C v) { S[I::out1(j, k, tx)] = v; });
     __syncthreads();
     stockham_pass2<R1, R2, -1, true, C>(
@@ -265,7 +285,14 @@ k_fft_x_green(typename Cx<T>::t* __restrict__ data, long long es_, long long os_
         ty, [&](int j, int r) { return S[I::in1(j, r, tx)]; }, [&](int j, int k, C v) { S[I::out1(j, k, tx)] = v; });
     __syncthreads();
     stockham_pass2<R1, R2, +1, false, C>(
-        ty, p2ld, [&](int j, int k, C v) { if (active) obase[j * oes + k * oes2] = v; },
+        ty, p2ld,
+        [&](int j, int k, C v) {
+            if (!active) return;
+            if (SLABX)
+                obase[soff(j + k * R1)] = v;
+            else
+                obase[j * oes + k * oes2] = v;
+        },
         pass2_twiddles<+1, kSplitTw>(tw, ty));
 }
 
@@ -448,6 +475,8 @@ template <typename T, int N, int TK = tk_cols<T, N>(), int RV = 0> struct Launch
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_x_green<T, N, TK, RV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_x_green<T, N, TK, RV, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, +1, TK, RV, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
+        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, -1, TK, RV, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
+        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, +1, TK, RV, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, -1, TK, RV, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, +1, TK, RV, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_x_green<T, N, TK, RV, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
@@ -495,13 +524,34 @@ template <typename T, int N, int TK = tk_cols<T, N>(), int RV = 0> struct Launch
             k_fft_strided<T, N, +1, TK, RV, -1><<<grid, strided_threads<N, TK, RV>(), smem_s(), p.stream>>>(
                 d, es, os, 0, ncols, tw, d);
     }
-    static void xgreen_slab(const Plan& p, T* spec, double cg, int planes, int ky0) {
-        C* d = reinterpret_cast<C*>(spec);
-        const dim3 grid((H + TK - 1) / TK, planes);
+    // x forward + Green + x inverse of an x-slab's nx = 2^nxl ky planes,
+    // from the received transpose buffer into the one to send back
+    static void xgreen_slab(const Plan& p, const T* in, T* out, double cg, int ky0, int nxl) {
+        const dim3 grid((H + TK - 1) / TK, 1 << nxl);
         Timed t(p, ST_FFT_X_GREEN);
         k_fft_x_green<T, N, TK, RV, false, true><<<grid, strided_threads<N, TK, RV>(), smem_s(), p.stream>>>(
-            d, H, (long long)N * H, 0, H, static_cast<const C*>(p.tw), static_cast<const T*>(p.g1d), cg,
-            p.green_kind, d, ky0);
+            const_cast<C*>(reinterpret_cast<const C*>(in)), H, (long long)N * H, 0, H, static_cast<const C*>(p.tw),
+            static_cast<const T*>(p.g1d), cg, p.green_kind, reinterpret_cast<C*>(out), ky0, nxl);
+    }
+    // y forward of the nx own planes [x][y][kz] of an x-slab, stored as the
+    // rows [ky][x][kz] of its transpose buffer
+    static void y_to_rows(const Plan& p, const T* own, T* rows, int nx) {
+        const dim3 grid((H + TK - 1) / TK, nx);
+        const C* tw = static_cast<const C*>(p.tw);
+        Timed t(p, ST_FFT_Y_FWD);
+        k_fft_strided<T, N, -1, TK, RV, 3><<<grid, strided_threads<N, TK, RV>(), smem_s(), p.stream>>>(
+            const_cast<C*>(reinterpret_cast<const C*>(own)), (long long)nx * H, H, 0, H, tw,
+            reinterpret_cast<C*>(rows));
+    }
+    // y inverse from the rows [ky][x][kz] of an x-slab's transpose buffer
+    // into its nx own planes [x][y][kz]
+    static void y_from_rows(const Plan& p, const T* rows, T* own, int nx) {
+        const dim3 grid((H + TK - 1) / TK, nx);
+        const C* tw = static_cast<const C*>(p.tw);
+        Timed t(p, ST_FFT_Y_INV);
+        k_fft_strided<T, N, +1, TK, RV, 4><<<grid, strided_threads<N, TK, RV>(), smem_s(), p.stream>>>(
+            const_cast<C*>(reinterpret_cast<const C*>(rows)), (long long)nx * H, H, 0, H, tw,
+            reinterpret_cast<C*>(own));
     }
     static constexpr bool kTransposedX = true;
     static void z(const Plan& p, T* mesh, bool forward, int nbox = 1) {
@@ -765,22 +815,24 @@ int poisson_after_z_f32(const Plan& p, float* mesh, double c_poisson, int nbox) 
         }                                                                          \
     })
 
-int slab_fft_forward_y_f32(const Plan& p, float* own, int nx) {
-    PMB_SLAB_LAUNCH(p, L_::y_planes(p, own, -1, nx));
+int slab_fft_forward_y_f32(const Plan& p, const float* own, float* send, int nx) {
+    PMB_SLAB_LAUNCH(p, L_::y_to_rows(p, own, send, nx));
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;
 }
 
-int slab_fft_xgreen_f32(const Plan& p, float* spec, double c_poisson, int nyl, int ky0) {
+int slab_fft_xgreen_f32(const Plan& p, const float* recv, float* send, double c_poisson, int nx, int ky0) {
     const double cg = green_scale(p, c_poisson);
-    PMB_SLAB_LAUNCH(p, L_::xgreen_slab(p, spec, cg, nyl, ky0));
+    int nxl = 0;
+    while ((1 << nxl) < nx) ++nxl;
+    PMB_SLAB_LAUNCH(p, L_::xgreen_slab(p, recv, send, cg, ky0, nxl));
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;
 }
 
-int slab_fft_backward_f32(const Plan& p, float* own, int nx) {
+int slab_fft_backward_f32(const Plan& p, const float* recv, float* own, int nx) {
     PMB_SLAB_LAUNCH(p, {
-        L_::y_planes(p, own, +1, nx);
+        L_::y_from_rows(p, recv, own, nx);
         L_::z_rows(p, own, false, (long long)nx * N_);
     });
     PMB_CUDA_CHECK(cudaGetLastError());

@@ -426,7 +426,7 @@ __global__ void __launch_bounds__(256, 4) k_interp_f32(const float* __restrict__
 // below and three above (buffer plane = x - x0 + 2); a particle outside the
 // slab is recorded in *err and clamped into it.
 template <int ORDER, bool POW2, bool SLAB = false>
-__global__ void __launch_bounds__(256, SLAB ? 3 : 4) k_kick_drift_f32(const float* __restrict__ phi, uint32_t* __restrict__ cell,
+__global__ void __launch_bounds__(256, 4) k_kick_drift_f32(const float* __restrict__ phi, uint32_t* __restrict__ cell,
                                  float* __restrict__ ox, float* __restrict__ oy, float* __restrict__ oz,
                                  float* __restrict__ vx, float* __restrict__ vy, float* __restrict__ vz,
                                  long long np, float c_kick, double dt, int n,
@@ -435,6 +435,7 @@ __global__ void __launch_bounds__(256, SLAB ? 3 : 4) k_kick_drift_f32(const floa
                                  int x0 = 0, int nxl = 0, int* __restrict__ err = nullptr) {
     const long long lo = pbeg ? pbeg[blockIdx.y] : 0, hi = pbeg ? pend[blockIdx.y] : np;
     if (pbeg) phi += blockIdx.y * mesh_stride;
+    bool outside = false;
     for (long long p = lo + blockIdx.x * (long long)blockDim.x + threadIdx.x; p < hi;
          p += (long long)gridDim.x * blockDim.x) {
         // the particle arrays are touched once per step: streaming (evict-
@@ -446,11 +447,8 @@ __global__ void __launch_bounds__(256, SLAB ? 3 : 4) k_kick_drift_f32(const floa
         const float tx = __ldcs(ox + p), ty = __ldcs(oy + p), tz = __ldcs(oz + p);
         float gx, gy, gz;
         if constexpr (SLAB) {
-            int li = (i & (n - 1)) - x0;
-            if (li < 0 || li >= nxl) {
-                atomicOr(err, ERRBIT_RANGE);
-                li = li < 0 ? 0 : nxl - 1;
-            }
+            const int li0 = (i & (n - 1)) - x0, li = min(max(li0, 0), nxl - 1);
+            outside |= li != li0;
             force_at<ORDER, POW2, true>(phi, n, li + 2, j, k, tx, ty, tz, gx, gy, gz);
             i = li + x0;  // the drift below starts from the (clamped) cell
         } else {
@@ -473,6 +471,7 @@ __global__ void __launch_bounds__(256, SLAB ? 3 : 4) k_kick_drift_f32(const floa
             __stcs(oz + p, qc);
         }
     }
+    if (SLAB && outside) atomicOr(err, ERRBIT_RANGE);
 }
 
 // ---------------------------------------- tiled gather + kick + drift

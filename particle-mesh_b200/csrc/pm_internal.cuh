@@ -223,9 +223,11 @@ int kick_drift_f32(const Plan& p, const float* phi, uint32_t* cell, float* ox, f
 int slab_deposit_zr2c_f32(Plan& p, int x0, int nx, const uint32_t* cell, const float* ox, const float* oy,
                           const float* oz, int64_t np, float mass, float* mesh);
 int slab_rank_sort(Plan& p, int nranks, int nx, const uint32_t* cell, int64_t np, int64_t* counts);
-int slab_fft_forward_y_f32(const Plan& p, float* own, int nx);
-int slab_fft_xgreen_f32(const Plan& p, float* spec, double c_poisson, int nyl, int ky0);
-int slab_fft_backward_f32(const Plan& p, float* own, int nx);
+// x-slab FFT passes that read / write the transpose buffers directly (rows
+// [ky][x][kz] after the y forward; blocks [rank][kyl][x][kz] around x + Green)
+int slab_fft_forward_y_f32(const Plan& p, const float* own, float* send, int nx);
+int slab_fft_xgreen_f32(const Plan& p, const float* recv, float* send, double c_poisson, int nx, int ky0);
+int slab_fft_backward_f32(const Plan& p, const float* recv, float* own, int nx);
 int slab_kick_drift_f32(const Plan& p, int x0, int nx, const float* phi, uint32_t* cell, float* ox, float* oy,
                         float* oz, float* vx, float* vy, float* vz, int64_t np, double c_kick, double dt);
 int plan_create_internal(int ng, int precision, int green_kind, int grad_order, void* stream, pm_plan** out);

@@ -11,13 +11,16 @@
 //   deposit      the slab's particles, fused with the z R2C, into its own
 //                planes plus one ghost plane (the +1 corners of its last
 //                plane), which the next slab adds to its first plane;
-//   y forward    over the own planes, then rows packed [ky][x][kz] so that
-//                each destination's ky range is contiguous;
+//   y forward    over the own planes, stored as rows [ky][x][kz] of the
+//                send buffer so that each destination's ky range is
+//                contiguous;
 //   (all-to-all) the global transpose;
-//   x + Green    rows unpacked to [ky][kx][kz], x forward, Green, x inverse
-//                along the middle axis, rows packed back [x owner][ky][x];
+//   x + Green    x lines read across the received blocks [rank][kyl][x][kz],
+//                x forward, Green, x inverse, written into the same layout
+//                of the send buffer (block d back to rank d);
 //   (all-to-all) the transpose back;
-//   y inverse, z C2R over the own planes;
+//   y inverse    read from the received rows [ky][x][kz], written into
+//                the own planes; z C2R over them;
 //   (halo)       two planes from the previous slab, three from the next
 //                (the 4-point stencil reaches x - 2 .. x + 3);
 //   gather + kick + drift, then particles that left the slab migrate to
@@ -35,53 +38,6 @@
 namespace pmb {
 
 namespace {
-
-// Row permutations of a slab's share of the half spectrum (rows of H
-// complex, one warp per row, coalesced).  nx = ng / P own x planes, nyl =
-// ng / P ky planes after the transpose, P = ng / nx ranks.
-enum : int { ROWS_PACK_FWD = 0, ROWS_UNPACK_X = 1, ROWS_PACK_X = 2, ROWS_UNPACK_BACK = 3 };
-
-__device__ __forceinline__ long long slab_dst_row(long long row, int mode, int ng, int nx) {
-    const int nyl = nx;
-    switch (mode) {
-        case ROWS_PACK_FWD: {  // [x][ky] -> [ky][x]
-            const long long xl = row / ng, ky = row % ng;
-            return ky * nx + xl;
-        }
-        case ROWS_UNPACK_X: {  // [src][kyl][x] -> [kyl][src x0 + x]
-            const long long xl = row % nx, t = row / nx, kyl = t % nyl, src = t / nyl;
-            return kyl * ng + src * nx + xl;
-        }
-        case ROWS_PACK_X: {  // [kyl][kx] -> [owner of kx][kyl][kx - x0]
-            const long long kx = row % ng, kyl = row / ng;
-            return ((kx / nx) * nyl + kyl) * nx + kx % nx;
-        }
-        default: {  // [ky][x] -> [x][ky]
-            const long long xl = row % nx, ky = row / nx;
-            return xl * ng + ky;
-        }
-    }
-}
-
-__global__ void k_slab_rows(const float2* __restrict__ src, float2* __restrict__ dst, long long nrows, int h,
-                            int mode, int ng, int nx) {
-    const int lane = threadIdx.x & 31;
-    const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long row = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; row < nrows; row += warps) {
-        const float2* s = src + row * h;
-        float2* d = dst + slab_dst_row(row, mode, ng, nx) * h;
-        // eight loads in flight per lane, then the stores
-        for (int e0 = lane; e0 < h; e0 += 32 * 8) {
-            float2 v[8];
-#pragma unroll
-            for (int u = 0; u < 8; ++u)
-                if (e0 + 32 * u < h) v[u] = __ldcs(s + e0 + 32 * u);
-#pragma unroll
-            for (int u = 0; u < 8; ++u)
-                if (e0 + 32 * u < h) d[e0 + 32 * u] = v[u];
-        }
-    }
-}
 
 // plane += ghost over one padded plane of ng (ng + 2) floats (float2 pairs).
 __global__ void k_fold_plane(float2* __restrict__ plane, const float2* __restrict__ ghost, long long n2) {
@@ -124,15 +80,6 @@ struct Slab {
     float* own() const { return buf + 2 * plane_floats(); }
     long long rows() const { return (long long)nx * ng; }
 };
-
-static int slab_rows(const Slab& s, const float2* src, float2* dst, int mode) {
-    const Plan& p = s.plan->p;
-    const int h = s.ng / 2 + 1;
-    const long long rows = s.rows();
-    k_slab_rows<<<grid_for(p, rows * 32, 256, 8), 256, 0, p.stream>>>(src, dst, rows, h, mode, s.ng, s.nx);
-    PMB_CUDA_CHECK(cudaGetLastError());
-    return PM_OK;
-}
 
 static void slab_release(Slab& s) {
     if (s.buf) cudaFree(s.buf);
@@ -302,35 +249,27 @@ int pm_slab_fold_f32(pm_slab* slab, const float* ghost) {
     return PM_OK;
 }
 
+// The row permutations of the transposes are folded into the FFT passes'
+// loads and stores: the y forward writes the rows [ky][x][kz] of `send`, the
+// x + Green pass reads the received blocks and writes the ones to send back,
+// the y inverse reads the received rows (no separate copy of the spectrum).
 int pm_slab_forward_f32(pm_slab* slab) {
     PM_TRY_S(slab_ok(slab));
     Slab& s = slab->s;
-    PM_TRY_S(slab_fft_forward_y_f32(s.plan->p, s.own(), s.nx));
-    Timed t(s.plan->p, ST_SORT);
-    return slab_rows(s, reinterpret_cast<const float2*>(s.own()), s.send, ROWS_PACK_FWD);
+    return slab_fft_forward_y_f32(s.plan->p, s.own(), reinterpret_cast<float*>(s.send), s.nx);
 }
 
 int pm_slab_xgreen_f32(pm_slab* slab, double c_poisson) {
     PM_TRY_S(slab_ok(slab));
     Slab& s = slab->s;
-    float2* x = reinterpret_cast<float2*>(s.own());  // the own planes are free between the transposes
-    {
-        Timed t(s.plan->p, ST_SORT);
-        PM_TRY_S(slab_rows(s, s.recv, x, ROWS_UNPACK_X));
-    }
-    PM_TRY_S(slab_fft_xgreen_f32(s.plan->p, s.own(), c_poisson, s.nyl, s.ky0));
-    Timed t(s.plan->p, ST_SORT);
-    return slab_rows(s, x, s.send, ROWS_PACK_X);
+    return slab_fft_xgreen_f32(s.plan->p, reinterpret_cast<const float*>(s.recv), reinterpret_cast<float*>(s.send),
+                               c_poisson, s.nx, s.ky0);
 }
 
 int pm_slab_backward_f32(pm_slab* slab) {
     PM_TRY_S(slab_ok(slab));
     Slab& s = slab->s;
-    {
-        Timed t(s.plan->p, ST_SORT);
-        PM_TRY_S(slab_rows(s, s.recv, reinterpret_cast<float2*>(s.own()), ROWS_UNPACK_BACK));
-    }
-    return slab_fft_backward_f32(s.plan->p, s.own(), s.nx);
+    return slab_fft_backward_f32(s.plan->p, reinterpret_cast<const float*>(s.recv), s.own(), s.nx);
 }
 
 int pm_slab_kick_drift_f32(pm_slab* slab, uint32_t* cell, float* ox, float* oy, float* oz, float* vx, float* vy,
