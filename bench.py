@@ -425,11 +425,18 @@ def ours_slab(args, pm, torch, dist, world, rank, dev, stream, barrier, max_over
     # algorithmic bytes of this rank's share: the single-box byte model scaled
     # by the slab's share of the mesh and of the particles
     share = 1.0 / world
-    dom_bytes = stage_bytes(dom, ng, np_, 4) * share if dom in ("deposit", "kick_drift", "bin") or \
-        dom.startswith("fft_") else None
-    dom_ms = stages[dom][0] / args.steps
+    if args.pencil and dom == "sort":
+        # the pencil's staging copies: own rows out of / back into the halo
+        # buffer and the kz chunks packed / unpacked, each a read and a write
+        # of the rank's half-spectrum share (4 per step)
+        dom_bytes = 4 * 2 * ng * ng * (ng + 2) * 4 * share
+    else:
+        dom_bytes = stage_bytes(dom, ng, np_, 4) * share if dom in ("deposit", "kick_drift", "bin") or \
+            dom.startswith("fft_") else None
+    dom_ms = stages[dom][0] / args.steps  # per step (bytes per step likewise)
     roofline = {"bound": "hbm", "kernel": dom, "peak": peak, "unit": "GB/s",
                 "peak_source": f"{peak_kind} hbm_gbs (copy bandwidth)", "ms_per_launch": dom_ms,
+                "launches_per_step": stages[dom][1] / args.steps,
                 "achieved": dom_bytes / (dom_ms / 1e3) / 1e9 if dom_bytes else None,
                 "frac": dom_bytes / (dom_ms / 1e3) / 1e9 / peak if dom_bytes else None, "traffic": None,
                 "note": f"per rank; the byte model of one box times the {'pencil' if args.pencil else 'slab'}'s "

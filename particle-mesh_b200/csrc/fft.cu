@@ -197,6 +197,34 @@ k_fft_strided(typename Cx<T>::t* __restrict__ data, long long es_, long long os_
         pass2_twiddles<DIR, (R2 >= 16 && sizeof(T) == 4)>(tw, ty));
 }
 
+// Lines of N complex read from `in` and written to `out` through line maps
+// (plane blockIdx.y, columns [bx TK, bx TK + TK) consecutive): the y passes
+// of a pencil, reading the blocks one transpose delivered and writing the
+// blocks the next one sends.
+template <typename T, int N, int DIR, int TK, int RV = 0>
+__global__ void __launch_bounds__(strided_threads<N, TK, RV>(), 2)
+k_fft_lines_map(const typename Cx<T>::t* __restrict__ in, typename Cx<T>::t* __restrict__ out, LineMap mi,
+                LineMap mo, int ncols, const typename Cx<T>::t* __restrict__ tw) {
+    using C = typename Cx<T>::t;
+    constexpr int R1 = RadixV<N, RV>::R1, R2 = RadixV<N, RV>::R2;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* S = reinterpret_cast<C*>(smraw);
+    const int tx = threadIdx.x % TK, ty = threadIdx.x / TK;
+    const int col = blockIdx.x * TK + tx;
+    const bool active = col < ncols;
+    const C* ib = in + (long long)blockIdx.y * mi.ps + (active ? col : 0);
+    C* ob = out + (long long)blockIdx.y * mo.ps + (active ? col : 0);
+    using I = SIdx<R1, R2, TK>;
+    stockham_pass1<R1, R2, DIR, false, C>(
+        ty, [&](int j, int r) { return active ? ib[lm_off(mi, j + r * R2)] : cmake<C>(0, 0); },
+        [&](int j, int k, C v) { S[I::out1(j, k, tx)] = v; });
+    __syncthreads();
+    stockham_pass2<R1, R2, DIR, false, C>(
+        ty, [&](int j, int r) { return S[I::p2(j, r, tx)]; },
+        [&](int j, int k, C v) { if (active) ob[lm_off(mo, j + k * R1)] = v; },
+        pass2_twiddles<DIR, (R2 >= 16 && sizeof(T) == 4)>(tw, ty));
+}
+
 // Green's function times c / N^3 (cg = c / N^3) at (kx, ky, kz).
 //   FP64 discrete: -cg / (2 (3 - cos - cos - cos)), the reference's own
 //     expression (src/fft/fftw/fft.cpp:55) on the rounded cosines.
@@ -227,17 +255,17 @@ __device__ __forceinline__ T green_value(int kx, int ky, int kz, int kind, doubl
 // written to `out` in the transposed layout [ky][kx][kz] (element stride H),
 // so that neither this pass nor the next one both reads and writes lines
 // whose elements lie N H apart; otherwise in place.
-// SLABX: the x lines of one x-slab's share of the spectrum straight from the
-// transpose buffer `data` into the one to send back, `out`: plane blockIdx.y
-// holds ky = ky0 + blockIdx.y, and element kx of a line lies at
-// (kx >> nxl) nx^2 H + (kx & (nx - 1)) H from the plane's start
-// blockIdx.y nx H (nx = 2^nxl planes per slab; rank kx / nx's block of
-// [ky][x][kz] rows), in both buffers.
+// SLABX: the x lines of a decomposed mesh's share of the spectrum, read
+// from the received transpose buffer `data` and written to the one to send
+// back, `out`, both through the line map `lm` (plane blockIdx.y holds
+// ky = ky0 + blockIdx.y, column c holds kz = kz0 + c).  An x-slab's blocks
+// [rank][kyl][x][kz] map kx to (kx >> log2 nx) nx^2 H + (kx & (nx - 1)) H; a
+// pencil's [kx][kyl][kz] to kx yc hc.
 template <typename T, int N, int TK, int RV = 0, bool XT = false, bool SLABX = false>
 __global__ void __launch_bounds__(strided_threads<N, TK, RV>(), 2)
 k_fft_x_green(typename Cx<T>::t* __restrict__ data, long long es_, long long os_, long long bs, int ncols,
               const typename Cx<T>::t* __restrict__ tw, const T* __restrict__ g1d, double cg, int kind,
-              typename Cx<T>::t* out, int ky0 = 0, int nxl = 0) {
+              typename Cx<T>::t* out, int ky0 = 0, LineMap lm = LineMap{}, int kz0 = 0) {
     using C = typename Cx<T>::t;
     constexpr int R1 = RadixV<N, RV>::R1, R2 = RadixV<N, RV>::R2;
     // x lines of the padded spectrum: compile-time strides (es_ = N H and
@@ -254,13 +282,10 @@ k_fft_x_green(typename Cx<T>::t* __restrict__ data, long long es_, long long os_
     const int col = blockIdx.x * TK + tx;
     const bool active = col < ncols;
     const int ky = SLABX ? ky0 + (int)blockIdx.y : (int)(blockIdx.y % N);
-    constexpr int H = N / 2 + 1;
-    // (SLABX offsets fit 32 bits: nx^2 H * (N / nx) <= N^2 H < 2^31)
-    const int nmask = (1 << nxl) - 1, sstride = (1 << (2 * nxl)) * H;
-    auto soff = [&](int n) { return (n >> nxl) * sstride + (n & nmask) * H; };
-    C* base = SLABX ? data + (long long)blockIdx.y * ((long long)H << nxl) + (active ? col : 0)
+    auto soff = [&](int n) { return lm_off(lm, n); };
+    C* base = SLABX ? data + (long long)blockIdx.y * lm.ps + (active ? col : 0)
                     : data + (long long)(blockIdx.y / N) * bs + (long long)ky * os + (active ? col : 0);
-    C* obase = SLABX ? out + (long long)blockIdx.y * ((long long)H << nxl) + (active ? col : 0)
+    C* obase = SLABX ? out + (long long)blockIdx.y * lm.ps + (active ? col : 0)
                      : (XT ? out + (long long)(blockIdx.y / N) * bs + (long long)ky * oos + (active ? col : 0) : base);
 
     using I = SIdx<R1, R2, TK>;
@@ -277,7 +302,8 @@ k_fft_x_green(typename Cx<T>::t* __restrict__ data, long long es_, long long os_
     stockham_pass2<R1, R2, -1, true, C>(
         ty, p2ld,
         [&](int j, int k, C v) {
-            S[I::p2(j, k, tx)] = cscale(v, active ? green_value<T>(j + k * R1, ky, col, kind, cg, tw, g1d) : (T)0);
+            S[I::p2(j, k, tx)] =
+                cscale(v, active ? green_value<T>(j + k * R1, ky, col + kz0, kind, cg, tw, g1d) : (T)0);
         },
         pass2_twiddles<-1, kSplitTw>(tw, ty));
     __syncthreads();
@@ -477,8 +503,8 @@ template <typename T, int N, int TK = tk_cols<T, N>(), int RV = 0> struct Launch
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, +1, TK, RV, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, -1, TK, RV, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, +1, TK, RV, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
-        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, -1, TK, RV, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
-        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, +1, TK, RV, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
+        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_lines_map<T, N, -1, TK, RV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
+        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_lines_map<T, N, +1, TK, RV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_x_green<T, N, TK, RV, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         return PM_OK;
     }
@@ -508,30 +534,30 @@ template <typename T, int N, int TK = tk_cols<T, N>(), int RV = 0> struct Launch
             k_fft_strided<T, N, +1, TK, RV, 1><<<grid, strided_threads<N, TK, RV>(), smem_s(), p.stream>>>(
                 d, H, (long long)N * H, 0, H, tw, d);
     }
-    // x forward + Green + x inverse over `planes` ky planes [ky - ky0][kx][kz]
-    // lines of N complex at runtime element stride es: `planes` planes at
-    // stride os, ncols columns (consecutive) per plane; every plane < N
-    static void strided_rt(const Plan& p, T* data, long long es, long long os, int planes, int ncols, int dir,
-                           int stage) {
-        C* d = reinterpret_cast<C*>(data);
+    // lines through line maps (pencil y passes)
+    static void lines_map(const Plan& p, const T* in, T* out, LineMap mi, LineMap mo, int planes, int ncols, int dir,
+                          int stage) {
         const dim3 grid((ncols + TK - 1) / TK, planes);
         const C* tw = static_cast<const C*>(p.tw);
+        const C* i = reinterpret_cast<const C*>(in);
+        C* o = reinterpret_cast<C*>(out);
         Timed t(p, stage);
         if (dir < 0)
-            k_fft_strided<T, N, -1, TK, RV, -1><<<grid, strided_threads<N, TK, RV>(), smem_s(), p.stream>>>(
-                d, es, os, 0, ncols, tw, d);
+            k_fft_lines_map<T, N, -1, TK, RV><<<grid, strided_threads<N, TK, RV>(), smem_s(), p.stream>>>(
+                i, o, mi, mo, ncols, tw);
         else
-            k_fft_strided<T, N, +1, TK, RV, -1><<<grid, strided_threads<N, TK, RV>(), smem_s(), p.stream>>>(
-                d, es, os, 0, ncols, tw, d);
+            k_fft_lines_map<T, N, +1, TK, RV><<<grid, strided_threads<N, TK, RV>(), smem_s(), p.stream>>>(
+                i, o, mi, mo, ncols, tw);
     }
-    // x forward + Green + x inverse of an x-slab's nx = 2^nxl ky planes,
-    // from the received transpose buffer into the one to send back
-    static void xgreen_slab(const Plan& p, const T* in, T* out, double cg, int ky0, int nxl) {
-        const dim3 grid((H + TK - 1) / TK, 1 << nxl);
+    // x forward + Green + x inverse of `planes` ky planes (ky0 + plane) and
+    // ncols kz columns (kz0 + column) through the line map m, from `in` to `out`
+    static void xgreen_map(const Plan& p, const T* in, T* out, double cg, LineMap m, int planes, int ncols, int ky0,
+                           int kz0) {
+        const dim3 grid((ncols + TK - 1) / TK, planes);
         Timed t(p, ST_FFT_X_GREEN);
         k_fft_x_green<T, N, TK, RV, false, true><<<grid, strided_threads<N, TK, RV>(), smem_s(), p.stream>>>(
-            const_cast<C*>(reinterpret_cast<const C*>(in)), H, (long long)N * H, 0, H, static_cast<const C*>(p.tw),
-            static_cast<const T*>(p.g1d), cg, p.green_kind, reinterpret_cast<C*>(out), ky0, nxl);
+            const_cast<C*>(reinterpret_cast<const C*>(in)), H, (long long)N * H, 0, ncols, static_cast<const C*>(p.tw),
+            static_cast<const T*>(p.g1d), cg, p.green_kind, reinterpret_cast<C*>(out), ky0, m, kz0);
     }
     // y forward of the nx own planes [x][y][kz] of an x-slab, stored as the
     // rows [ky][x][kz] of its transpose buffer
@@ -825,7 +851,10 @@ int slab_fft_xgreen_f32(const Plan& p, const float* recv, float* send, double c_
     const double cg = green_scale(p, c_poisson);
     int nxl = 0;
     while ((1 << nxl) < nx) ++nxl;
-    PMB_SLAB_LAUNCH(p, L_::xgreen_slab(p, recv, send, cg, ky0, nxl));
+    const int H = p.ng / 2 + 1;
+    // rank kx / nx's block [kyl][x][kz]: (nx^2 H * (ng / nx) <= ng^2 H < 2^31)
+    const LineMap m{(long long)nx * H, nx * nx * H, H, nxl, nx - 1};
+    PMB_SLAB_LAUNCH(p, L_::xgreen_map(p, recv, send, cg, m, nx, H, ky0, 0));
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;
 }
@@ -840,61 +869,55 @@ int slab_fft_backward_f32(const Plan& p, const float* recv, float* own, int nx) 
 }
 
 // ---------------------------------------------- pencil decomposition
-// The FFT passes of one pencil (x range nx, y range ny, all z) of a
-// power-of-two FP32 mesh, on the pencil's buffers between the transposes:
-//   y stage  [nx][ng][hc]  y lines (element stride hc), one kz chunk of hc
-//   x stage  [ng][yc][hc]  x lines (element stride yc hc), yc ky planes
-// and the Green multiply of the x stage at global (kx, ky0 + y, kz0 + kz).
-__global__ void k_green_pencil(float2* __restrict__ spec, int ng, int yc, int hc, int ky0, int kz0,
-                               const float2* __restrict__ tw, const float* __restrict__ g1d, double cg, int kind) {
-    const long long n = (long long)ng * yc * hc;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
-        const int kz = (int)(e % hc);
-        const long long t = e / hc;
-        const int ky = (int)(t % yc), kx = (int)(t / yc);
-        spec[e] = cscale(spec[e], green_value<float>(kx, ky0 + ky, kz0 + kz, kind, cg, tw, g1d));
-    }
-}
-
 // dst block [a][b][c] (strides da, db, 1) <- src block (strides sa, sb, 1),
-// complex elements; one thread per element of the c axis, coalesced.
+// complex elements, one warp per (a, b) row with eight loads in flight per
+// lane.  bg: subtracted from both halves of every element but a row's last
+// (the density contrast's -1 background of the real rows; their last
+// element is the z padding).
 __global__ void k_copy3(const float2* __restrict__ src, long long sa, long long sb, float2* __restrict__ dst,
-                        long long da, long long db, int A, int B, int Cn) {
-    const long long rows = (long long)A * B;
-    for (long long r = blockIdx.y; r < rows; r += gridDim.y) {
-        const long long a = r / B, b = r % B;
+                        long long da, long long db, int B, long long rows, int Cn, float bg) {
+    const int lane = threadIdx.x & 31;
+    const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long r = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; r < rows; r += warps) {
+        const long long a = r / B, b = r - a * B;
         const float2* s = src + a * sa + b * sb;
         float2* d = dst + a * da + b * db;
-        for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < Cn; c += gridDim.x * blockDim.x) d[c] = s[c];
+        for (int e0 = lane; e0 < Cn; e0 += 32 * 8) {
+            float2 v[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                if (e0 + 32 * u < Cn) v[u] = __ldcs(s + e0 + 32 * u);
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int c = e0 + 32 * u;
+                if (c < Cn) d[c] = c < Cn - 1 ? make_float2(v[u].x - bg, v[u].y - bg) : v[u];
+            }
+        }
     }
 }
 
 int pencil_copy3(const Plan& p, const float2* src, long long sa, long long sb, float2* dst, long long da,
-                 long long db, int A, int B, int C) {
-    if ((long long)A * B * C == 0) return PM_OK;
-    const unsigned gx = (unsigned)((C + 255) / 256);
+                 long long db, int A, int B, int C, float bg) {
     const long long rows = (long long)A * B;
-    const unsigned gy = (unsigned)(rows < 65535 ? rows : 65535);
-    k_copy3<<<dim3(gx, gy), 256, 0, p.stream>>>(src, sa, sb, dst, da, db, A, B, C);
+    if (rows * C == 0) return PM_OK;
+    k_copy3<<<grid_for(p, rows * 32, 256, 8), 256, 0, p.stream>>>(src, sa, sb, dst, da, db, B, rows, C, bg);
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;
 }
 
-int pencil_fft_lines_f32(const Plan& p, float* data, long long es, long long os, int planes, int ncols, int dir,
-                         int stage) {
-    PMB_SLAB_LAUNCH(p, L_::strided_rt(p, data, es, os, planes, ncols, dir, stage));
+int pencil_lines_f32(const Plan& p, const float* in, float* out, LineMap mi, LineMap mo, int planes, int ncols,
+                     int dir, int stage) {
+    if (planes <= 0 || ncols <= 0) return PM_OK;
+    PMB_SLAB_LAUNCH(p, L_::lines_map(p, in, out, mi, mo, planes, ncols, dir, stage));
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;
 }
 
-int pencil_green_f32(const Plan& p, float* spec, int yc, int hc, int ky0, int kz0, double c_poisson) {
-    const long long n = (long long)p.ng * yc * hc;
-    {
-        Timed t(p, ST_GREEN);
-        k_green_pencil<<<grid_for(p, n, 256, 8), 256, 0, p.stream>>>(
-            reinterpret_cast<float2*>(spec), p.ng, yc, hc, ky0, kz0, static_cast<const float2*>(p.tw),
-            static_cast<const float*>(p.g1d), green_scale(p, c_poisson), p.green_kind);
-    }
+int pencil_xgreen_f32(const Plan& p, const float* in, float* out, LineMap m, int planes, int ncols, double c_poisson,
+                      int ky0, int kz0) {
+    if (planes <= 0 || ncols <= 0) return PM_OK;
+    const double cg = green_scale(p, c_poisson);
+    PMB_SLAB_LAUNCH(p, L_::xgreen_map(p, in, out, cg, m, planes, ncols, ky0, kz0));
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;
 }

@@ -604,20 +604,9 @@ k_kick_drift_tiles(const float* __restrict__ phi, uint32_t* __restrict__ cell, f
 
 // ------------------------------------------------ pencil decomposition
 // One pencil (x in [x0, x0 + nx), y in [y0, y0 + ny), all z) with its halo
-// rows: buffer [nx + 5][ny + 5][n + 2], row (x - x0 + 2, y - y0 + 2).
-// Every row to 0, the own rows' cells to -1 (the density contrast's
-// background); padding 0.
-__global__ void k_pencil_init(float* __restrict__ buf, int nx, int ny, int n) {
-    const long long pz = n + 2, rows = (long long)(nx + 5) * (ny + 5);
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < rows * pz;
-         e += (long long)gridDim.x * blockDim.x) {
-        const long long r = e / pz;
-        const int z = (int)(e - r * pz), xl = (int)(r / (ny + 5)), yl = (int)(r % (ny + 5));
-        const bool own = xl >= 2 && xl < nx + 2 && yl >= 2 && yl < ny + 2;
-        buf[e] = (own && z < n) ? -1.0f : 0.0f;
-    }
-}
-
+// rows: buffer [nx + 5][ny + 5][n + 2], row (x - x0 + 2, y - y0 + 2), zeroed
+// before the deposit (the -1 background is added when the own rows are
+// copied out for the z FFT).
 // CIC deposit of the pencil's particles into its buffer with shared-nothing
 // FP32 atomics: the +1 corners of the last x plane / y row land in the ghost
 // rows x = nx (buffer row nx + 2) and y = ny, which the neighbours fold.  A
@@ -997,11 +986,7 @@ int slab_kick_drift_f32(const Plan& p, int x0, int nx, const float* phi, uint32_
 
 int pencil_deposit_f32(const Plan& p, int x0, int y0, int nx, int ny, const uint32_t* cell, const float* ox,
                        const float* oy, const float* oz, int64_t np, float mass, float* buf) {
-    const long long n = (long long)(nx + 5) * (ny + 5) * (p.ng + 2);
-    {
-        Timed t(p, ST_MESH_INIT);
-        k_pencil_init<<<grid_for(p, n, kThreads, 8), kThreads, 0, p.stream>>>(buf, nx, ny, p.ng);
-    }
+    PMB_CUDA_CHECK(cudaMemsetAsync(buf, 0, (size_t)(nx + 5) * (ny + 5) * (p.ng + 2) * sizeof(float), p.stream));
     if (np > 0) {
         Timed t(p, ST_DEPOSIT);
         k_pencil_deposit<<<grid_for(p, np, kThreads, 8), kThreads, 0, p.stream>>>(cell, ox, oy, oz, np, mass, buf, x0,

@@ -103,6 +103,15 @@ struct TileScratch {
     int64_t np_cap = 0;
 };
 
+// Where the FFT passes of a decomposed mesh find the elements of a line in
+// the transpose buffers: element n of the line of plane p at complex offset
+// p * ps + (n >> sl) * s1 + (n & mask) * s0 (the element term below 2^31).
+struct LineMap {
+    long long ps = 0;
+    int s1 = 0, s0 = 0, sl = 0, mask = 0;
+};
+__host__ __device__ __forceinline__ int lm_off(const LineMap& m, int n) { return (n >> m.sl) * m.s1 + (n & m.mask) * m.s0; }
+
 // ---------------------------------------------------------------- the plan
 struct Plan {
     int ng = 0;
@@ -234,10 +243,13 @@ int plan_create_internal(int ng, int precision, int green_kind, int grad_order, 
 // pencil decomposition (tiles.cu, fft.cu, particles.cu, slab.cu)
 int pencil_rank_sort(Plan& p, int px, int py, int nx, int ny, const uint32_t* cell, int64_t np, int64_t* counts);
 int pencil_copy3(const Plan& p, const float2* src, long long sa, long long sb, float2* dst, long long da, long long db,
-                 int A, int B, int C);
-int pencil_fft_lines_f32(const Plan& p, float* data, long long es, long long os, int planes, int ncols, int dir,
-                         int stage);
-int pencil_green_f32(const Plan& p, float* spec, int yc, int hc, int ky0, int kz0, double c_poisson);
+                 int A, int B, int C, float bg = 0.0f);
+// y lines read / written through line maps; x + Green (kz = kz0 + column,
+// ky = ky0 + plane) from `in` to `out` through one map
+int pencil_lines_f32(const Plan& p, const float* in, float* out, LineMap mi, LineMap mo, int planes, int ncols,
+                     int dir, int stage);
+int pencil_xgreen_f32(const Plan& p, const float* in, float* out, LineMap m, int planes, int ncols, double c_poisson,
+                      int ky0, int kz0);
 int pencil_z_f32(const Plan& p, float* rows, long long nrows, bool forward);
 int pencil_deposit_f32(const Plan& p, int x0, int y0, int nx, int ny, const uint32_t* cell, const float* ox,
                        const float* oy, const float* oz, int64_t np, float mass, float* buf);

@@ -100,10 +100,9 @@ struct Pencil {
     int ng = 0, px = 1, py = 1, rank = 0, rx = 0, ry = 0, nx = 0, ny = 0, x0 = 0, y0 = 0, yc = 0, h = 0;
     float* halo = nullptr;  // [nx + 5][ny + 5][ng + 2]
     float2* own = nullptr;  // [nx][ny][h]
-    float2* work = nullptr;  // [nx][ng][hc] (y stage)
     float2* send = nullptr;
     float2* recv = nullptr;
-    long long xfer = 0;  // complex entries of each of work / send / recv
+    long long xfer = 0;  // complex entries of each of send / recv
     size_t bytes = 0;
     int kb(int c) const { return (int)((long long)c * h / py); }
     int hc(int c) const { return kb(c + 1) - kb(c); }
@@ -113,7 +112,7 @@ struct Pencil {
 };
 
 static void pencil_release(Pencil& q) {
-    for (void* b : {(void*)q.halo, (void*)q.own, (void*)q.work, (void*)q.send, (void*)q.recv})
+    for (void* b : {(void*)q.halo, (void*)q.own, (void*)q.send, (void*)q.recv})
         if (b) cudaFree(b);
     if (q.plan) pm_plan_destroy(q.plan);
     q = Pencil{};
@@ -381,14 +380,14 @@ int pm_pencil_create(int ng, int px, int py, int rank, int green_kind, int grad_
     const size_t haloB = (size_t)(q.nx + 5) * (q.ny + 5) * (ng + 2) * sizeof(float);
     const size_t ownB = (size_t)q.nx * q.ny * q.h * sizeof(float2), xB = (size_t)q.xfer * sizeof(float2);
     if (cudaMalloc(&q.halo, haloB) != cudaSuccess || cudaMalloc(&q.own, ownB) != cudaSuccess ||
-        cudaMalloc(&q.work, xB) != cudaSuccess || cudaMalloc(&q.send, xB) != cudaSuccess ||
-        cudaMalloc(&q.recv, xB) != cudaSuccess || cudaMemset(q.halo, 0, haloB) != cudaSuccess) {
+        cudaMalloc(&q.send, xB) != cudaSuccess || cudaMalloc(&q.recv, xB) != cudaSuccess ||
+        cudaMemset(q.halo, 0, haloB) != cudaSuccess) {
         cudaGetLastError();
         pencil_release(q);
         delete pen;
         return fail(PM_ERR_NOMEM, "pencil buffer allocation failed");
     }
-    q.bytes = haloB + ownB + 3 * xB;
+    q.bytes = haloB + ownB + 2 * xB;
     *out = pen;
     return PM_OK;
 }
@@ -462,7 +461,8 @@ int pm_pencil_forward_f32(pm_pencil* pen) {
     const long long H = q.h, ny = q.ny, nx = q.nx;
     {
         Timed t(p, ST_SORT);
-        PM_TRY_S(pencil_copy3(p, q.halo_c() + q.hrow(2, 2), (ny + 5) * H, H, q.own, ny * H, H, q.nx, q.ny, q.h));
+        // own rows into the compact buffer, with the density contrast's -1
+        PM_TRY_S(pencil_copy3(p, q.halo_c() + q.hrow(2, 2), (ny + 5) * H, H, q.own, ny * H, H, q.nx, q.ny, q.h, 1.0f));
     }
     PM_TRY_S(pencil_z_f32(p, reinterpret_cast<float*>(q.own), nx * ny, true));
     Timed t(p, ST_SORT);
@@ -472,56 +472,49 @@ int pm_pencil_forward_f32(pm_pencil* pen) {
     return PM_OK;
 }
 
+static int log2i(int v) {
+    int l = 0;
+    while ((1 << l) < v) ++l;
+    return l;
+}
+
+// The y passes read the blocks a transpose delivered and write the blocks
+// the next one sends, through line maps (no staging copies):
+//   y group blocks [member s][nx][ny][hc]: y = s ny + yl
+//   x group blocks [member d][nx][yc][hc]: ky = d yc + kyl
+// (plane = x, columns = the rank's hc kz planes; offsets below nx ng hc < 2^31).
+static LineMap ymap(const Pencil& q, long long hc) {
+    return LineMap{(long long)q.ny * hc, (int)((long long)q.nx * q.ny * hc), (int)hc, log2i(q.ny), q.ny - 1};
+}
+static LineMap kymap(const Pencil& q, long long hc) {
+    return LineMap{(long long)q.yc * hc, (int)((long long)q.nx * q.yc * hc), (int)hc, log2i(q.yc), q.yc - 1};
+}
+
 int pm_pencil_yfwd_f32(pm_pencil* pen) {
     PM_TRY_S(pencil_ok(pen));
     Pencil& q = pen->q;
-    const Plan& p = q.plan->p;
-    const long long hc = q.hc(q.ry), ng = q.ng, nx = q.nx, ny = q.ny, yc = q.yc;
-    {
-        Timed t(p, ST_SORT);
-        for (int s = 0; s < q.py; ++s)  // [src][nx][ny][hc] -> [nx][ng][hc]
-            PM_TRY_S(pencil_copy3(p, q.recv + (long long)s * nx * ny * hc, ny * hc, hc, q.work + (long long)s * ny * hc,
-                                  ng * hc, hc, q.nx, q.ny, (int)hc));
-    }
-    PM_TRY_S(pencil_fft_lines_f32(p, reinterpret_cast<float*>(q.work), hc, ng * hc, q.nx, (int)hc, -1, ST_FFT_Y_FWD));
-    Timed t(p, ST_SORT);
-    for (int d = 0; d < q.px; ++d)  // ky chunk d: [nx][yc][hc]
-        PM_TRY_S(pencil_copy3(p, q.work + (long long)d * yc * hc, ng * hc, hc, q.send + (long long)d * nx * yc * hc,
-                              yc * hc, hc, q.nx, q.yc, (int)hc));
-    return PM_OK;
+    const long long hc = q.hc(q.ry);
+    return pencil_lines_f32(q.plan->p, reinterpret_cast<const float*>(q.recv), reinterpret_cast<float*>(q.send),
+                            ymap(q, hc), kymap(q, hc), q.nx, (int)hc, -1, ST_FFT_Y_FWD);
 }
 
 int pm_pencil_xgreen_f32(pm_pencil* pen, double c_poisson) {
     PM_TRY_S(pencil_ok(pen));
     Pencil& q = pen->q;
-    const Plan& p = q.plan->p;
-    const long long hc = q.hc(q.ry), yc = q.yc;
-    float* x = reinterpret_cast<float*>(q.recv);  // [src x block][nx][yc][hc] = [ng][yc][hc]
-    PM_TRY_S(pencil_fft_lines_f32(p, x, yc * hc, hc, q.yc, (int)hc, -1, ST_FFT_X_FWD));
-    PM_TRY_S(pencil_green_f32(p, x, q.yc, (int)hc, q.rx * q.yc, q.kb(q.ry), c_poisson));
-    PM_TRY_S(pencil_fft_lines_f32(p, x, yc * hc, hc, q.yc, (int)hc, +1, ST_FFT_X_INV));
-    PMB_CUDA_CHECK(cudaMemcpyAsync(q.send, q.recv, (size_t)q.ng * yc * hc * sizeof(float2), cudaMemcpyDeviceToDevice,
-                                   p.stream));
-    return PM_OK;
+    const long long hc = q.hc(q.ry);
+    // the received blocks [src][nx][yc][hc] are the x lines [kx][kyl][kz]
+    // (element stride yc hc), written to the same layout of send
+    const LineMap m{hc, 0, (int)(q.yc * hc), 30, (1 << 30) - 1};
+    return pencil_xgreen_f32(q.plan->p, reinterpret_cast<const float*>(q.recv), reinterpret_cast<float*>(q.send), m,
+                             q.yc, (int)hc, c_poisson, q.rx * q.yc, q.kb(q.ry));
 }
 
 int pm_pencil_yinv_f32(pm_pencil* pen) {
     PM_TRY_S(pencil_ok(pen));
     Pencil& q = pen->q;
-    const Plan& p = q.plan->p;
-    const long long hc = q.hc(q.ry), ng = q.ng, nx = q.nx, ny = q.ny, yc = q.yc;
-    {
-        Timed t(p, ST_SORT);
-        for (int s = 0; s < q.px; ++s)  // [src ky chunk][nx][yc][hc] -> [nx][ng][hc]
-            PM_TRY_S(pencil_copy3(p, q.recv + (long long)s * nx * yc * hc, yc * hc, hc, q.work + (long long)s * yc * hc,
-                                  ng * hc, hc, q.nx, q.yc, (int)hc));
-    }
-    PM_TRY_S(pencil_fft_lines_f32(p, reinterpret_cast<float*>(q.work), hc, ng * hc, q.nx, (int)hc, +1, ST_FFT_Y_INV));
-    Timed t(p, ST_SORT);
-    for (int d = 0; d < q.py; ++d)  // y block d: [nx][ny][hc]
-        PM_TRY_S(pencil_copy3(p, q.work + (long long)d * ny * hc, ng * hc, hc, q.send + (long long)d * nx * ny * hc,
-                              ny * hc, hc, q.nx, q.ny, (int)hc));
-    return PM_OK;
+    const long long hc = q.hc(q.ry);
+    return pencil_lines_f32(q.plan->p, reinterpret_cast<const float*>(q.recv), reinterpret_cast<float*>(q.send),
+                            kymap(q, hc), ymap(q, hc), q.nx, (int)hc, +1, ST_FFT_Y_INV);
 }
 
 int pm_pencil_backward_f32(pm_pencil* pen) {
