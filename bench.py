@@ -12,7 +12,8 @@ over every particle; particle-updates/s = particles x steps / time.
   fp64       the plain FP64 path on the same initial state
   force_err  relative L2 of FP32 vs FP64 particle forces on that state
   e2e        the FP32 step through the C ABI with the particle state copied
-             from pinned host memory and back every step
+             from pinned host memory and back every step (chunked on two copy
+             streams, both PCIe directions at once; the serial figure beside)
   roofline   dominant kernel, algorithmic bytes / CUDA-event time, vs the
              measured HBM copy bandwidth
   cpu_baseline the reference's CPU code on a bounded sample (rank 0, N = 1)
@@ -147,6 +148,79 @@ def throughput(world: int, particles_per_rank: int, steps: int, t_ms: float) -> 
 def rank_seed(rank: int) -> int:
     """Each rank's box has its own initial conditions."""
     return SEED + rank
+
+
+# ------------------------------------------------- end-to-end host copies
+class HostRoundTrip:
+    """Per step: the particle state from pinned host memory to the device,
+    the step, the new state back to the host.  The arrays move in `chunks`
+    particle ranges on two copy streams; a chunk's host-to-device copy waits
+    for the device-to-host copy of the same range in the previous step (the
+    host copy it reads), so every step still moves all of its inputs in and all
+    of its results out, and PCIe carries the two directions at once.
+    serial=True: every copy on the compute stream, one after another."""
+
+    def __init__(self, torch, stream, dev_arrays, host_arrays, chunks: int = 16, serial: bool = False):
+        self.torch, self.stream, self.dev, self.host = torch, stream, dev_arrays, host_arrays
+        self.chunks, self.serial = chunks, serial
+        self.h2d = torch.cuda.Stream(device=stream.device)
+        self.d2h = torch.cuda.Stream(device=stream.device)
+        self.done = []  # (lo, hi, event) of the last step's device-to-host copies
+
+    def _bounds(self, n):
+        return [(n * k // self.chunks, n * (k + 1) // self.chunks) for k in range(self.chunks)]
+
+    def start(self, event):
+        """Copies of the next step start after `event` (the timing start)."""
+        self.h2d.wait_event(event)
+        self.d2h.wait_event(event)
+
+    def step(self, n_in: int, run, n_out=None):
+        """run() advances the state on the compute stream; n_out() the live
+        count after it (particles may migrate); returns the bytes moved."""
+        torch = self.torch
+        if self.serial:
+            with torch.cuda.stream(self.stream):
+                for h, d in zip(self.host, self.dev):
+                    d[:n_in].copy_(h[:n_in], non_blocking=True)
+                run()
+                n = n_out() if n_out else n_in
+                for h, d in zip(self.host, self.dev):
+                    h[:n].copy_(d[:n], non_blocking=True)
+            return n_in, n
+        arrived = []
+        for lo, hi in self._bounds(n_in):
+            with torch.cuda.stream(self.h2d):
+                for dlo, dhi, ev in self.done:
+                    if dlo < hi and lo < dhi:
+                        self.h2d.wait_event(ev)
+                for h, d in zip(self.host, self.dev):
+                    d[lo:hi].copy_(h[lo:hi], non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(self.h2d)
+                arrived.append(ev)
+        for ev in arrived:
+            self.stream.wait_event(ev)
+        with torch.cuda.stream(self.stream):
+            run()
+        n = n_out() if n_out else n_in
+        stepped = torch.cuda.Event()
+        stepped.record(self.stream)
+        self.d2h.wait_event(stepped)
+        self.done = []
+        for lo, hi in self._bounds(n):
+            with torch.cuda.stream(self.d2h):
+                for h, d in zip(self.host, self.dev):
+                    h[lo:hi].copy_(d[lo:hi], non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(self.d2h)
+                self.done.append((lo, hi, ev))
+        return n_in, n
+
+    def finish(self):
+        """The compute stream waits for the last step's copies (timing end)."""
+        for _, _, ev in self.done:
+            self.stream.wait_event(ev)
 
 
 # ------------------------------------------------------------- byte model
@@ -446,32 +520,39 @@ def ours_slab(args, pm, torch, dist, world, rank, dev, stream, barrier, max_over
     host = torch.empty(part.words.shape, dtype=torch.int32, pin_memory=True)
     host.copy_(part.words)
     nbytes = part.n * 8 * 4
+    # one contiguous copy per particle word and range (a strided view of
+    # pinned memory would be staged through pageable memory)
+    rows_dev = [part.words[w] for w in range(part.words.shape[0])]
+    rows_host = [host[w] for w in range(host.shape[0])]
 
-    def e2e_step():
-        # one contiguous copy per particle word (a strided view of pinned
-        # memory would be staged through pageable memory)
-        for w in range(part.words.shape[0]):
-            part.words[w, :part.n].copy_(host[w, :part.n], non_blocking=True)
-        step_fn([slab], [part], ex, mass, cp, ck, DT)
-        for w in range(part.words.shape[0]):
-            host[w, :part.n].copy_(part.words[w, :part.n], non_blocking=True)
+    def e2e_time(serial):
+        trip = HostRoundTrip(torch, stream, rows_dev, rows_host, serial=serial)
 
-    for _ in range(max(1, args.warmup)):
-        e2e_step()
-    barrier()
-    torch.cuda.synchronize()
-    e0.record(stream)
-    for _ in range(args.steps):
-        e2e_step()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    barrier()
-    te = max_over_ranks(e0.elapsed_time(e1))
+        def run():
+            step_fn([slab], [part], ex, mass, cp, ck, DT)
+
+        for _ in range(max(1, args.warmup)):
+            trip.step(part.n, run, lambda: part.n)
+        trip.finish()
+        barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        trip.start(e0)
+        for _ in range(args.steps):
+            trip.step(part.n, run, lambda: part.n)
+        trip.finish()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1))
+
+    te = e2e_time(False)
+    te_serial = e2e_time(True)
     e2e = {"value": np_ * args.steps / (te / 1e3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
-           "d2h_bytes_per_step": nbytes, "ms_per_step": te / args.steps,
+           "d2h_bytes_per_step": nbytes, "ms_per_step": te / args.steps, "serial_ms_per_step": te_serial / args.steps,
            "path": f"{'pencil' if args.pencil else 'slab'}.step (pm_{'pencil' if args.pencil else 'slab'}_* "
-                   "through the C ABI, NCCL exchanges); this rank's particle words copied from pinned host memory "
-                   "and back every step"}
+                   "through the C ABI, NCCL exchanges); every step this rank's particle words copied from pinned "
+                   "host memory and back, in 16 ranges on two copy streams (as the single-box leg)"}
     ensemble = None
     if not args.skip_ensemble:
         slab.close()
@@ -772,28 +853,36 @@ def ours(args):
         dbuf = [cell, *off, *v32]
         nbytes = sum(h.numel() * h.element_size() for h in host)
 
-        def e2e_step():
-            for h, d in zip(host, dbuf):
-                d.copy_(h, non_blocking=True)
-            p32.step_split(cell, off, v32, mass, cp, ck, DT)
-            for h, d in zip(host, dbuf):
-                h.copy_(d, non_blocking=True)
+        def e2e_time(serial):
+            trip = HostRoundTrip(torch, stream, dbuf, host, serial=serial)
 
-        for _ in range(max(1, args.warmup)):
-            e2e_step()
-        barrier()
-        torch.cuda.synchronize()
-        e0.record(stream)
-        for _ in range(args.steps):
-            e2e_step()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        barrier()
-        te = max_over_ranks(e0.elapsed_time(e1))
+            def run():
+                p32.step_split(cell, off, v32, mass, cp, ck, DT)
+
+            for _ in range(max(1, args.warmup)):
+                trip.step(np_, run)
+            trip.finish()
+            barrier()
+            torch.cuda.synchronize()
+            e0.record(stream)
+            trip.start(e0)
+            for _ in range(args.steps):
+                trip.step(np_, run)
+            trip.finish()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            barrier()
+            return max_over_ranks(e0.elapsed_time(e1))
+
+        te = e2e_time(False)
+        te_serial = e2e_time(True)
         e2e = {"value": throughput(world, np_, args.steps, te), "unit": UNIT, "h2d_bytes_per_step": nbytes,
                "d2h_bytes_per_step": nbytes, "ms_per_step": te / args.steps,
-               "path": "pm_step_f32 through the C ABI; particle state copied from pinned host memory and back "
-                       "every step"}
+               "serial_ms_per_step": te_serial / args.steps,
+               "path": "pm_step_f32 through the C ABI; every step the particle state copied from pinned host memory "
+                       "and the new state back, in 16 particle ranges on two copy streams (a range's host-to-device "
+                       "copy waits for its device-to-host copy of the step before; PCIe carries both directions "
+                       "at once); serial_ms_per_step: the same copies one after another on the compute stream"}
         del host
 
     cpu = None

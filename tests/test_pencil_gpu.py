@@ -106,3 +106,41 @@ def test_pencil_rejects_bad_geometry(pmpkg):
     for args in ((64, 3, 2, 0), (64, 32, 1, 0), (48, 2, 2, 0), (64, 2, 2, 4)):
         with pytest.raises(pmpkg.PMError):
             P.Pencil(*args)
+
+
+def test_pencil_ranks_without_particles(pmpkg):
+    """All particles in a clump inside pencil (0, 0) of 2 x 2: the other
+    pencils deposit nothing, gather nothing and migrate nothing; the result
+    still matches the undecomposed step."""
+    P = pmpkg.pencil
+    ng, px, py, n, dt = 64, 2, 2, 20000, 0.1
+    g = torch.Generator(device="cpu").manual_seed(4)
+    pos = [torch.rand(n, generator=g, dtype=torch.float64) * 6 + 5 for _ in range(2)]
+    pos.append(torch.rand(n, generator=g, dtype=torch.float64) * ng)
+    pos = [a.to(DEV) for a in pos]
+    vel = [(torch.rand(n, generator=g) - 0.5).to(DEV) for _ in range(3)]
+    plan = pmpkg.Plan(ng, "fp32", "spectral", 4)
+    cell, off = plan.split(*pos)
+    ids = torch.arange(n, dtype=torch.int32, device=DEV)
+    pens = [P.Pencil(ng, px, py, r, "spectral", 4) for r in range(px * py)]
+    parts = P.distribute(cell, off, vel, ids, ng, px, py, range(px * py), cap_factor=5.0)
+    assert [q.n for q in parts] == [n, 0, 0, 0]
+    c1, o1, v1 = cell.clone(), [a.clone() for a in off], [a.clone() for a in vel]
+    mass, cp = ng ** 3 / n, 4 * np.pi
+    for _ in range(2):
+        P.step(pens, parts, P.LocalExchange(), mass, cp, dt, dt)
+        plan.step_split(c1, o1, v1, mass, cp, dt, dt)
+    for s in pens:
+        s.check()
+    phi = assemble(pens, ng)
+    phi1 = plan.workspace_mesh()[:, :, :ng].double()
+    assert float((phi - phi1).norm() / phi1.norm()) < 1e-6
+    w = torch.cat([q.words[:, :q.n] for q in parts], dim=1)
+    w = w[:, torch.argsort(w[7])]
+    assert torch.equal(w[7], ids)
+    vel_s = torch.stack([w[4 + a].view(torch.float32) for a in range(3)]).double()
+    vref = torch.stack(v1).double()
+    assert float((vel_s - vref).norm() / vref.norm()) < 1e-5
+    for s in pens:
+        s.close()
+    plan.close()

@@ -94,3 +94,41 @@ def test_slab_first_kick_matches_oracle_forces(pmpkg, O):
     O.force_step(ng, *(a.cpu().numpy().copy() for a in pos), *f, 1.0, 4 * np.pi, 1.0, 1, 4)
     err = np.linalg.norm((v - v0) / dt - np.stack(f)) / np.linalg.norm(np.stack(f))
     assert err < 1e-4, err
+
+
+def test_slab_ranks_without_particles(pmpkg):
+    """All particles in a clump inside slab 0: the other slabs deposit only
+    the background, gather nothing and migrate nothing; the result still
+    matches the undecomposed step."""
+    S = pmpkg.slab
+    ng, nranks, n, dt = 64, 4, 20000, 0.1
+    g = torch.Generator(device="cpu").manual_seed(3)
+    pos = [torch.rand(n, generator=g, dtype=torch.float64) * 6 + 5 for _ in range(2)]
+    pos.append(torch.rand(n, generator=g, dtype=torch.float64) * ng)
+    pos = [a.to(DEV) for a in pos]
+    vel = [(torch.rand(n, generator=g) - 0.5).to(DEV) for _ in range(3)]
+    plan = pmpkg.Plan(ng, "fp32", "spectral", 4)
+    cell, off = plan.split(*pos)
+    ids = torch.arange(n, dtype=torch.int32, device=DEV)
+    slabs = [S.Slab(ng, nranks, r, "spectral", 4) for r in range(nranks)]
+    parts = S.distribute(cell, off, vel, ids, ng, nranks, range(nranks), cap_factor=5.0)
+    assert [q.n for q in parts] == [n, 0, 0, 0]
+    c1, o1, v1 = cell.clone(), [a.clone() for a in off], [a.clone() for a in vel]
+    mass, cp = ng ** 3 / n, 4 * np.pi
+    for _ in range(2):
+        S.step(slabs, parts, S.LocalExchange(), mass, cp, dt, dt)
+        plan.step_split(c1, o1, v1, mass, cp, dt, dt)
+    for s in slabs:
+        s.check()
+    phi = torch.cat([s.potential()[:, :, :ng] for s in slabs]).double()
+    phi1 = plan.workspace_mesh()[:, :, :ng].double()
+    assert float((phi - phi1).norm() / phi1.norm()) < 1e-6
+    w = torch.cat([q.words[:, :q.n] for q in parts], dim=1)
+    w = w[:, torch.argsort(w[7])]
+    assert torch.equal(w[7], ids)
+    vel_s = torch.stack([w[4 + a].view(torch.float32) for a in range(3)]).double()
+    vref = torch.stack(v1).double()
+    assert float((vel_s - vref).norm() / vref.norm()) < 1e-5
+    for s in slabs:
+        s.close()
+    plan.close()
