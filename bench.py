@@ -385,20 +385,40 @@ def ensemble_leg(pm, torch, args, world, rank, dev, stream, barrier, max_over_ra
     t_setup = time.perf_counter() - t0
     cp = pm.unit_box_coefficients(0.01)[0]
     esteps, edt = 20, 0.01
+    init = (ecell.clone(), [t.clone() for t in eoff], [t.clone() for t in evel])
+
+    def restore():
+        """The configuration's initial state into the graph's particle arrays."""
+        ecell.copy_(init[0])
+        for a in range(3):
+            eoff[a].copy_(init[1][a])
+            evel[a].copy_(init[2][a])
+
     ens.run(ecell, eoff, evel, cp, edt, esteps)  # capture + first replay
     torch.cuda.synchronize()
-    barrier()
     reps = 3
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(reps):
+    runs = []
+    for _ in range(reps):  # each timed run: the 20 KDK steps from the initial state
+        restore()
+        torch.cuda.synchronize()
+        barrier()
+        e0.record(stream)
         ens.run(ecell, eoff, evel, cp, edt, esteps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        runs.append(e0.elapsed_time(e1))
+    barrier()
+    t_ens = max_over_ranks(sum(runs)) / reps
+    # one more run continuing from the state those steps reached (steps 21 - 40)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    ens.run(ecell, eoff, evel, cp, edt, esteps)
     e1.record(stream)
     torch.cuda.synchronize()
-    barrier()
-    t_ens = max_over_ranks(e0.elapsed_time(e1)) / reps
+    t_cont = max_over_ranks(e0.elapsed_time(e1))
     # the same run launched eagerly (no graph): the launch overhead the graph removes
-    ec, eo, ev = ecell.clone(), [t.clone() for t in eoff], [t.clone() for t in evel]
+    ec, eo, ev = init[0].clone(), [t.clone() for t in init[1]], [t.clone() for t in init[2]]
     torch.cuda.synchronize()
     e0.record(stream)
     for s_ in range(esteps + 1):
@@ -414,6 +434,7 @@ def ensemble_leg(pm, torch, args, world, rank, dev, stream, barrier, max_over_ra
            "particles": total, "value": total * esteps / (t_ens / 1e3),
            "unit": UNIT, "ms_per_run": t_ens, "ms_per_step": t_ens / esteps,
            "boxes_per_rank": len(mine), "graph_nodes": info["graph_nodes"], "classes": info["classes"],
+           "continued_ms_per_run": t_cont,
            "eager_ms_per_run": t_eager,
            "launch_overhead_removed_by_graph": {"ms_per_run": t_eager - t_ens,
                                                 "share_of_eager": (t_eager - t_ens) / t_eager,
@@ -421,9 +442,11 @@ def ensemble_leg(pm, torch, args, world, rank, dev, stream, barrier, max_over_ra
            "tune_cache": "committed" if os.path.exists(TUNE_CACHE) else "autotuned at creation",
            "setup_s_incl_autotune": t_setup,
            "note": "one CUDA graph per run of 20 KDK steps (21 force evaluations); batched kernels per "
-                   "mesh-size class, classes on parallel graph branches; boxes dealt to ranks"}
+                   "mesh-size class, classes on parallel graph branches; boxes dealt to ranks; every timed run "
+                   "starts from the initial conditions (the state copied back outside the timed region); "
+                   "continued_ms_per_run: steps 21-40 from the state the timed runs reached"}
     ens.close()
-    del ens, ecell, eoff, evel
+    del ens, ecell, eoff, evel, init
     torch.cuda.empty_cache()
     return out
 
