@@ -11,9 +11,11 @@ over every particle; particle-updates/s = particles x steps / time.
              HBM, K steps timed with CUDA events (max over ranks)
   fp64       the plain FP64 path on the same initial state
   force_err  relative L2 of FP32 vs FP64 particle forces on that state
-  e2e        the FP32 step through the C ABI with the particle state copied
-             from pinned host memory and back every step (chunked on two copy
-             streams, both PCIe directions at once; the serial figure beside)
+  e2e        the FP32 step through the C ABI (pm_potential_f32, then
+             pm_kick_drift_f32 over particle ranges) with the particle state
+             copied from pinned host memory and back every step, on two copy
+             streams so both PCIe directions and the kernels overlap; the
+             whole-step and serial figures beside it
   roofline   dominant kernel, algorithmic bytes / CUDA-event time, vs the
              measured HBM copy bandwidth
   cpu_baseline the reference's CPU code on a bounded sample (rank 0, N = 1)
@@ -221,6 +223,70 @@ class HostRoundTrip:
         """The compute stream waits for the last step's copies (timing end)."""
         for _, _, ev in self.done:
             self.stream.wait_event(ev)
+
+
+class SplitRoundTrip:
+    """HostRoundTrip for a step in two calls, potential(positions) then
+    kick_drift(range) per particle range: the positions (cell, offsets) move
+    first and the velocities after them, in both directions, so the velocity
+    upload runs under the potential's kernels and each range's download
+    starts when its gather is done.  Every step still moves all seven words of
+    every particle in and out; a range of a word group goes up only after its
+    download of the step before."""
+
+    def __init__(self, torch, stream, pos_dev, vel_dev, pos_host, vel_host, chunks: int = 16):
+        self.torch, self.stream, self.chunks = torch, stream, chunks
+        self.groups = ((pos_dev, pos_host), (vel_dev, vel_host))
+        self.h2d = torch.cuda.Stream(device=stream.device)
+        self.d2h = torch.cuda.Stream(device=stream.device)
+        self.done = None  # [group][range] events of the last downloads
+
+    def start(self, event):
+        self.h2d.wait_event(event)
+        self.d2h.wait_event(event)
+
+    def _event(self, s):
+        ev = self.torch.cuda.Event()
+        ev.record(s)
+        return ev
+
+    def step(self, n, potential, kick_drift):
+        torch = self.torch
+        rng = [(n * k // self.chunks, n * (k + 1) // self.chunks) for k in range(self.chunks)]
+        up = []
+        for g, (dev, host) in enumerate(self.groups):
+            evs = []
+            for k, (lo, hi) in enumerate(rng):
+                with torch.cuda.stream(self.h2d):
+                    if self.done is not None:
+                        self.h2d.wait_event(self.done[g][k])
+                    for h, d in zip(host, dev):
+                        d[lo:hi].copy_(h[lo:hi], non_blocking=True)
+                    evs.append(self._event(self.h2d))
+            up.append(evs)
+        for ev in up[0]:
+            self.stream.wait_event(ev)
+        with torch.cuda.stream(self.stream):
+            potential()
+        gathered = []
+        for k, (lo, hi) in enumerate(rng):
+            self.stream.wait_event(up[1][k])
+            with torch.cuda.stream(self.stream):
+                kick_drift(lo, hi)
+            gathered.append(self._event(self.stream))
+        self.done = [[], []]
+        for g, (dev, host) in enumerate(self.groups):
+            for k, (lo, hi) in enumerate(rng):
+                with torch.cuda.stream(self.d2h):
+                    self.d2h.wait_event(gathered[k])
+                    for h, d in zip(host, dev):
+                        h[lo:hi].copy_(d[lo:hi], non_blocking=True)
+                    self.done[g].append(self._event(self.d2h))
+
+    def finish(self):
+        for evs in self.done or []:
+            for ev in evs:
+                self.stream.wait_event(ev)
 
 
 # ------------------------------------------------------------- byte model
@@ -876,36 +942,49 @@ def ours(args):
         dbuf = [cell, *off, *v32]
         nbytes = sum(h.numel() * h.element_size() for h in host)
 
-        def e2e_time(serial):
-            trip = HostRoundTrip(torch, stream, dbuf, host, serial=serial)
+        def e2e_time(mode):
+            if mode == "split":
+                trip = SplitRoundTrip(torch, stream, dbuf[:4], dbuf[4:], host[:4], host[4:])
 
-            def run():
-                p32.step_split(cell, off, v32, mass, cp, ck, DT)
+                def one():
+                    trip.step(np_, lambda: p32.potential_split(cell, off, mass, cp),
+                              lambda lo, hi: p32.kick_drift_split(p32.workspace_mesh(), cell[lo:hi],
+                                                                  [a[lo:hi] for a in off], [a[lo:hi] for a in v32],
+                                                                  ck, DT))
+            else:
+                trip = HostRoundTrip(torch, stream, dbuf, host, serial=mode == "serial")
+
+                def one():
+                    trip.step(np_, lambda: p32.step_split(cell, off, v32, mass, cp, ck, DT))
 
             for _ in range(max(1, args.warmup)):
-                trip.step(np_, run)
+                one()
             trip.finish()
             barrier()
             torch.cuda.synchronize()
             e0.record(stream)
             trip.start(e0)
             for _ in range(args.steps):
-                trip.step(np_, run)
+                one()
             trip.finish()
             e1.record(stream)
             torch.cuda.synchronize()
             barrier()
             return max_over_ranks(e0.elapsed_time(e1))
 
-        te = e2e_time(False)
-        te_serial = e2e_time(True)
+        te = e2e_time("split")
+        te_whole = e2e_time("whole")
+        te_serial = e2e_time("serial")
         e2e = {"value": throughput(world, np_, args.steps, te), "unit": UNIT, "h2d_bytes_per_step": nbytes,
                "d2h_bytes_per_step": nbytes, "ms_per_step": te / args.steps,
-               "serial_ms_per_step": te_serial / args.steps,
-               "path": "pm_step_f32 through the C ABI; every step the particle state copied from pinned host memory "
-                       "and the new state back, in 16 particle ranges on two copy streams (a range's host-to-device "
-                       "copy waits for its device-to-host copy of the step before; PCIe carries both directions "
-                       "at once); serial_ms_per_step: the same copies one after another on the compute stream"}
+               "whole_step_ms_per_step": te_whole / args.steps, "serial_ms_per_step": te_serial / args.steps,
+               "path": "pm_potential_f32 then pm_kick_drift_f32 over 16 particle ranges (the two halves of "
+                       "pm_step_f32, same result) through the C ABI; every step all seven words of every particle "
+                       "copied from pinned host memory and the new state back on two copy streams: positions "
+                       "first, velocities after them (uploaded while the potential is computed), each range "
+                       "downloaded when its gather is done and uploaded again for the next step after its "
+                       "download; whole_step_ms_per_step: pm_step_f32 with the same copies in 16 ranges; "
+                       "serial_ms_per_step: every copy one after another on the compute stream"}
         del host
 
     cpu = None

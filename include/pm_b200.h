@@ -275,6 +275,14 @@ int pm_interp_f32(pm_plan* plan, const float* phi, const uint32_t* cell, const f
 int pm_kick_drift_f32(pm_plan* plan, const float* phi, uint32_t* cell, float* ox, float* oy,
                       float* oz, float* vx, float* vy, float* vz, int64_t np, double c_kick,
                       double dt);
+/* The first part of pm_step_f32: binning, the deposit fused with the z FFT
+ * pass, the y / x + Green / y passes and z C2R -- the potential of the
+ * particles in the plan's workspace mesh (pm_plan_mesh, [ng][ng][ng+2]).
+ * pm_kick_drift_f32 on that mesh completes the step with the same result
+ * as pm_step_f32 (its default gather), possibly over particle ranges: the
+ * velocities are not read until then. */
+int pm_potential_f32(pm_plan* plan, const uint32_t* cell, const float* ox, const float* oy,
+                     const float* oz, int64_t np, float mass, double c_poisson);
 /* One full FP32 step on the plan's workspace: binning by 4 x 4-cell column
  * tile, the deposit fused with the z R2C pass (power-of-two ng >= 32; the
  * tile deposit otherwise), the y / x + Green / y passes, z C2R, then

@@ -53,6 +53,7 @@ SIGNATURES = {
     "pm_interp_f32": [_V, _V, _V, _V, _V, _V, _L, _V, _V, _V],
     "pm_kick_drift_f32": [_V, _V, _V, _V, _V, _V, _V, _V, _V, _L, _D, _D],
     "pm_step_f32": [_V, _V, _V, _V, _V, _V, _V, _V, _L, _F, _D, _D, _D],
+    "pm_potential_f32": [_V, _V, _V, _V, _V, _L, _F, _D],
     "pm_plan_set_fft_shape": [_V, _I, _I],
     "pm_plan_set_gather": [_V, _I],
     "pm_reduce_f32": [_V, _V, _V, _V, _V, _L, _D, _V],

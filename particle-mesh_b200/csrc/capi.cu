@@ -566,6 +566,29 @@ int pm_kick_drift_f32(pm_plan* plan, const float* phi, uint32_t* cell, float* ox
     return kick_drift_f32(plan->p, phi, cell, ox, oy, oz, vx, vy, vz, np, c_kick, dt);
 }
 
+// The potential of the particles in the plan's workspace mesh: binning, the
+// deposit fused with the z FFT pass (zcb: z-chunk bits of the bins), the
+// remaining passes.  Shared by pm_potential_f32 and pm_step_f32.
+static int potential_f32(Plan& p, const uint32_t* cell, const float* ox, const float* oy, const float* oz,
+                         int64_t np, float mass, double c_poisson, int zcb) {
+    PM_TRY(ensure_workspace(p, false));
+    float* m = static_cast<float*>(p.mesh);
+    if (zcol_supported(p.ng)) {  // deposit fused with the z FFT pass
+        PM_TRY(deposit_zr2c_f32(p, cell, ox, oy, oz, np, mass, m, zcb));
+        return poisson_after_z_f32(p, m, c_poisson);
+    }
+    PM_TRY(deposit_f32_tiles(p, cell, ox, oy, oz, np, mass, m));
+    return poisson_fused<float>(p, m, c_poisson);
+}
+
+int pm_potential_f32(pm_plan* plan, const uint32_t* cell, const float* ox, const float* oy, const float* oz,
+                     int64_t np, float mass, double c_poisson) {
+    PM_TRY(check_plan(plan, PM_FP32));
+    PM_TRY(check_np(np, {cell, ox, oy, oz}));
+    PM_TRY(set_device(plan->p));
+    return potential_f32(plan->p, cell, ox, oy, oz, np, mass, c_poisson, 0);
+}
+
 int pm_step_f32(pm_plan* plan, uint32_t* cell, float* ox, float* oy, float* oz, float* vx,
                 float* vy, float* vz, int64_t np, float mass, double c_poisson, double c_kick,
                 double dt) {
@@ -573,25 +596,18 @@ int pm_step_f32(pm_plan* plan, uint32_t* cell, float* ox, float* oy, float* oz, 
     PM_TRY(check_np(np, {cell, ox, oy, oz, vx, vy, vz}));
     PM_TRY(set_device(plan->p));
     Plan& p = plan->p;
-    PM_TRY(ensure_workspace(p, false));
-    float* m = static_cast<float*>(p.mesh);
+    float* m = nullptr;
     if (p.gather == PM_GATHER_TILED && tiled_gather_supported(p.ng)) {
         // binned by (column tile, class, z chunk): the deposit fused with the
         // z FFT pass, and the gather from potential tiles staged in shared
         // memory in the same bin order
-        PM_TRY(deposit_zr2c_f32(p, cell, ox, oy, oz, np, mass, m, tiled_gather_zcb(p.ng)));
-        PM_TRY(poisson_after_z_f32(p, m, c_poisson));
+        PM_TRY(potential_f32(p, cell, ox, oy, oz, np, mass, c_poisson, tiled_gather_zcb(p.ng)));
+        m = static_cast<float*>(p.mesh);
         return kick_drift_tiles_f32(p, m, cell, ox, oy, oz, vx, vy, vz, np, c_kick, dt);
     }
-    if (zcol_supported(p.ng)) {  // deposit fused with the z FFT pass
-        PM_TRY(deposit_zr2c_f32(p, cell, ox, oy, oz, np, mass, m));
-        PM_TRY(poisson_after_z_f32(p, m, c_poisson));
-    } else {
-        PM_TRY(deposit_f32_tiles(p, cell, ox, oy, oz, np, mass, m));
-        PM_TRY(poisson_fused<float>(p, m, c_poisson));
-    }
-    PM_TRY(kick_drift_f32(p, m, cell, ox, oy, oz, vx, vy, vz, np, c_kick, dt));
-    return PM_OK;
+    PM_TRY(potential_f32(p, cell, ox, oy, oz, np, mass, c_poisson, 0));
+    m = static_cast<float*>(p.mesh);
+    return kick_drift_f32(p, m, cell, ox, oy, oz, vx, vy, vz, np, c_kick, dt);
 }
 
 // ------------------------------------------------------- FP32 adjoints

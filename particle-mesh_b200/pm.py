@@ -299,6 +299,14 @@ class Plan:
         check(self.lib.pm_kick_drift_f32(self._h, _vp(self._mesh(phi, "phi")), _vp(cell), *(_vp(t) for t in off),
                                          *(_vp(t) for t in vel), np_, float(c_kick), float(dt)))
 
+    def potential_split(self, cell, off, mass: float, c_poisson: float) -> torch.Tensor:
+        """The first part of step_split: the particles' potential in the
+        workspace mesh (returned); kick_drift_split on it completes the step."""
+        np_ = self._split_args(cell, off)
+        check(self.lib.pm_potential_f32(self._h, _vp(cell), *(_vp(t) for t in off), np_, float(mass),
+                                        float(c_poisson)))
+        return self.workspace_mesh()
+
     def step_split(self, cell, off, vel, mass: float, c_poisson: float, c_kick: float, dt: float):
         np_ = self._split_args(cell, off, vel)
         check(self.lib.pm_step_f32(self._h, _vp(cell), *(_vp(t) for t in off), *(_vp(t) for t in vel), np_,

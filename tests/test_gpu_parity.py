@@ -668,3 +668,34 @@ def test_tiled_gather_matches_cached(pmpkg, O, ng, nrow):
         assert d < 1e-5, d
     with pytest.raises(pmpkg.PMError):
         pmpkg.Plan(128, "fp32").set_gather("tiled")  # below 256 cells: PM_ERR_SIZE
+
+
+@pytest.mark.parametrize("ng,nrow", [(64, 32), (1024, 64)])
+def test_potential_then_ranged_kick_drift_equals_step(pmpkg, O, ng, nrow):
+    """pm_potential_f32 followed by pm_kick_drift_f32: over four particle
+    ranges it gives the whole-range gather's state bit for bit (the gather is
+    per particle), and the pair gives pm_step_f32's state within FP32
+    rounding (the deposit's shared-memory atomics sum in no fixed order)."""
+    pos, vel = O.zeldovich_ic(ng, nrow, -1.5, 1.0, seed=ng + 7)
+    mass, cp, dt = ng ** 3 / nrow ** 3, 4 * np.pi, 0.01
+    plan = pmpkg.Plan(ng, "fp32", "spectral", 4)
+    cell, off = plan.split(*(T(a) for a in pos))
+    v = [T(a, torch.float32) for a in vel]
+    c1, o1, v1 = cell.clone(), [a.clone() for a in off], [a.clone() for a in v]
+    c2, o2, v2 = cell.clone(), [a.clone() for a in off], [a.clone() for a in v]
+    plan.step_split(cell, off, v, mass, cp, dt, dt)
+    phi = plan.potential_split(c1, o1, mass, cp)
+    plan.kick_drift_split(phi, c2, o2, v2, dt, dt)
+    n = nrow ** 3
+    for lo, hi in ((0, n // 3), (n // 3, n // 2), (n // 2, n - 5), (n - 5, n)):
+        plan.kick_drift_split(phi, c1[lo:hi], [a[lo:hi] for a in o1], [a[lo:hi] for a in v1], dt, dt)
+    plan.check()
+    assert torch.equal(c1, c2)
+    for a, b in zip(o1 + v1, o2 + v2):
+        assert torch.equal(a, b)
+    err = rel(np.stack([H(a) for a in v1]), np.stack([H(a) for a in v]))
+    assert err < 1e-6, err
+    x0, x1 = plan.join(cell, off), plan.join(c1, o1)
+    d = max(float((torch.remainder(a - b + ng / 2, ng) - ng / 2).abs().max()) for a, b in zip(x1, x0))
+    assert d < 1e-5, d
+    plan.close()
