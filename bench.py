@@ -77,6 +77,9 @@ def parse():
                     help="gather of the FP32 step (pm_plan_set_gather)")
     ap.add_argument("--slab", action="store_true",
                     help="run the x-slab decomposition at N = 1 too (at N > 1 it is the default)")
+    ap.add_argument("--peer", action="store_true",
+                    help="slab path: the transposes by the FFT kernels' stores into the other GPUs' memory "
+                         "(symmetric memory) instead of NCCL all-to-alls")
     ap.add_argument("--pencil", action="store_true",
                     help="run the pencil decomposition instead (px x py = N pencils, px >= py; 1 x 1 at N = 1)")
     return ap.parse_args()
@@ -558,7 +561,10 @@ def ours_slab(args, pm, torch, dist, world, rank, dev, stream, barrier, max_over
         step_fn = P.step
     else:
         slab = S.Slab(ng, world, rank, "spectral", 4, stream=stream, device=dev)
-        ex = S.DistExchange()
+        if args.peer:
+            ex = S.PeerExchange(slab) if world > 1 else S.LocalPeerExchange([slab])
+        else:
+            ex = S.DistExchange()
         step_fn = S.step
     sampler = ClockSampler(bus_id(torch, dev))
     for _ in range(args.warmup):
@@ -663,7 +669,9 @@ def ours_slab(args, pm, torch, dist, world, rank, dev, stream, barrier, max_over
                                        f"GPU; ghost rows, two y-group and two x-group all-to-all transposes, "
                                        f"two-axis potential halo, particle migration" if args.pencil else
                                        f"slab{world}: x-slabs of {ng // world} planes, one per GPU; NCCL ghost "
-                                       f"fold, two all-to-all transposes, potential halo, particle migration")},
+                                       f"fold, two " + ("transposes by the FFT kernels' stores into the other "
+                                                        "GPUs' memory" if args.peer else "all-to-all transposes")
+                                       + ", potential halo, particle migration")},
             "stages": per_stage, "ensemble": ensemble, "e2e": e2e, "roofline": roofline, "cpu_baseline": None,
             "clocks": clocks, "gpu_launches": launches}
     print(json.dumps(line), flush=True)
@@ -698,7 +706,7 @@ def ours(args):
     mass = ng ** 3 / np_
     cp, ck = pm.unit_box_coefficients(DT)
     stream = torch.cuda.current_stream(dev)
-    if world > 1 or args.slab or args.pencil:
+    if world > 1 or args.slab or args.pencil or args.peer:
         return ours_slab(args, pm, torch, dist, world, rank, dev, stream, barrier, max_over_ranks)
 
     pos, vel = pm.zeldovich_ic(ng, nrow, N_S, RMS, rank_seed(rank), device=dev)

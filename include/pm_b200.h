@@ -417,6 +417,24 @@ int pm_slab_migrate_pack(pm_slab* slab, void* const* arrays, int narrays, int64_
 int pm_slab_migrate_unpack(pm_slab* slab, const uint32_t* packed, int64_t n, void* const* arrays, int narrays,
                            int64_t at);
 int pm_slab_check(pm_slab* slab);
+/* Transposes by peer stores (new; the fused form of exchange B): the y
+ * forward and the x + Green pass store each output row straight into the
+ * buffer of the rank that owns it, through peer device pointers (one per
+ * rank, in rank order, each xfer_floats floats and mapped into this
+ * process, e.g. symmetric memory), at this rank's block -- the layouts
+ * exchange B would deliver.  No collective moves the spectrum; the caller
+ * puts a barrier across the ranks after each of the two stores (every
+ * store done before any rank reads) and before the next step's forward.
+ *   pm_slab_forward_peers_f32    y forward; rows (ky, x) into peer_recv[ky / nx]
+ *   pm_slab_xgreen_peers_f32     x + Green on `recv` (this rank's buffer the
+ *                                forwards filled); rows into peer_rows[kx / nx]
+ *   pm_slab_backward_rows_f32    y inverse from `rows` (this rank's buffer the
+ *                                x + Green passes filled), z C2R
+ * At most 16 ranks (PM_ERR_SIZE beyond). */
+int pm_slab_forward_peers_f32(pm_slab* slab, void* const* peer_recv, int npeers);
+int pm_slab_xgreen_peers_f32(pm_slab* slab, const void* recv, double c_poisson, void* const* peer_rows,
+                             int npeers);
+int pm_slab_backward_rows_f32(pm_slab* slab, const void* rows);
 
 /* ------------------------------------- pencil decomposition (FP32, new)
  * The decomposition the reference's Makefile names (DECOMP_CHOICES "pencil",

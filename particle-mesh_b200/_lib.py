@@ -83,6 +83,9 @@ SIGNATURES = {
     "pm_slab_migrate_pack": [_V, _V, _I, _L, _V],
     "pm_slab_migrate_unpack": [_V, _V, _L, _V, _I, _L],
     "pm_slab_check": [_V],
+    "pm_slab_forward_peers_f32": [_V, _V, _I],
+    "pm_slab_xgreen_peers_f32": [_V, _V, _D, _V, _I],
+    "pm_slab_backward_rows_f32": [_V, _V],
     "pm_pencil_create": [_I, _I, _I, _I, _I, _I, _V, ctypes.POINTER(_V)],
     "pm_pencil_destroy": [_V],
     "pm_pencil_info": [_V, _V, _V, _V, _V, _V, _V, _V, _V, _V],

@@ -201,10 +201,11 @@ k_fft_strided(typename Cx<T>::t* __restrict__ data, long long es_, long long os_
 // (plane blockIdx.y, columns [bx TK, bx TK + TK) consecutive): the y passes
 // of a pencil, reading the blocks one transpose delivered and writing the
 // blocks the next one sends.
-template <typename T, int N, int DIR, int TK, int RV = 0>
+// PEER: the outputs go through the peer map `po` instead of `out` / `mo`.
+template <typename T, int N, int DIR, int TK, int RV = 0, bool PEER = false>
 __global__ void __launch_bounds__(strided_threads<N, TK, RV>(), 2)
 k_fft_lines_map(const typename Cx<T>::t* __restrict__ in, typename Cx<T>::t* __restrict__ out, LineMap mi,
-                LineMap mo, int ncols, const typename Cx<T>::t* __restrict__ tw) {
+                LineMap mo, int ncols, const typename Cx<T>::t* __restrict__ tw, PeerMap po = PeerMap{}) {
     using C = typename Cx<T>::t;
     constexpr int R1 = RadixV<N, RV>::R1, R2 = RadixV<N, RV>::R2;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -221,7 +222,14 @@ k_fft_lines_map(const typename Cx<T>::t* __restrict__ in, typename Cx<T>::t* __r
     __syncthreads();
     stockham_pass2<R1, R2, DIR, false, C>(
         ty, [&](int j, int r) { return S[I::p2(j, r, tx)]; },
-        [&](int j, int k, C v) { if (active) ob[lm_off(mo, j + k * R1)] = v; },
+        [&](int j, int k, C v) {
+            if (!active) return;
+            const int m = j + k * R1;
+            if (PEER)
+                reinterpret_cast<C*>(po.base[m >> po.sl])[(long long)blockIdx.y * po.ps + (m & po.mask) * po.s0 + col] = v;
+            else
+                ob[lm_off(mo, m)] = v;
+        },
         pass2_twiddles<DIR, (R2 >= 16 && sizeof(T) == 4)>(tw, ty));
 }
 
@@ -261,11 +269,13 @@ __device__ __forceinline__ T green_value(int kx, int ky, int kz, int kind, doubl
 // ky = ky0 + blockIdx.y, column c holds kz = kz0 + c).  An x-slab's blocks
 // [rank][kyl][x][kz] map kx to (kx >> log2 nx) nx^2 H + (kx & (nx - 1)) H; a
 // pencil's [kx][kyl][kz] to kx yc hc.
-template <typename T, int N, int TK, int RV = 0, bool XT = false, bool SLABX = false>
+// PEER (with SLABX): the outputs go through the peer map `po` (element kx to
+// the rank owning x = kx) instead of `out`.
+template <typename T, int N, int TK, int RV = 0, bool XT = false, bool SLABX = false, bool PEER = false>
 __global__ void __launch_bounds__(strided_threads<N, TK, RV>(), 2)
 k_fft_x_green(typename Cx<T>::t* __restrict__ data, long long es_, long long os_, long long bs, int ncols,
               const typename Cx<T>::t* __restrict__ tw, const T* __restrict__ g1d, double cg, int kind,
-              typename Cx<T>::t* out, int ky0 = 0, LineMap lm = LineMap{}, int kz0 = 0) {
+              typename Cx<T>::t* out, int ky0 = 0, LineMap lm = LineMap{}, int kz0 = 0, PeerMap po = PeerMap{}) {
     using C = typename Cx<T>::t;
     constexpr int R1 = RadixV<N, RV>::R1, R2 = RadixV<N, RV>::R2;
     // x lines of the padded spectrum: compile-time strides (es_ = N H and
@@ -314,10 +324,14 @@ k_fft_x_green(typename Cx<T>::t* __restrict__ data, long long es_, long long os_
         ty, p2ld,
         [&](int j, int k, C v) {
             if (!active) return;
-            if (SLABX)
+            if (PEER) {
+                const int m = j + k * R1;
+                reinterpret_cast<C*>(po.base[m >> po.sl])[(long long)blockIdx.y * po.ps + (m & po.mask) * po.s0 + col] = v;
+            } else if (SLABX) {
                 obase[soff(j + k * R1)] = v;
-            else
+            } else {
                 obase[j * oes + k * oes2] = v;
+            }
         },
         pass2_twiddles<+1, kSplitTw>(tw, ty));
 }
@@ -504,6 +518,8 @@ template <typename T, int N, int TK = tk_cols<T, N>(), int RV = 0> struct Launch
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, -1, TK, RV, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, +1, TK, RV, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_lines_map<T, N, -1, TK, RV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
+        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_lines_map<T, N, -1, TK, RV, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
+        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_x_green<T, N, TK, RV, false, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_lines_map<T, N, +1, TK, RV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_x_green<T, N, TK, RV, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         return PM_OK;
@@ -558,6 +574,23 @@ template <typename T, int N, int TK = tk_cols<T, N>(), int RV = 0> struct Launch
         k_fft_x_green<T, N, TK, RV, false, true><<<grid, strided_threads<N, TK, RV>(), smem_s(), p.stream>>>(
             const_cast<C*>(reinterpret_cast<const C*>(in)), H, (long long)N * H, 0, ncols, static_cast<const C*>(p.tw),
             static_cast<const T*>(p.g1d), cg, p.green_kind, reinterpret_cast<C*>(out), ky0, m, kz0);
+    }
+    // the y forward of an x-slab's own planes storing each ky row straight
+    // into the rank owning ky (peer map), and x + Green likewise by kx
+    static void y_to_peers(const Plan& p, const T* own, const PeerMap& po, int nx) {
+        const dim3 grid((H + TK - 1) / TK, nx);
+        const LineMap mi{(long long)N * H, 0, H, 30, (1 << 30) - 1};
+        Timed t(p, ST_FFT_Y_FWD);
+        k_fft_lines_map<T, N, -1, TK, RV, true><<<grid, strided_threads<N, TK, RV>(), smem_s(), p.stream>>>(
+            reinterpret_cast<const C*>(own), nullptr, mi, LineMap{}, H, static_cast<const C*>(p.tw), po);
+    }
+    static void xgreen_peers(const Plan& p, const T* in, double cg, LineMap m, const PeerMap& po, int planes,
+                             int ky0) {
+        const dim3 grid((H + TK - 1) / TK, planes);
+        Timed t(p, ST_FFT_X_GREEN);
+        k_fft_x_green<T, N, TK, RV, false, true, true><<<grid, strided_threads<N, TK, RV>(), smem_s(), p.stream>>>(
+            const_cast<C*>(reinterpret_cast<const C*>(in)), H, (long long)N * H, 0, H, static_cast<const C*>(p.tw),
+            static_cast<const T*>(p.g1d), cg, p.green_kind, nullptr, ky0, m, 0, po);
     }
     // y forward of the nx own planes [x][y][kz] of an x-slab, stored as the
     // rows [ky][x][kz] of its transpose buffer
@@ -855,6 +888,24 @@ int slab_fft_xgreen_f32(const Plan& p, const float* recv, float* send, double c_
     // rank kx / nx's block [kyl][x][kz]: (nx^2 H * (ng / nx) <= ng^2 H < 2^31)
     const LineMap m{(long long)nx * H, nx * nx * H, H, nxl, nx - 1};
     PMB_SLAB_LAUNCH(p, L_::xgreen_map(p, recv, send, cg, m, nx, H, ky0, 0));
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+int slab_fft_forward_peers_f32(const Plan& p, const float* own, const PeerMap& po, int nx) {
+    PMB_SLAB_LAUNCH(p, L_::y_to_peers(p, own, po, nx));
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+int slab_fft_xgreen_peers_f32(const Plan& p, const float* recv, const PeerMap& po, double c_poisson, int nx,
+                              int ky0) {
+    const double cg = green_scale(p, c_poisson);
+    int nxl = 0;
+    while ((1 << nxl) < nx) ++nxl;
+    const int H = p.ng / 2 + 1;
+    const LineMap m{(long long)nx * H, nx * nx * H, H, nxl, nx - 1};
+    PMB_SLAB_LAUNCH(p, L_::xgreen_peers(p, recv, cg, m, po, nx, ky0));
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;
 }

@@ -112,6 +112,17 @@ struct LineMap {
 };
 __host__ __device__ __forceinline__ int lm_off(const LineMap& m, int n) { return (n >> m.sl) * m.s1 + (n & m.mask) * m.s0; }
 
+// Where an FFT pass of a decomposed mesh stores its outputs straight into the
+// other ranks' buffers (peer device pointers): element n of the line of plane
+// p goes to base[n >> sl] + p * ps + (n & mask) * s0 (complex units; base
+// already offset to this rank's block in each destination).
+constexpr int kMaxPeers = 16;
+struct PeerMap {
+    void* base[kMaxPeers] = {};
+    long long ps = 0;
+    int s0 = 0, sl = 0, mask = 0;
+};
+
 // ---------------------------------------------------------------- the plan
 struct Plan {
     int ng = 0;
@@ -237,6 +248,10 @@ int slab_rank_sort(Plan& p, int nranks, int nx, const uint32_t* cell, int64_t np
 int slab_fft_forward_y_f32(const Plan& p, const float* own, float* send, int nx);
 int slab_fft_xgreen_f32(const Plan& p, const float* recv, float* send, double c_poisson, int nx, int ky0);
 int slab_fft_backward_f32(const Plan& p, const float* recv, float* own, int nx);
+// the same two passes storing into the other ranks' buffers (PeerMap)
+int slab_fft_forward_peers_f32(const Plan& p, const float* own, const PeerMap& po, int nx);
+int slab_fft_xgreen_peers_f32(const Plan& p, const float* recv, const PeerMap& po, double c_poisson, int nx,
+                              int ky0);
 int slab_kick_drift_f32(const Plan& p, int x0, int nx, const float* phi, uint32_t* cell, float* ox, float* oy,
                         float* oz, float* vx, float* vy, float* vz, int64_t np, double c_kick, double dt);
 int plan_create_internal(int ng, int precision, int green_kind, int grad_order, void* stream, pm_plan** out);

@@ -271,6 +271,57 @@ int pm_slab_backward_f32(pm_slab* slab) {
     return slab_fft_backward_f32(s.plan->p, reinterpret_cast<const float*>(s.recv), s.own(), s.nx);
 }
 
+// Transposes by stores into the other ranks' memory: the y forward and the
+// x + Green pass write each output row into the buffer of the rank that
+// owns it (peer device pointers, e.g. from symmetric memory), at this rank's
+// block; no collective moves the spectrum.  The caller separates the phases
+// with a barrier across the ranks (every store done before a rank reads).
+static int peer_map(const Slab& s, void* const* peers, int npeers, long long block, long long ps, int s0, int n,
+                    PeerMap& po) {
+    if (!peers || npeers != s.nranks) return fail(PM_ERR_ARG, "one peer buffer per rank expected");
+    if (npeers > kMaxPeers) return fail(PM_ERR_SIZE, "at most 16 ranks for the peer-store transposes");
+    for (int d = 0; d < npeers; ++d) {
+        if (!peers[d]) return fail(PM_ERR_ARG, "NULL peer buffer");
+        po.base[d] = static_cast<float2*>(peers[d]) + block;
+    }
+    int l = 0;
+    while ((1 << l) < n) ++l;
+    po.ps = ps;
+    po.s0 = s0;
+    po.sl = l;
+    po.mask = n - 1;
+    return PM_OK;
+}
+
+int pm_slab_forward_peers_f32(pm_slab* slab, void* const* peer_recv, int npeers) {
+    PM_TRY_S(slab_ok(slab));
+    Slab& s = slab->s;
+    const int H = s.ng / 2 + 1;
+    // row (ky, x) to rank ky / nyl, its block `rank`, at (ky mod nyl) nx + x
+    PeerMap po;
+    PM_TRY_S(peer_map(s, peer_recv, npeers, (long long)s.rank * s.nyl * s.nx * H, H, s.nx * H, s.nyl, po));
+    return slab_fft_forward_peers_f32(s.plan->p, s.own(), po, s.nx);
+}
+
+int pm_slab_xgreen_peers_f32(pm_slab* slab, const void* recv, double c_poisson, void* const* peer_rows,
+                             int npeers) {
+    PM_TRY_S(slab_ok(slab));
+    if (!recv) return fail(PM_ERR_ARG, "recv is NULL");
+    Slab& s = slab->s;
+    const int H = s.ng / 2 + 1;
+    // line (kyl, kx) to rank kx / nx, row (ky0 + kyl) nx + kx mod nx of its rows [ky][x][kz]
+    PeerMap po;
+    PM_TRY_S(peer_map(s, peer_rows, npeers, (long long)s.ky0 * s.nx * H, (long long)s.nx * H, H, s.nx, po));
+    return slab_fft_xgreen_peers_f32(s.plan->p, static_cast<const float*>(recv), po, c_poisson, s.nx, s.ky0);
+}
+
+int pm_slab_backward_rows_f32(pm_slab* slab, const void* rows) {
+    PM_TRY_S(slab_ok(slab));
+    if (!rows) return fail(PM_ERR_ARG, "rows is NULL");
+    Slab& s = slab->s;
+    return slab_fft_backward_f32(s.plan->p, static_cast<const float*>(rows), s.own(), s.nx);
+}
+
 int pm_slab_kick_drift_f32(pm_slab* slab, uint32_t* cell, float* ox, float* oy, float* oz, float* vx, float* vy,
                            float* vz, int64_t np, double c_kick, double dt) {
     PM_TRY_S(slab_ok(slab));

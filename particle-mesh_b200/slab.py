@@ -178,6 +178,20 @@ class Slab:
     def backward(self):
         check(self.lib.pm_slab_backward_f32(self._h))
 
+    # transposes by peer stores (pm_slab_*_peers_f32): one device pointer per
+    # rank, in rank order
+    def forward_peers(self, peer_recv):
+        arr = (ctypes.c_void_p * len(peer_recv))(*peer_recv)
+        check(self.lib.pm_slab_forward_peers_f32(self._h, arr, len(peer_recv)))
+
+    def xgreen_peers(self, recv_ptr: int, c_poisson: float, peer_rows):
+        arr = (ctypes.c_void_p * len(peer_rows))(*peer_rows)
+        check(self.lib.pm_slab_xgreen_peers_f32(self._h, ctypes.c_void_p(recv_ptr), float(c_poisson), arr,
+                                                len(peer_rows)))
+
+    def backward_rows(self, rows_ptr: int):
+        check(self.lib.pm_slab_backward_rows_f32(self._h, ctypes.c_void_p(rows_ptr)))
+
     def kick_drift(self, q: SlabParticles, c_kick: float, dt: float):
         check(self.lib.pm_slab_kick_drift_f32(self._h, _vp(q.cell), *(_vp(t) for t in q.off),
                                               *(_vp(t) for t in q.vel), q.n, float(c_kick), float(dt)))
@@ -199,7 +213,26 @@ class Slab:
 
 
 # ------------------------------------------------------------------ exchanges
-class LocalExchange:
+class _Transposes:
+    """The spectrum passes around the two global transposes, with the
+    transposes as all-to-alls of the send / recv buffers."""
+
+    def forward(self, slabs):
+        for s in slabs:
+            s.forward()
+        self.alltoall(slabs)
+
+    def xgreen(self, slabs, c_poisson):
+        for s in slabs:
+            s.xgreen(c_poisson)
+        self.alltoall(slabs)
+
+    def backward(self, slabs):
+        for s in slabs:
+            s.backward()
+
+
+class LocalExchange(_Transposes):
     """Every slab of the decomposition in this process; the exchanges are
     device copies on the current stream, slab after slab."""
 
@@ -239,7 +272,7 @@ class LocalExchange:
             q.n = incoming.shape[0]
 
 
-class DistExchange:
+class DistExchange(_Transposes):
     """This process's one slab; the exchanges are torch.distributed
     collectives (NCCL between GPUs, gloo on CPU tensors), taken by every rank
     in the same order."""
@@ -309,6 +342,64 @@ class DistExchange:
         q.n = total
 
 
+class _PeerTransposes:
+    """The two transposes as stores into the other ranks' buffers
+    (pm_slab_forward_peers_f32, pm_slab_xgreen_peers_f32): `recv[r]` and
+    `rows[r]` are the device addresses of rank r's two transpose buffers;
+    `fence()` separates the phases across the ranks."""
+
+    def forward(self, slabs):
+        self.fence()  # every rank done reading its buffers of the last step
+        for s in slabs:
+            s.forward_peers(self.recv)
+        self.fence()
+
+    def xgreen(self, slabs, c_poisson):
+        for s in slabs:
+            s.xgreen_peers(self.recv[s.rank], c_poisson, self.rows)
+        self.fence()
+
+    def backward(self, slabs):
+        for s in slabs:
+            s.backward_rows(self.rows[s.rank])
+
+
+class LocalPeerExchange(_PeerTransposes, LocalExchange):
+    """LocalExchange with the transposes done by the kernels' stores into the
+    other slabs' buffers (all in one process on one GPU: the slabs' own send
+    / recv buffers; stream order separates the phases)."""
+
+    def __init__(self, slabs):
+        self.recv = [s.recv.data_ptr() for s in slabs]
+        self.rows = [s.send.data_ptr() for s in slabs]
+
+    def fence(self):
+        pass
+
+
+class PeerExchange(_PeerTransposes, DistExchange):
+    """DistExchange with the transposes done by the kernels' stores into the
+    other GPUs' memory: two buffers per rank in torch symmetric memory
+    (peer-mapped; no multicast is used), a host-side barrier (stream
+    synchronize, then dist.barrier) between the phases.  Construct it on
+    every rank at the same point (the rendezvous is collective)."""
+
+    def __init__(self, slab, group=None):
+        DistExchange.__init__(self, group)
+        import torch.distributed._symmetric_memory as symm
+        n = slab.recv.numel()
+        self._bufs = [symm.empty(n, dtype=torch.float32, device=slab.device) for _ in range(2)]
+        grp = group if group is not None else self.dist.group.WORLD
+        hs = [symm.rendezvous(b, grp) for b in self._bufs]
+        self.recv, self.rows = (list(h.buffer_ptrs) for h in hs)
+        self._handles = hs
+        self._stream = slab.stream
+
+    def fence(self):
+        self._stream.synchronize()
+        self.dist.barrier(group=self.group)
+
+
 def step(slabs, parts, exchange, mass: float, c_poisson: float, c_kick: float, dt: float):
     """One PM step of a decomposed mesh: deposit, Poisson solve, gather +
     kick + drift, migration.  `slabs` / `parts` are every slab of the
@@ -316,14 +407,9 @@ def step(slabs, parts, exchange, mass: float, c_poisson: float, c_kick: float, d
     for s, q in zip(slabs, parts):
         s.deposit(q, mass)
     exchange.ghost(slabs)
-    for s in slabs:
-        s.forward()
-    exchange.alltoall(slabs)
-    for s in slabs:
-        s.xgreen(c_poisson)
-    exchange.alltoall(slabs)
-    for s in slabs:
-        s.backward()
+    exchange.forward(slabs)
+    exchange.xgreen(slabs, c_poisson)
+    exchange.backward(slabs)
     exchange.halo(slabs)
     for s, q in zip(slabs, parts):
         s.kick_drift(q, c_kick, dt)

@@ -25,7 +25,7 @@ def _cuda():
         pytest.skip("no CUDA device")
 
 
-def run_pair(pmpkg, ng, nrow, nranks, steps, dt, seed):
+def run_pair(pmpkg, ng, nrow, nranks, steps, dt, seed, peer=False):
     S = pmpkg.slab
     cp, mass = 4 * np.pi, ng ** 3 / nrow ** 3
     pos, vel = pmpkg.zeldovich_ic(ng, nrow, -2.0, 0.5, seed=seed, device=DEV)
@@ -36,7 +36,7 @@ def run_pair(pmpkg, ng, nrow, nranks, steps, dt, seed):
     slabs = [S.Slab(ng, nranks, r, "spectral", 4) for r in range(nranks)]
     parts = S.distribute(cell, off, v, ids, ng, nranks, range(nranks))
     n0 = [q.n for q in parts]
-    ex = S.LocalExchange()
+    ex = S.LocalPeerExchange(slabs) if peer else S.LocalExchange()
     c1, o1, v1 = cell.clone(), [a.clone() for a in off], [a.clone() for a in v]
     for _ in range(steps):
         S.step(slabs, parts, ex, mass, cp, dt, dt)
@@ -47,11 +47,16 @@ def run_pair(pmpkg, ng, nrow, nranks, steps, dt, seed):
     return plan, slabs, parts, n0, (c1, o1, v1), (pos, vel)
 
 
-@pytest.mark.parametrize("ng,nrow,nranks", [(64, 64, 1), (64, 64, 2), (64, 64, 4), (256, 128, 4), (1024, 128, 2)])
-def test_slab_step_matches_single_box(pmpkg, ng, nrow, nranks):
+@pytest.mark.parametrize("ng,nrow,nranks,peer", [(64, 64, 1, False), (64, 64, 2, False), (64, 64, 4, False),
+                                                 (256, 128, 4, False), (1024, 128, 2, False), (64, 64, 1, True),
+                                                 (64, 64, 4, True), (256, 128, 8, True), (1024, 128, 2, True)])
+def test_slab_step_matches_single_box(pmpkg, ng, nrow, nranks, peer):
+    """(peer: the transposes by the kernels' stores into the other slabs'
+    buffers, LocalPeerExchange)"""
     S = pmpkg.slab
     steps, dt = 3, (0.1 if ng <= 64 else 0.05)
-    plan, slabs, parts, n0, (c1, o1, v1), _ = run_pair(pmpkg, ng, nrow, nranks, steps, dt, seed=ng + nranks)
+    plan, slabs, parts, n0, (c1, o1, v1), _ = run_pair(pmpkg, ng, nrow, nranks, steps, dt, seed=ng + nranks,
+                                                       peer=peer)
     phi = torch.cat([s.potential()[:, :, :ng] for s in slabs]).double()
     phi1 = plan.workspace_mesh()[:, :, :ng].double()
     perr = float((phi - phi1).norm() / phi1.norm())
