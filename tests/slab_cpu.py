@@ -90,16 +90,42 @@ class CpuSlab:
     def fold(self, ghost):
         self.buf[2] += ghost
 
-    def forward(self):
-        ng, nx, h = self.ng, self.nx, self.h
+    def _yfwd_rows(self):
+        """y forward of the own planes, as rows [ky][x][kz]."""
+        nx = self.nx
         own = self.buf[2:nx + 2].numpy().view(np.complex128)
         own[:] = np.fft.fft(own, axis=1)
-        self._spec(self.send, (ng, nx, h))[:] = own.transpose(1, 0, 2)
+        return own.transpose(1, 0, 2)
+
+    def forward(self):
+        ng, nx, h = self.ng, self.nx, self.h
+        self._spec(self.send, (ng, nx, h))[:] = self._yfwd_rows()
+
+    def forward_peers(self, peer_recv):
+        """The rows of ky in rank d's range stored into peer_recv[d], block
+        `rank` (the layout the all-to-all would deliver)."""
+        nx, h, p = self.nx, self.h, self.nranks
+        rows = self._yfwd_rows()
+        for d in range(p):
+            self._spec(peer_recv[d], (p, nx, nx, h))[self.rank] = rows[d * nx:(d + 1) * nx]
 
     def xgreen(self, c_poisson):
         ng, nx, h, p = self.ng, self.nx, self.h, self.nranks
+        self._spec(self.send, (p, nx, nx, h))[:] = self._xgreen_lines(self.recv, c_poisson).reshape(
+            nx, p, nx, h).transpose(1, 0, 2, 3)
+
+    def xgreen_peers(self, recv, c_poisson, peer_rows):
+        """x + Green on `recv`; line element kx stored into peer_rows[kx // nx]
+        as row (ky0 + kyl, kx mod nx), i.e. its block `rank`."""
+        nx, h, p = self.nx, self.h, self.nranks
+        x = self._xgreen_lines(recv, c_poisson)
+        for d in range(p):
+            self._spec(peer_rows[d], (p, nx, nx, h))[self.rank] = x[:, d * nx:(d + 1) * nx]
+
+    def _xgreen_lines(self, recv, c_poisson):
+        ng, nx, h, p = self.ng, self.nx, self.h, self.nranks
         nyl = nx
-        r = self._spec(self.recv, (p, nyl, nx, h))
+        r = self._spec(recv, (p, nyl, nx, h))
         x = r.transpose(1, 0, 2, 3).reshape(nyl, ng, h)
         x = np.fft.fft(x, axis=1)
         kx = np.arange(ng)[None, :, None]
@@ -110,12 +136,14 @@ class CpuSlab:
         with np.errstate(divide="ignore", invalid="ignore"):
             g = -c_poisson / (float(ng) ** 3 * w * w * (mx * mx + my * my + kz * kz))
         g[(mx == 0) & (my == 0) & (kz == 0)] = 0.0
-        x = np.fft.ifft(x * g, axis=1) * ng
-        self._spec(self.send, (p, nyl, nx, h))[:] = x.reshape(nyl, p, nx, h).transpose(1, 0, 2, 3)
+        return np.fft.ifft(x * g, axis=1) * ng
 
     def backward(self):
+        self.backward_rows(self.recv)
+
+    def backward_rows(self, rows):
         ng, nx, h = self.ng, self.nx, self.h
-        spec = self._spec(self.recv, (ng, nx, h)).transpose(1, 0, 2)
+        spec = self._spec(rows, (ng, nx, h)).transpose(1, 0, 2)
         spec = np.fft.ifft(spec, axis=1) * ng
         phi = np.fft.irfft(spec, n=ng, axis=2) * ng
         b = self.buf.numpy()

@@ -163,3 +163,62 @@ def test_first_kick_matches_oracle_forces():
     kick = v - np.stack([a.astype(np.float32).astype(np.float64) for a in vel])
     err = np.linalg.norm(kick / DT - np.stack(f)) / np.linalg.norm(np.stack(f))
     assert err < 1e-5, err
+
+
+def _peer_rank(rank, world, port, q, recv, rows):
+    """One rank of the peer-store transposes: its CpuSlab stores into the
+    other rank's buffers (shared-memory tensors standing in for peer-mapped
+    device memory); the exchange's fences are gloo barriers."""
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    _paths()
+    from datetime import timedelta
+    from loader import load_package
+    from slab_cpu import CpuSlab
+    S = load_package().slab
+
+    class SharedPeerExchange(S._PeerTransposes, S.DistExchange):
+        def __init__(self):
+            S.DistExchange.__init__(self)
+            self.recv, self.rows = recv, rows
+
+        def fence(self):
+            self.dist.barrier()
+
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=120))
+    _, _, cell, off, v, ids = initial_state()
+    s = CpuSlab(NG, world, rank)
+    (part,) = S.distribute(cell, off, v, ids, NG, world, [rank])
+    ex = SharedPeerExchange()
+    mass = NG ** 3 / NROW ** 3
+    for _ in range(STEPS):
+        S.step([s], [part], ex, mass, CP, DT, DT)
+    q.put((rank, part.words[:, :part.n].clone().numpy(), s.potential()[:, :, :NG].clone().numpy()))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_peer_store_transposes_on_two_gloo_ranks():
+    """The fused-transpose protocol (slab._PeerTransposes: each rank's y
+    forward and x + Green store straight into the other rank's buffers, fences
+    between the phases) on two processes gives bit for bit the state of the
+    all-to-all transposes."""
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    n = (NG // world) * NG * (NG + 2)
+    recv = [torch.zeros(n, dtype=torch.float64).share_memory_() for _ in range(world)]
+    rows = [torch.zeros(n, dtype=torch.float64).share_memory_() for _ in range(world)]
+    procs = [ctx.Process(target=_peer_rank, args=(r, world, port, q, recv, rows)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = sorted((q.get(timeout=300) for _ in range(world)), key=lambda t: t[0])
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    w = np.concatenate([o[1] for o in out], axis=1)
+    w = w[:, np.argsort(w[7])]
+    phi = np.concatenate([o[2] for o in out])
+    slabs2, parts2 = run_local(2)
+    assert np.array_equal(w, state_by_id(parts2).numpy())
+    assert np.array_equal(phi, potential(slabs2).numpy())
