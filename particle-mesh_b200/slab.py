@@ -20,7 +20,10 @@ torch.distributed (NCCL between GPUs; every rank takes the same collective
 steps in the same order), or ``LocalExchange``, which holds every slab of the
 decomposition in one process and moves the data with device copies (the
 slabs run one after another; nothing waits on another slab's kernel).
-``step`` is written once against both.
+``PeerExchange`` / ``LocalPeerExchange`` replace the two spectrum all-to-alls
+by the FFT passes' own stores into the other ranks' buffers (peer-mapped
+symmetric memory; a barrier between the phases).  ``step`` is written once
+against all of them.
 
 Particles: split positions (cell word, three FP32 offsets), FP32
 velocities, and a 32-bit particle id, held per rank in ``SlabParticles``
