@@ -557,7 +557,10 @@ def ours_slab(args, pm, torch, dist, world, rank, dev, stream, barrier, max_over
     torch.cuda.empty_cache()
     if args.pencil:
         slab = P.Pencil(ng, px, py, rank, "spectral", 4, stream=stream, device=dev)
-        ex = P.DistExchange(px, py) if world > 1 else P.LocalExchange()
+        if args.peer:
+            ex = P.PeerExchange(slab, px, py) if world > 1 else P.LocalPeerExchange([slab])
+        else:
+            ex = P.DistExchange(px, py) if world > 1 else P.LocalExchange()
         step_fn = P.step
     else:
         slab = S.Slab(ng, world, rank, "spectral", 4, stream=stream, device=dev)

@@ -508,6 +508,28 @@ int pm_pencil_migrate_pack(pm_pencil* pencil, void* const* arrays, int narrays, 
 int pm_pencil_migrate_unpack(pm_pencil* pencil, const uint32_t* packed, int64_t n, void* const* arrays,
                              int narrays, int64_t at);
 int pm_pencil_check(pm_pencil* pencil);
+/* Transposes by peer stores (new; the fused form of exchanges B and C): each
+ * pass stores its output blocks straight into the buffers of the group
+ * members that own them -- peer device pointers in member order (y group:
+ * member c = rank rx py + c; x group: member d = rank d py + ry), xfer_floats
+ * floats each, mapped into this process -- at the block the all-to-all would
+ * have filled.  Two such buffers per rank, A and B, alternate:
+ *   pm_pencil_forward_peers_f32   z R2C, kz chunk c into A of y member c
+ *   pm_pencil_yfwd_peers_f32      y forward of `in` (own A); ky chunk d into B
+ *                                 of x member d
+ *   pm_pencil_xgreen_peers_f32    x + Green of `in` (own B); x block d into A
+ *                                 of x member d
+ *   pm_pencil_yinv_peers_f32      y inverse of `in` (own A); y block d into B
+ *                                 of y member d
+ *   pm_pencil_backward_from_f32   z C2R of `in` (own B) into the halo buffer
+ * The caller puts a barrier across the ranks after every store phase (and
+ * before the next step's forward).  At most 16 members per group. */
+int pm_pencil_forward_peers_f32(pm_pencil* pencil, void* const* peer_a, int npeers);
+int pm_pencil_yfwd_peers_f32(pm_pencil* pencil, const void* in, void* const* peer_b, int npeers);
+int pm_pencil_xgreen_peers_f32(pm_pencil* pencil, const void* in, double c_poisson, void* const* peer_a,
+                               int npeers);
+int pm_pencil_yinv_peers_f32(pm_pencil* pencil, const void* in, void* const* peer_b, int npeers);
+int pm_pencil_backward_from_f32(pm_pencil* pencil, const void* in);
 
 /* ---------------------------------------------- initial conditions (new)
  * Zel'dovich particles on an nrow^3 lattice q = (i + 1/2) ng/nrow from a

@@ -102,6 +102,11 @@ SIGNATURES = {
     "pm_pencil_migrate_pack": [_V, _V, _I, _L, _V],
     "pm_pencil_migrate_unpack": [_V, _V, _L, _V, _I, _L],
     "pm_pencil_check": [_V],
+    "pm_pencil_forward_peers_f32": [_V, _V, _I],
+    "pm_pencil_yfwd_peers_f32": [_V, _V, _V, _I],
+    "pm_pencil_xgreen_peers_f32": [_V, _V, _D, _V, _I],
+    "pm_pencil_yinv_peers_f32": [_V, _V, _V, _I],
+    "pm_pencil_backward_from_f32": [_V, _V],
 }
 
 _lib = None

@@ -519,6 +519,7 @@ template <typename T, int N, int TK = tk_cols<T, N>(), int RV = 0> struct Launch
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, +1, TK, RV, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_lines_map<T, N, -1, TK, RV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_lines_map<T, N, -1, TK, RV, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
+        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_lines_map<T, N, +1, TK, RV, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_x_green<T, N, TK, RV, false, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_lines_map<T, N, +1, TK, RV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_x_green<T, N, TK, RV, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
@@ -585,12 +586,26 @@ template <typename T, int N, int TK = tk_cols<T, N>(), int RV = 0> struct Launch
             reinterpret_cast<const C*>(own), nullptr, mi, LineMap{}, H, static_cast<const C*>(p.tw), po);
     }
     static void xgreen_peers(const Plan& p, const T* in, double cg, LineMap m, const PeerMap& po, int planes,
-                             int ky0) {
-        const dim3 grid((H + TK - 1) / TK, planes);
+                             int ncols, int ky0, int kz0) {
+        const dim3 grid((ncols + TK - 1) / TK, planes);
         Timed t(p, ST_FFT_X_GREEN);
         k_fft_x_green<T, N, TK, RV, false, true, true><<<grid, strided_threads<N, TK, RV>(), smem_s(), p.stream>>>(
-            const_cast<C*>(reinterpret_cast<const C*>(in)), H, (long long)N * H, 0, H, static_cast<const C*>(p.tw),
-            static_cast<const T*>(p.g1d), cg, p.green_kind, nullptr, ky0, m, 0, po);
+            const_cast<C*>(reinterpret_cast<const C*>(in)), H, (long long)N * H, 0, ncols,
+            static_cast<const C*>(p.tw), static_cast<const T*>(p.g1d), cg, p.green_kind, nullptr, ky0, m, kz0, po);
+    }
+    // lines read through a line map, stored through a peer map (pencil y passes)
+    static void lines_peers(const Plan& p, const T* in, LineMap mi, const PeerMap& po, int planes, int ncols, int dir,
+                            int stage) {
+        const dim3 grid((ncols + TK - 1) / TK, planes);
+        const C* tw = static_cast<const C*>(p.tw);
+        const C* i = reinterpret_cast<const C*>(in);
+        Timed t(p, stage);
+        if (dir < 0)
+            k_fft_lines_map<T, N, -1, TK, RV, true><<<grid, strided_threads<N, TK, RV>(), smem_s(), p.stream>>>(
+                i, nullptr, mi, LineMap{}, ncols, tw, po);
+        else
+            k_fft_lines_map<T, N, +1, TK, RV, true><<<grid, strided_threads<N, TK, RV>(), smem_s(), p.stream>>>(
+                i, nullptr, mi, LineMap{}, ncols, tw, po);
     }
     // y forward of the nx own planes [x][y][kz] of an x-slab, stored as the
     // rows [ky][x][kz] of its transpose buffer
@@ -905,7 +920,7 @@ int slab_fft_xgreen_peers_f32(const Plan& p, const float* recv, const PeerMap& p
     while ((1 << nxl) < nx) ++nxl;
     const int H = p.ng / 2 + 1;
     const LineMap m{(long long)nx * H, nx * nx * H, H, nxl, nx - 1};
-    PMB_SLAB_LAUNCH(p, L_::xgreen_peers(p, recv, cg, m, po, nx, ky0));
+    PMB_SLAB_LAUNCH(p, L_::xgreen_peers(p, recv, cg, m, po, nx, H, ky0, 0));
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;
 }
@@ -969,6 +984,23 @@ int pencil_xgreen_f32(const Plan& p, const float* in, float* out, LineMap m, int
     if (planes <= 0 || ncols <= 0) return PM_OK;
     const double cg = green_scale(p, c_poisson);
     PMB_SLAB_LAUNCH(p, L_::xgreen_map(p, in, out, cg, m, planes, ncols, ky0, kz0));
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+int pencil_lines_peers_f32(const Plan& p, const float* in, LineMap mi, const PeerMap& po, int planes, int ncols,
+                           int dir, int stage) {
+    if (planes <= 0 || ncols <= 0) return PM_OK;
+    PMB_SLAB_LAUNCH(p, L_::lines_peers(p, in, mi, po, planes, ncols, dir, stage));
+    PMB_CUDA_CHECK(cudaGetLastError());
+    return PM_OK;
+}
+
+int pencil_xgreen_peers_f32(const Plan& p, const float* in, LineMap m, const PeerMap& po, int planes, int ncols,
+                            double c_poisson, int ky0, int kz0) {
+    if (planes <= 0 || ncols <= 0) return PM_OK;
+    const double cg = green_scale(p, c_poisson);
+    PMB_SLAB_LAUNCH(p, L_::xgreen_peers(p, in, cg, m, po, planes, ncols, ky0, kz0));
     PMB_CUDA_CHECK(cudaGetLastError());
     return PM_OK;
 }

@@ -266,6 +266,11 @@ int pencil_lines_f32(const Plan& p, const float* in, float* out, LineMap mi, Lin
 int pencil_xgreen_f32(const Plan& p, const float* in, float* out, LineMap m, int planes, int ncols, double c_poisson,
                       int ky0, int kz0);
 int pencil_z_f32(const Plan& p, float* rows, long long nrows, bool forward);
+// the same passes storing into the other ranks' buffers
+int pencil_lines_peers_f32(const Plan& p, const float* in, LineMap mi, const PeerMap& po, int planes, int ncols,
+                           int dir, int stage);
+int pencil_xgreen_peers_f32(const Plan& p, const float* in, LineMap m, const PeerMap& po, int planes, int ncols,
+                            double c_poisson, int ky0, int kz0);
 int pencil_deposit_f32(const Plan& p, int x0, int y0, int nx, int ny, const uint32_t* cell, const float* ox,
                        const float* oy, const float* oz, int64_t np, float mass, float* buf);
 int pencil_kick_drift_f32(const Plan& p, int x0, int y0, int nx, int ny, const float* buf, uint32_t* cell, float* ox,

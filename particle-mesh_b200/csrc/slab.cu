@@ -505,9 +505,9 @@ int pm_pencil_fold_f32(pm_pencil* pen, const float* xghost, const float* yghost,
     return PM_OK;
 }
 
-int pm_pencil_forward_f32(pm_pencil* pen) {
-    PM_TRY_S(pencil_ok(pen));
-    Pencil& q = pen->q;
+// own rows out of the halo buffer (with the -1 background) and the z R2C;
+// then kz chunk c ([nx][ny][hc(c)]) to dst[c] (row strides ny hc(c), hc(c))
+static int pencil_forward_to(Pencil& q, const std::vector<float2*>& dst) {
     const Plan& p = q.plan->p;
     const long long H = q.h, ny = q.ny, nx = q.nx;
     {
@@ -518,9 +518,16 @@ int pm_pencil_forward_f32(pm_pencil* pen) {
     PM_TRY_S(pencil_z_f32(p, reinterpret_cast<float*>(q.own), nx * ny, true));
     Timed t(p, ST_SORT);
     for (int c = 0; c < q.py; ++c)
-        PM_TRY_S(pencil_copy3(p, q.own + q.kb(c), ny * H, H, q.send + q.yoff(c), ny * q.hc(c), q.hc(c), q.nx, q.ny,
-                              q.hc(c)));
+        PM_TRY_S(pencil_copy3(p, q.own + q.kb(c), ny * H, H, dst[c], ny * q.hc(c), q.hc(c), q.nx, q.ny, q.hc(c)));
     return PM_OK;
+}
+
+int pm_pencil_forward_f32(pm_pencil* pen) {
+    PM_TRY_S(pencil_ok(pen));
+    Pencil& q = pen->q;
+    std::vector<float2*> dst(q.py);
+    for (int c = 0; c < q.py; ++c) dst[c] = q.send + q.yoff(c);
+    return pencil_forward_to(q, dst);
 }
 
 static int log2i(int v) {
@@ -568,20 +575,103 @@ int pm_pencil_yinv_f32(pm_pencil* pen) {
                             kymap(q, hc), ymap(q, hc), q.nx, (int)hc, +1, ST_FFT_Y_INV);
 }
 
-int pm_pencil_backward_f32(pm_pencil* pen) {
-    PM_TRY_S(pencil_ok(pen));
-    Pencil& q = pen->q;
+// the blocks [src kz chunk][nx][ny][hc(src)] of `in` into the own rows, z
+// C2R, the potential into the halo buffer's own rows
+static int pencil_backward_from(Pencil& q, const float2* in) {
     const Plan& p = q.plan->p;
     const long long H = q.h, nx = q.nx, ny = q.ny;
     {
         Timed t(p, ST_SORT);
-        for (int s = 0; s < q.py; ++s)  // [src kz chunk][nx][ny][hc(src)] -> own [nx][ny][H]
-            PM_TRY_S(pencil_copy3(p, q.recv + q.yoff(s), ny * q.hc(s), q.hc(s), q.own + q.kb(s), ny * H, H, q.nx, q.ny,
+        for (int s = 0; s < q.py; ++s)
+            PM_TRY_S(pencil_copy3(p, in + q.yoff(s), ny * q.hc(s), q.hc(s), q.own + q.kb(s), ny * H, H, q.nx, q.ny,
                                   q.hc(s)));
     }
     PM_TRY_S(pencil_z_f32(p, reinterpret_cast<float*>(q.own), nx * ny, false));
     Timed t(p, ST_SORT);
     return pencil_copy3(p, q.own, ny * H, H, q.halo_c() + q.hrow(2, 2), (ny + 5) * H, H, q.nx, q.ny, q.h);
+}
+
+int pm_pencil_backward_f32(pm_pencil* pen) {
+    PM_TRY_S(pencil_ok(pen));
+    return pencil_backward_from(pen->q, pen->q.recv);
+}
+
+// Transposes by peer stores: each pass writes its output blocks straight
+// into the buffers of the group members that own them (peer device
+// pointers in member order), at the block this rank's all-to-all would have
+// filled; `in` is this rank's buffer the previous phase filled.
+static int pencil_peers(const Pencil& q, void* const* peers, int npeers, int want, const long long* block,
+                        long long ps, int s0, int n, PeerMap& po) {
+    if (!peers || npeers != want) return fail(PM_ERR_ARG, "one peer buffer per group member expected");
+    if (npeers > kMaxPeers) return fail(PM_ERR_SIZE, "at most 16 ranks per group for the peer-store transposes");
+    for (int d = 0; d < npeers; ++d) {
+        if (!peers[d]) return fail(PM_ERR_ARG, "NULL peer buffer");
+        po.base[d] = static_cast<float2*>(peers[d]) + block[d];
+    }
+    po.ps = ps;
+    po.s0 = s0;
+    po.sl = log2i(n);
+    po.mask = n - 1;
+    (void)q;
+    return PM_OK;
+}
+
+int pm_pencil_forward_peers_f32(pm_pencil* pen, void* const* peer_a, int npeers) {
+    PM_TRY_S(pencil_ok(pen));
+    Pencil& q = pen->q;
+    if (!peer_a || npeers != q.py) return fail(PM_ERR_ARG, "one peer buffer per y-group member expected");
+    for (int c = 0; c < q.py; ++c)
+        if (!peer_a[c]) return fail(PM_ERR_ARG, "NULL peer buffer");
+    // chunk c to member c, its block ry (blocks of nx ny hc(c))
+    std::vector<float2*> dst(q.py);
+    for (int c = 0; c < q.py; ++c) dst[c] = static_cast<float2*>(peer_a[c]) + (long long)q.ry * q.nx * q.ny * q.hc(c);
+    return pencil_forward_to(q, dst);
+}
+
+int pm_pencil_yfwd_peers_f32(pm_pencil* pen, const void* in, void* const* peer_b, int npeers) {
+    PM_TRY_S(pencil_ok(pen));
+    if (!in) return fail(PM_ERR_ARG, "in is NULL");
+    Pencil& q = pen->q;
+    const long long hc = q.hc(q.ry);
+    // ky chunk d to x-group member d, its block rx ([nx][yc][hc])
+    std::vector<long long> block(q.px, (long long)q.rx * q.nx * q.yc * hc);
+    PeerMap po;
+    PM_TRY_S(pencil_peers(q, peer_b, npeers, q.px, block.data(), q.yc * hc, (int)hc, q.yc, po));
+    return pencil_lines_peers_f32(q.plan->p, static_cast<const float*>(in), ymap(q, hc), po, q.nx, (int)hc, -1,
+                                  ST_FFT_Y_FWD);
+}
+
+int pm_pencil_xgreen_peers_f32(pm_pencil* pen, const void* in, double c_poisson, void* const* peer_a, int npeers) {
+    PM_TRY_S(pencil_ok(pen));
+    if (!in) return fail(PM_ERR_ARG, "in is NULL");
+    Pencil& q = pen->q;
+    const long long hc = q.hc(q.ry);
+    // element kx to x-group member kx / nx, its block rx, at (kx mod nx) yc hc
+    std::vector<long long> block(q.px, (long long)q.rx * q.nx * q.yc * hc);
+    PeerMap po;
+    PM_TRY_S(pencil_peers(q, peer_a, npeers, q.px, block.data(), hc, (int)(q.yc * hc), q.nx, po));
+    const LineMap m{hc, 0, (int)(q.yc * hc), 30, (1 << 30) - 1};
+    return pencil_xgreen_peers_f32(q.plan->p, static_cast<const float*>(in), m, po, q.yc, (int)hc, c_poisson,
+                                   q.rx * q.yc, q.kb(q.ry));
+}
+
+int pm_pencil_yinv_peers_f32(pm_pencil* pen, const void* in, void* const* peer_b, int npeers) {
+    PM_TRY_S(pencil_ok(pen));
+    if (!in) return fail(PM_ERR_ARG, "in is NULL");
+    Pencil& q = pen->q;
+    const long long hc = q.hc(q.ry);
+    // y block d to y-group member d, at its kz chunk ry (complex offset nx ny kb(ry))
+    std::vector<long long> block(q.py, q.yoff(q.ry));
+    PeerMap po;
+    PM_TRY_S(pencil_peers(q, peer_b, npeers, q.py, block.data(), q.ny * hc, (int)hc, q.ny, po));
+    return pencil_lines_peers_f32(q.plan->p, static_cast<const float*>(in), kymap(q, hc), po, q.nx, (int)hc, +1,
+                                  ST_FFT_Y_INV);
+}
+
+int pm_pencil_backward_from_f32(pm_pencil* pen, const void* in) {
+    PM_TRY_S(pencil_ok(pen));
+    if (!in) return fail(PM_ERR_ARG, "in is NULL");
+    return pencil_backward_from(pen->q, static_cast<const float2*>(in));
 }
 
 int pm_pencil_kick_drift_f32(pm_pencil* pen, uint32_t* cell, float* ox, float* oy, float* oz, float* vx, float* vy,

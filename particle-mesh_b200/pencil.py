@@ -19,7 +19,9 @@ The y group of a rank is the py ranks of its rx, the x group the px ranks of
 its ry.  The per-pencil work runs in this package's CUDA kernels
 (``pm_pencil_*`` of the C ABI); the exchanges belong to ``LocalExchange``
 (every pencil in one process, device copies) or ``DistExchange``
-(torch.distributed; NCCL sub-groups for the transposes), as for the slabs.
+(torch.distributed; NCCL sub-groups for the transposes), as for the slabs;
+``PeerExchange`` / ``LocalPeerExchange`` do the four transposes as the FFT
+passes' own stores into the group members' buffers.
 """
 from __future__ import annotations
 
@@ -160,6 +162,28 @@ class Pencil:
     def backward(self):
         check(self.lib.pm_pencil_backward_f32(self._h))
 
+    # transposes by peer stores (pm_pencil_*_peers_f32): peer buffer addresses
+    # in group-member order, `inp` this rank's buffer the last phase filled
+    @staticmethod
+    def _ptrs(ptrs):
+        return (ctypes.c_void_p * len(ptrs))(*ptrs), len(ptrs)
+
+    def forward_peers(self, peer_a):
+        check(self.lib.pm_pencil_forward_peers_f32(self._h, *self._ptrs(peer_a)))
+
+    def yfwd_peers(self, inp: int, peer_b):
+        check(self.lib.pm_pencil_yfwd_peers_f32(self._h, ctypes.c_void_p(inp), *self._ptrs(peer_b)))
+
+    def xgreen_peers(self, inp: int, c_poisson: float, peer_a):
+        check(self.lib.pm_pencil_xgreen_peers_f32(self._h, ctypes.c_void_p(inp), float(c_poisson),
+                                                  *self._ptrs(peer_a)))
+
+    def yinv_peers(self, inp: int, peer_b):
+        check(self.lib.pm_pencil_yinv_peers_f32(self._h, ctypes.c_void_p(inp), *self._ptrs(peer_b)))
+
+    def backward_from(self, inp: int):
+        check(self.lib.pm_pencil_backward_from_f32(self._h, ctypes.c_void_p(inp)))
+
     def kick_drift(self, q: SlabParticles, c_kick: float, dt: float):
         check(self.lib.pm_pencil_kick_drift_f32(self._h, _vp(q.cell), *(_vp(t) for t in q.off),
                                                 *(_vp(t) for t in q.vel), q.n, float(c_kick), float(dt)))
@@ -190,7 +214,74 @@ def _rank(q, rx, ry):
 
 
 # ------------------------------------------------------------------ exchanges
-class LocalExchange(_slab.LocalExchange):
+class _PencilTransposes:
+    """The spectrum passes with the four transposes as all-to-alls of the
+    send / recv buffers in the y and x groups."""
+
+    def forward(self, pens):
+        for p in pens:
+            p.forward()
+        self.ytrans(pens, True)
+
+    def yfwd(self, pens):
+        for p in pens:
+            p.yfwd()
+        self.xtrans(pens)
+
+    def xgreen(self, pens, c_poisson):
+        for p in pens:
+            p.xgreen(c_poisson)
+        self.xtrans(pens)
+
+    def yinv(self, pens):
+        for p in pens:
+            p.yinv()
+        self.ytrans(pens, False)
+
+    def backward(self, pens):
+        for p in pens:
+            p.backward()
+
+
+class _PencilPeerTransposes:
+    """The four transposes as stores into the group members' buffers
+    (pm_pencil_*_peers_f32): `a[r]`, `b[r]` are the device addresses of rank
+    r's two transpose buffers, which alternate between the phases; `fence()`
+    separates the phases across the ranks."""
+
+    def _ygroup(self, q, bufs):
+        return [bufs[q.rx * q.py + c] for c in range(q.py)]
+
+    def _xgroup(self, q, bufs):
+        return [bufs[d * q.py + q.ry] for d in range(q.px)]
+
+    def forward(self, pens):
+        self.fence()  # every rank done with its buffers of the last step
+        for p in pens:
+            p.forward_peers(self._ygroup(p, self.a))
+        self.fence()
+
+    def yfwd(self, pens):
+        for p in pens:
+            p.yfwd_peers(self.a[p.rank], self._xgroup(p, self.b))
+        self.fence()
+
+    def xgreen(self, pens, c_poisson):
+        for p in pens:
+            p.xgreen_peers(self.b[p.rank], c_poisson, self._xgroup(p, self.a))
+        self.fence()
+
+    def yinv(self, pens):
+        for p in pens:
+            p.yinv_peers(self.a[p.rank], self._ygroup(p, self.b))
+        self.fence()
+
+    def backward(self, pens):
+        for p in pens:
+            p.backward_from(self.b[p.rank])
+
+
+class LocalExchange(_PencilTransposes, _slab.LocalExchange):
     """Every pencil of the decomposition in this process (list index = rank);
     the exchanges are device copies, pencil after pencil."""
 
@@ -234,7 +325,7 @@ class LocalExchange(_slab.LocalExchange):
             dn.halo[:, ny + 2:ny + 5].copy_(q.halo[:, 2:5])
 
 
-class DistExchange(_slab.DistExchange):
+class DistExchange(_PencilTransposes, _slab.DistExchange):
     """This process's one pencil; the transposes are all-to-alls in the row
     and column sub-groups, the ghost rows and halo point-to-point messages.
     Every rank must construct it at the same point (new_group is collective)."""
@@ -304,6 +395,41 @@ class DistExchange(_slab.DistExchange):
         b[:, ny + 2:ny + 5].copy_(hi)
 
 
+class LocalPeerExchange(_PencilPeerTransposes, LocalExchange):
+    """LocalExchange with the transposes done by the kernels' stores into the
+    other pencils' buffers (all in one process on one GPU: the pencils' own
+    recv / send buffers as A / B; stream order separates the phases)."""
+
+    def __init__(self, pens):
+        self.a = [p.recv.data_ptr() for p in pens]
+        self.b = [p.send.data_ptr() for p in pens]
+
+    def fence(self):
+        pass
+
+
+class PeerExchange(_PencilPeerTransposes, DistExchange):
+    """DistExchange with the four transposes done by the kernels' stores into
+    the group members' memory: two buffers per rank in torch symmetric memory
+    (peer-mapped; no multicast is used), a host-side barrier between the
+    phases.  Construct it on every rank at the same point (collective)."""
+
+    def __init__(self, pen, px: int, py: int, group=None):
+        DistExchange.__init__(self, px, py, group)
+        import torch.distributed._symmetric_memory as symm
+        n = pen.recv.numel()
+        self._bufs = [symm.empty(n, dtype=torch.float32, device=pen.device) for _ in range(2)]
+        grp = group if group is not None else self.dist.group.WORLD
+        hs = [symm.rendezvous(b, grp) for b in self._bufs]
+        self.a, self.b = (list(h.buffer_ptrs) for h in hs)
+        self._handles = hs
+        self._stream = pen.stream
+
+    def fence(self):
+        self._stream.synchronize()
+        self.dist.barrier(group=self.group)
+
+
 def step(pens, parts, exchange, mass: float, c_poisson: float, c_kick: float, dt: float):
     """One PM step of a pencil-decomposed mesh.  `pens` / `parts` are every
     pencil of the decomposition (LocalExchange) or this rank's one
@@ -311,20 +437,11 @@ def step(pens, parts, exchange, mass: float, c_poisson: float, c_kick: float, dt
     for p, q in zip(pens, parts):
         p.deposit(q, mass)
     exchange.ghost(pens)
-    for p in pens:
-        p.forward()
-    exchange.ytrans(pens, True)
-    for p in pens:
-        p.yfwd()
-    exchange.xtrans(pens)
-    for p in pens:
-        p.xgreen(c_poisson)
-    exchange.xtrans(pens)
-    for p in pens:
-        p.yinv()
-    exchange.ytrans(pens, False)
-    for p in pens:
-        p.backward()
+    exchange.forward(pens)
+    exchange.yfwd(pens)
+    exchange.xgreen(pens, c_poisson)
+    exchange.yinv(pens)
+    exchange.backward(pens)
     exchange.halo(pens)
     for p, q in zip(pens, parts):
         p.kick_drift(q, c_kick, dt)

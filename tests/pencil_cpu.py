@@ -84,22 +84,56 @@ class CpuPencil:
         self.halo[2:self.nx + 2, 2] += yg
         self.halo[2, 2] += corner[0]
 
-    def forward(self):
+    def _zfwd(self):
         nx, ny, ng = self.nx, self.ny, self.ng
         self._own = np.fft.rfft(self.halo.numpy()[2:nx + 2, 2:ny + 2, :ng], axis=2)
+
+    def forward(self):
+        nx, ny = self.nx, self.ny
+        self._zfwd()
         for c in range(self.py):
             self._c(self.send, nx * ny * self.kb(c), (nx, ny, self.hc(c)))[:] = \
                 self._own[:, :, self.kb(c):self.kb(c + 1)]
 
-    def yfwd(self):
+    def forward_peers(self, peer_a):
+        """kz chunk c into peer_a[c] (y member c), block ry."""
+        nx, ny = self.nx, self.ny
+        self._zfwd()
+        for c in range(self.py):
+            self._c(peer_a[c], self.ry * nx * ny * self.hc(c), (nx, ny, self.hc(c)))[:] = \
+                self._own[:, :, self.kb(c):self.kb(c + 1)]
+
+    def _ywork(self, inp):
         nx, ny, ng, hc = self.nx, self.ny, self.ng, self.hc(self.ry)
-        r = self._c(self.recv, 0, (self.py, nx, ny, hc))
-        work = np.fft.fft(r.transpose(1, 0, 2, 3).reshape(nx, ng, hc), axis=1)
+        r = self._c(inp, 0, (self.py, nx, ny, hc))
+        return np.fft.fft(r.transpose(1, 0, 2, 3).reshape(nx, ng, hc), axis=1)
+
+    def yfwd(self):
+        nx, hc = self.nx, self.hc(self.ry)
+        work = self._ywork(self.recv)
         self._c(self.send, 0, (self.px, nx, nx, hc))[:] = work.reshape(nx, self.px, nx, hc).transpose(1, 0, 2, 3)
+
+    def yfwd_peers(self, inp, peer_b):
+        """ky chunk d into peer_b[d] (x member d), block rx."""
+        nx, hc = self.nx, self.hc(self.ry)
+        work = self._ywork(inp)
+        for d in range(self.px):
+            self._c(peer_b[d], self.rx * nx * nx * hc, (nx, nx, hc))[:] = work[:, d * nx:(d + 1) * nx]
 
     def xgreen(self, c_poisson):
         nx, ng, hc = self.nx, self.ng, self.hc(self.ry)
-        x = np.fft.fft(self._c(self.recv, 0, (ng, nx, hc)), axis=0)
+        self._c(self.send, 0, (ng, nx, hc))[:] = self._xlines(self.recv, c_poisson)
+
+    def xgreen_peers(self, inp, c_poisson, peer_a):
+        """x block d into peer_a[d] (x member d), block rx."""
+        nx, hc = self.nx, self.hc(self.ry)
+        x = self._xlines(inp, c_poisson)
+        for d in range(self.px):
+            self._c(peer_a[d], self.rx * nx * nx * hc, (nx, nx, hc))[:] = x[d * nx:(d + 1) * nx]
+
+    def _xlines(self, inp, c_poisson):
+        nx, ng, hc = self.nx, self.ng, self.hc(self.ry)
+        x = np.fft.fft(self._c(inp, 0, (ng, nx, hc)), axis=0)
         kx = np.arange(ng)[:, None, None]
         ky = (self.rx * nx + np.arange(nx))[None, :, None]
         kz = (self.kb(self.ry) + np.arange(hc))[None, None, :]
@@ -108,19 +142,33 @@ class CpuPencil:
         with np.errstate(divide="ignore", invalid="ignore"):
             g = -c_poisson / (float(ng) ** 3 * w * w * (mx * mx + my * my + kz * kz))
         g[(mx == 0) & (my == 0) & (kz == 0)] = 0.0
-        self._c(self.send, 0, (ng, nx, hc))[:] = np.fft.ifft(x * g, axis=0) * ng
+        return np.fft.ifft(x * g, axis=0) * ng
+
+    def _yiwork(self, inp):
+        nx, ng, hc = self.nx, self.ng, self.hc(self.ry)
+        r = self._c(inp, 0, (self.px, nx, nx, hc))
+        return np.fft.ifft(r.transpose(1, 0, 2, 3).reshape(nx, ng, hc), axis=1) * ng
 
     def yinv(self):
-        nx, ny, ng, hc = self.nx, self.ny, self.ng, self.hc(self.ry)
-        r = self._c(self.recv, 0, (self.px, nx, nx, hc))
-        work = np.fft.ifft(r.transpose(1, 0, 2, 3).reshape(nx, ng, hc), axis=1) * ng
+        nx, ny, hc = self.nx, self.ny, self.hc(self.ry)
+        work = self._yiwork(self.recv)
         self._c(self.send, 0, (self.py, nx, ny, hc))[:] = work.reshape(nx, self.py, ny, hc).transpose(1, 0, 2, 3)
 
+    def yinv_peers(self, inp, peer_b):
+        """y block d into peer_b[d] (y member d), at its kz chunk ry."""
+        nx, ny, hc = self.nx, self.ny, self.hc(self.ry)
+        work = self._yiwork(inp)
+        for d in range(self.py):
+            self._c(peer_b[d], nx * ny * self.kb(self.ry), (nx, ny, hc))[:] = work[:, d * ny:(d + 1) * ny]
+
     def backward(self):
+        self.backward_from(self.recv)
+
+    def backward_from(self, inp):
         nx, ny, ng = self.nx, self.ny, self.ng
         own = np.empty((nx, ny, self.h), dtype=np.complex128)
         for s in range(self.py):
-            own[:, :, self.kb(s):self.kb(s + 1)] = self._c(self.recv, nx * ny * self.kb(s), (nx, ny, self.hc(s)))
+            own[:, :, self.kb(s):self.kb(s + 1)] = self._c(inp, nx * ny * self.kb(s), (nx, ny, self.hc(s)))
         b = self.halo.numpy()
         b[2:nx + 2, 2:ny + 2, :ng] = np.fft.irfft(own, n=ng, axis=2) * ng
         b[2:nx + 2, 2:ny + 2, ng:] = 0.0

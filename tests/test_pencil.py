@@ -139,3 +139,69 @@ def test_owner_and_splits():
     assert sum(P.x_splits(q)) <= q.send.numel()
     cell = torch.tensor([(i << 20) | (j << 10) for i, j in ((0, 0), (15, 7), (16, 8), (31, 31))], dtype=torch.int32)
     assert P.owner_of(cell, 32, 2, 4).tolist() == [0, 0, 5, 7]
+
+
+def _peer_rank(rank, world, port, q, px, py, bufs_a, bufs_b):
+    """One rank of the peer-store transposes: its CpuPencil stores into the
+    group members' buffers (shared-memory tensors standing in for peer-mapped
+    device memory); the exchange's fences are gloo barriers."""
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    _paths()
+    from datetime import timedelta
+    from loader import load_package
+    from pencil_cpu import CpuPencil
+    P = load_package().pencil
+
+    class SharedPeerExchange(P._PencilPeerTransposes, P.DistExchange):
+        def __init__(self):
+            P.DistExchange.__init__(self, px, py)
+            self.a, self.b = bufs_a, bufs_b
+
+        def fence(self):
+            self.dist.barrier()
+
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=120))
+    _, _, cell, off, v, ids = initial_state()
+    s = CpuPencil(NG, px, py, rank)
+    (part,) = P.distribute(cell, off, v, ids, NG, px, py, [rank])
+    ex = SharedPeerExchange()
+    mass = NG ** 3 / NROW ** 3
+    for _ in range(STEPS):
+        P.step([s], [part], ex, mass, CP, DT, DT)
+    q.put((rank, part.words[:, :part.n].clone().numpy(), s.potential()[:, :, :NG].clone().numpy()))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_peer_store_transposes_on_four_gloo_ranks():
+    """The pencil's fused-transpose protocol (pencil._PencilPeerTransposes:
+    every pass stores into the group members' buffers, two buffers per rank
+    alternating, fences between the phases) on 2 x 2 processes gives bit for
+    bit the state of the all-to-all transposes."""
+    px, py = 2, 2
+    world = px * py
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    n = _xfer_floats(NG, px, py)
+    bufs_a = [torch.zeros(n, dtype=torch.float64).share_memory_() for _ in range(world)]
+    bufs_b = [torch.zeros(n, dtype=torch.float64).share_memory_() for _ in range(world)]
+    procs = [ctx.Process(target=_peer_rank, args=(r, world, port, q, px, py, bufs_a, bufs_b)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = sorted((q.get(timeout=300) for _ in range(world)), key=lambda t: t[0])
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    w = np.concatenate([o[1] for o in out], axis=1)
+    w = w[:, np.argsort(w[7])]
+    pens2, parts2 = run_local(px, py)
+    assert np.array_equal(w, state_by_id(parts2).numpy())
+    for o, pq in zip(out, pens2):
+        assert np.array_equal(o[2], pq.potential()[:, :, :NG].numpy())
+
+
+def _xfer_floats(ng, px, py):
+    _paths()
+    from pencil_cpu import CpuPencil
+    return CpuPencil(ng, px, py, 0).send.numel()

@@ -24,7 +24,7 @@ def _cuda():
         pytest.skip("no CUDA device")
 
 
-def run_pair(pmpkg, ng, nrow, px, py, steps, dt, seed):
+def run_pair(pmpkg, ng, nrow, px, py, steps, dt, seed, peer=False):
     P = pmpkg.pencil
     cp, mass = 4 * np.pi, ng ** 3 / nrow ** 3
     pos, vel = pmpkg.zeldovich_ic(ng, nrow, -2.0, 0.5, seed=seed, device=DEV)
@@ -35,7 +35,7 @@ def run_pair(pmpkg, ng, nrow, px, py, steps, dt, seed):
     pens = [P.Pencil(ng, px, py, r, "spectral", 4) for r in range(px * py)]
     parts = P.distribute(cell, off, v, ids, ng, px, py, range(px * py), cap_factor=2.0)
     n0 = [q.n for q in parts]
-    ex = P.LocalExchange()
+    ex = P.LocalPeerExchange(pens) if peer else P.LocalExchange()
     c1, o1, v1 = cell.clone(), [a.clone() for a in off], [a.clone() for a in v]
     for _ in range(steps):
         P.step(pens, parts, ex, mass, cp, dt, dt)
@@ -53,12 +53,17 @@ def assemble(pens, ng):
     return phi
 
 
-@pytest.mark.parametrize("ng,nrow,px,py", [(64, 64, 1, 1), (64, 64, 2, 2), (64, 64, 1, 4), (64, 64, 4, 2),
-                                           (256, 128, 2, 4), (512, 128, 2, 2)])
-def test_pencil_step_matches_single_box(pmpkg, ng, nrow, px, py):
+@pytest.mark.parametrize("ng,nrow,px,py,peer", [(64, 64, 1, 1, False), (64, 64, 2, 2, False), (64, 64, 1, 4, False),
+                                                (64, 64, 4, 2, False), (256, 128, 2, 4, False),
+                                                (512, 128, 2, 2, False), (64, 64, 1, 1, True), (64, 64, 2, 2, True),
+                                                (64, 64, 4, 2, True), (256, 128, 2, 4, True), (512, 128, 2, 2, True)])
+def test_pencil_step_matches_single_box(pmpkg, ng, nrow, px, py, peer):
+    """(peer: the transposes by the kernels' stores into the other pencils'
+    buffers, LocalPeerExchange)"""
     P = pmpkg.pencil
     steps, dt = 3, (0.1 if ng <= 64 else 0.05)
-    plan, pens, parts, n0, (c1, o1, v1), _ = run_pair(pmpkg, ng, nrow, px, py, steps, dt, seed=ng + px + 3 * py)
+    plan, pens, parts, n0, (c1, o1, v1), _ = run_pair(pmpkg, ng, nrow, px, py, steps, dt, seed=ng + px + 3 * py,
+                                                      peer=peer)
     phi = assemble(pens, ng)
     phi1 = plan.workspace_mesh()[:, :, :ng].double()
     perr = float((phi - phi1).norm() / phi1.norm())
