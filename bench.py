@@ -155,143 +155,6 @@ def rank_seed(rank: int) -> int:
     return SEED + rank
 
 
-# ------------------------------------------------- end-to-end host copies
-class HostRoundTrip:
-    """Per step: the particle state from pinned host memory to the device,
-    the step, the new state back to the host.  The arrays move in `chunks`
-    particle ranges on two copy streams; a chunk's host-to-device copy waits
-    for the device-to-host copy of the same range in the previous step (the
-    host copy it reads), so every step still moves all of its inputs in and all
-    of its results out, and PCIe carries the two directions at once.
-    serial=True: every copy on the compute stream, one after another."""
-
-    def __init__(self, torch, stream, dev_arrays, host_arrays, chunks: int = 16, serial: bool = False):
-        self.torch, self.stream, self.dev, self.host = torch, stream, dev_arrays, host_arrays
-        self.chunks, self.serial = chunks, serial
-        self.h2d = torch.cuda.Stream(device=stream.device)
-        self.d2h = torch.cuda.Stream(device=stream.device)
-        self.done = []  # (lo, hi, event) of the last step's device-to-host copies
-
-    def _bounds(self, n):
-        return [(n * k // self.chunks, n * (k + 1) // self.chunks) for k in range(self.chunks)]
-
-    def start(self, event):
-        """Copies of the next step start after `event` (the timing start)."""
-        self.h2d.wait_event(event)
-        self.d2h.wait_event(event)
-
-    def step(self, n_in: int, run, n_out=None):
-        """run() advances the state on the compute stream; n_out() the live
-        count after it (particles may migrate); returns the bytes moved."""
-        torch = self.torch
-        if self.serial:
-            with torch.cuda.stream(self.stream):
-                for h, d in zip(self.host, self.dev):
-                    d[:n_in].copy_(h[:n_in], non_blocking=True)
-                run()
-                n = n_out() if n_out else n_in
-                for h, d in zip(self.host, self.dev):
-                    h[:n].copy_(d[:n], non_blocking=True)
-            return n_in, n
-        arrived = []
-        for lo, hi in self._bounds(n_in):
-            with torch.cuda.stream(self.h2d):
-                for dlo, dhi, ev in self.done:
-                    if dlo < hi and lo < dhi:
-                        self.h2d.wait_event(ev)
-                for h, d in zip(self.host, self.dev):
-                    d[lo:hi].copy_(h[lo:hi], non_blocking=True)
-                ev = torch.cuda.Event()
-                ev.record(self.h2d)
-                arrived.append(ev)
-        for ev in arrived:
-            self.stream.wait_event(ev)
-        with torch.cuda.stream(self.stream):
-            run()
-        n = n_out() if n_out else n_in
-        stepped = torch.cuda.Event()
-        stepped.record(self.stream)
-        self.d2h.wait_event(stepped)
-        self.done = []
-        for lo, hi in self._bounds(n):
-            with torch.cuda.stream(self.d2h):
-                for h, d in zip(self.host, self.dev):
-                    h[lo:hi].copy_(d[lo:hi], non_blocking=True)
-                ev = torch.cuda.Event()
-                ev.record(self.d2h)
-                self.done.append((lo, hi, ev))
-        return n_in, n
-
-    def finish(self):
-        """The compute stream waits for the last step's copies (timing end)."""
-        for _, _, ev in self.done:
-            self.stream.wait_event(ev)
-
-
-class SplitRoundTrip:
-    """HostRoundTrip for a step in two calls, potential(positions) then
-    kick_drift(range) per particle range: the positions (cell, offsets) move
-    first and the velocities after them, in both directions, so the velocity
-    upload runs under the potential's kernels and each range's download
-    starts when its gather is done.  Every step still moves all seven words of
-    every particle in and out; a range of a word group goes up only after its
-    download of the step before."""
-
-    def __init__(self, torch, stream, pos_dev, vel_dev, pos_host, vel_host, chunks: int = 16):
-        self.torch, self.stream, self.chunks = torch, stream, chunks
-        self.groups = ((pos_dev, pos_host), (vel_dev, vel_host))
-        self.h2d = torch.cuda.Stream(device=stream.device)
-        self.d2h = torch.cuda.Stream(device=stream.device)
-        self.done = None  # [group][range] events of the last downloads
-
-    def start(self, event):
-        self.h2d.wait_event(event)
-        self.d2h.wait_event(event)
-
-    def _event(self, s):
-        ev = self.torch.cuda.Event()
-        ev.record(s)
-        return ev
-
-    def step(self, n, potential, kick_drift):
-        torch = self.torch
-        rng = [(n * k // self.chunks, n * (k + 1) // self.chunks) for k in range(self.chunks)]
-        up = []
-        for g, (dev, host) in enumerate(self.groups):
-            evs = []
-            for k, (lo, hi) in enumerate(rng):
-                with torch.cuda.stream(self.h2d):
-                    if self.done is not None:
-                        self.h2d.wait_event(self.done[g][k])
-                    for h, d in zip(host, dev):
-                        d[lo:hi].copy_(h[lo:hi], non_blocking=True)
-                    evs.append(self._event(self.h2d))
-            up.append(evs)
-        for ev in up[0]:
-            self.stream.wait_event(ev)
-        with torch.cuda.stream(self.stream):
-            potential()
-        gathered = []
-        for k, (lo, hi) in enumerate(rng):
-            self.stream.wait_event(up[1][k])
-            with torch.cuda.stream(self.stream):
-                kick_drift(lo, hi)
-            gathered.append(self._event(self.stream))
-        self.done = [[], []]
-        for g, (dev, host) in enumerate(self.groups):
-            for k, (lo, hi) in enumerate(rng):
-                with torch.cuda.stream(self.d2h):
-                    self.d2h.wait_event(gathered[k])
-                    for h, d in zip(host, dev):
-                        h[lo:hi].copy_(d[lo:hi], non_blocking=True)
-                    self.done[g].append(self._event(self.d2h))
-
-    def finish(self):
-        for evs in self.done or []:
-            for ev in evs:
-                self.stream.wait_event(ev)
-
-
 # ------------------------------------------------------------- byte model
 def stage_bytes(stage: str, ng: int, np_: int, esz: int) -> float:
     """Algorithmic bytes of one launch of a stage (the minimum it must move).
@@ -624,7 +487,7 @@ def ours_slab(args, pm, torch, dist, world, rank, dev, stream, barrier, max_over
     rows_host = [host[w] for w in range(host.shape[0])]
 
     def e2e_time(serial):
-        trip = HostRoundTrip(torch, stream, rows_dev, rows_host, serial=serial)
+        trip = pm.hostio.HostRoundTrip(stream, rows_dev, rows_host, serial=serial)
 
         def run():
             step_fn([slab], [part], ex, mass, cp, ck, DT)
@@ -955,7 +818,7 @@ def ours(args):
 
         def e2e_time(mode):
             if mode == "split":
-                trip = SplitRoundTrip(torch, stream, dbuf[:4], dbuf[4:], host[:4], host[4:])
+                trip = pm.hostio.SplitRoundTrip(stream, dbuf[:4], dbuf[4:], host[:4], host[4:])
 
                 def one():
                     trip.step(np_, lambda: p32.potential_split(cell, off, mass, cp),
@@ -963,7 +826,7 @@ def ours(args):
                                                                   [a[lo:hi] for a in off], [a[lo:hi] for a in v32],
                                                                   ck, DT))
             else:
-                trip = HostRoundTrip(torch, stream, dbuf, host, serial=mode == "serial")
+                trip = pm.hostio.HostRoundTrip(stream, dbuf, host, serial=mode == "serial")
 
                 def one():
                     trip.step(np_, lambda: p32.step_split(cell, off, v32, mass, cp, ck, DT))

@@ -3,7 +3,7 @@
 The C ABI is include/pm_b200.h (libpm_b200.so, built by build.py); ``pm``
 is the Python host side over it, with the reference's stage names.
 """
-from . import pencil, slab  # noqa: F401
+from . import hostio, pencil, slab  # noqa: F401
 from ._lib import PMError, load  # noqa: F401
 from .pm import (  # noqa: F401
     DA, FFT, OMEGA_0, Ensemble, OMEGA_K, OMEGA_L, OMEGA_M, START_A, Plan, centered_derivatives, cosmo_run,

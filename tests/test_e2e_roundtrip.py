@@ -1,23 +1,18 @@
-"""The bench's end-to-end legs move the particle state between pinned host
-memory and the device every step in particle ranges on two copy streams
-(bench.HostRoundTrip, bench.SplitRoundTrip); a race between a range's upload
-and its download of the step before would corrupt the state without changing
-the timing.  Here both round trips run several steps from the same state as
+"""The pipelined host round trips (hostio.HostRoundTrip, SplitRoundTrip; the
+bench's end-to-end legs) move the particle state between pinned host memory
+and the device every step in particle ranges on two copy streams; a race
+between a range's upload and its download of the step before would corrupt
+the state without changing the timing.  Here both round trips run several steps from the same state as
 plain device stepping (pm_step_f32 on resident arrays), and the host state
 they end with must match it: velocities within 1e-6 relative L2, positions
 within 1e-5 cells (the deposit's shared-memory atomics sum in no fixed
 order).  A range left stale by a race would be off by a whole step.
 """
-import os
-import sys
-
 import numpy as np
 import pytest
 
 torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
-
-ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 @pytest.fixture(scope="module", autouse=True)
@@ -26,16 +21,9 @@ def _cuda():
         pytest.skip("no CUDA device")
 
 
-def _bench():
-    if ROOT not in sys.path:
-        sys.path.insert(0, ROOT)
-    import bench
-    return bench
-
-
 @pytest.mark.parametrize("mode", ["split", "whole", "serial"])
 def test_round_trip_state_matches_resident_steps(pmpkg, mode):
-    B = _bench()
+    B = pmpkg.hostio
     ng, nrow, steps, dt = 256, 128, 4, 0.05
     dev = torch.device("cuda", 0)
     stream = torch.cuda.current_stream(dev)
@@ -55,13 +43,13 @@ def test_round_trip_state_matches_resident_steps(pmpkg, mode):
         d.zero_()
     n = cell.numel()
     if mode == "split":
-        trip = B.SplitRoundTrip(torch, stream, dbuf[:4], dbuf[4:], host[:4], host[4:])
+        trip = B.SplitRoundTrip(stream, dbuf[:4], dbuf[4:], host[:4], host[4:])
         for _ in range(steps):
             trip.step(n, lambda: plan.potential_split(cell, off, mass, cp),
                       lambda lo, hi: plan.kick_drift_split(plan.workspace_mesh(), cell[lo:hi],
                                                            [a[lo:hi] for a in off], [a[lo:hi] for a in v], dt, dt))
     else:
-        trip = B.HostRoundTrip(torch, stream, dbuf, host, serial=mode == "serial")
+        trip = B.HostRoundTrip(stream, dbuf, host, serial=mode == "serial")
         for _ in range(steps):
             trip.step(n, lambda: plan.step_split(cell, off, v, mass, cp, dt, dt))
     trip.finish()
