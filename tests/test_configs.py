@@ -17,7 +17,7 @@ Tolerances (relative L2, written in each assertion):
   FP32 fused step vs FP64: forces 1e-4 (the mixed-precision target);
   FFT: FP64 1e-13, FP32 2e-6.
 The oracle (oracle/pm_oracle.c + numpy.fft, pinned against the compiled
-reference in tests/test_oracle.py) runs on the host of the GPU box.
+reference in tests/test_oracle.py) runs on the host CPU beside the GPU.
 """
 import numpy as np
 import pytest
