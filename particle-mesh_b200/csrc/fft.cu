@@ -258,6 +258,41 @@ __device__ __forceinline__ T green_value(int kx, int ky, int kz, int kind, doubl
     }
 }
 
+// green_value along one x line (fixed ky, kz): the line's two table entries
+// loaded once, every element summed in green_value's order (same results).
+template <typename T> struct GreenLine {
+    using C = typename Cx<T>::t;
+    int ky, kz, kind;
+    double cg;
+    const C* __restrict__ tw;
+    const T* __restrict__ g1d;
+    T gy = 0, gz = 0;
+    __device__ __forceinline__ GreenLine(int ky_, int kz_, int kind_, double cg_, const C* __restrict__ tw_,
+                                         const T* __restrict__ g1d_, bool active)
+        : ky(ky_), kz(kz_), kind(kind_), cg(cg_), tw(tw_), g1d(g1d_) {
+        if (!active) return;
+        if (sizeof(T) == 8 && kind == PM_GREEN_DISCRETE) {
+            gy = (T)__ldg(&tw[ky].x);
+            gz = (T)__ldg(&tw[kz].x);
+        } else {
+            gy = __ldg(g1d + ky);
+            gz = __ldg(g1d + kz);
+        }
+    }
+    __device__ __forceinline__ T operator()(int kx) const {
+        if ((kx | ky | kz) == 0) return (T)0;
+        if constexpr (sizeof(T) == 8) {
+            if (kind == PM_GREEN_DISCRETE) {
+                const double s = ((3.0 - (double)__ldg(&tw[kx].x)) - (double)gy) - (double)gz;
+                return (T)(-cg / (2.0 * s));
+            }
+            return (T)(-cg / (((double)__ldg(g1d + kx) + (double)gy) + (double)gz));
+        } else {
+            return __fdividef((float)(-cg), (__ldg(g1d + kx) + gy) + gz);
+        }
+    }
+};
+
 // Fused x pass of the Poisson solve: forward FFT along x, multiply by G,
 // inverse FFT along x, for TK kz columns of one ky plane.  XT: the lines are
 // written to `out` in the transposed layout [ky][kx][kz] (element stride H),
@@ -309,12 +344,10 @@ k_fft_x_green(typename Cx<T>::t* __restrict__ data, long long es_, long long os_
         },
         [&](int j, int k, C v) { S[I::out1(j, k, tx)] = v; });
     __syncthreads();
+    const GreenLine<T> green(ky, col + kz0, kind, cg, tw, g1d, active);
     stockham_pass2<R1, R2, -1, true, C>(
         ty, p2ld,
-        [&](int j, int k, C v) {
-            S[I::p2(j, k, tx)] =
-                cscale(v, active ? green_value<T>(j + k * R1, ky, col + kz0, kind, cg, tw, g1d) : (T)0);
-        },
+        [&](int j, int k, C v) { S[I::p2(j, k, tx)] = cscale(v, active ? green(j + k * R1) : (T)0); },
         pass2_twiddles<-1, kSplitTw>(tw, ty));
     __syncthreads();
     stockham_pass1<R1, R2, +1, true, C>(
