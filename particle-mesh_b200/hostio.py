@@ -10,10 +10,11 @@ once, and the step itself needs the velocities only at its gather, so:
                   range's upload for the next step waiting only for its own
                   download of this step (serial=True: every copy in order on
                   the compute stream, for comparison)
-  SplitRoundTrip  pm_potential_f32 then pm_kick_drift_f32 by ranges: the
-                  positions go up first, the velocities while the potential
-                  is computed, and each range comes down when its gather is
-                  done
+  SplitRoundTrip  pm_potential_f32 then pm_kick_drift_f32 by ranges (or a
+                  decomposed step's potential part, then its gather and
+                  migration): the positions go up first, the velocities while
+                  the potential is computed, and each range comes down when
+                  its gather is done
 
 Every step still copies all of its inputs in and all of its results out;
 only the overlap changes.  Events order every copy against the kernels and
@@ -97,12 +98,14 @@ class HostRoundTrip:
 
 
 class SplitRoundTrip:
-    """HostRoundTrip for a step in two calls, potential(positions) then
-    kick_drift(range) per particle range: the positions (cell, offsets) move
-    first and the velocities after them, in both directions, so the velocity
-    upload runs under the potential's kernels and each range's download
-    starts when its gather is done.  Every step still moves all seven words of
-    every particle in and out; a range of a word group goes up only after its
+    """HostRoundTrip for a step in two parts: potential(), which reads only the
+    first word group (cell, offsets), then kick_drift(range) per particle
+    range -- or one finish() for a step that also moves particles between
+    ranks.  The first group moves first and the second (velocities, ids)
+    after it, in both directions, so the second group's upload runs under the
+    potential's kernels and, with kick_drift, each range's download starts
+    when its gather is done.  Every step still moves every word of every
+    particle in and out; a range of a word group goes up only after its
     download of the step before."""
 
     def __init__(self, stream, pos_dev, vel_dev, pos_host, vel_host, chunks: int = 16):
@@ -121,7 +124,11 @@ class SplitRoundTrip:
         ev.record(s)
         return ev
 
-    def step(self, n, potential, kick_drift):
+    def step(self, n, potential, kick_drift=None, finish=None, n_out=None):
+        """potential() reads the first word group; then either kick_drift(lo,
+        hi) per range (downloads follow range by range) or finish() once
+        (e.g. gather and particle migration; n_out() gives the live count
+        after it).  Returns (particles copied up, particles copied down)."""
         rng = [(n * k // self.chunks, n * (k + 1) // self.chunks) for k in range(self.chunks)]
         up = []
         for g, (dev, host) in enumerate(self.groups):
@@ -139,11 +146,21 @@ class SplitRoundTrip:
         with torch.cuda.stream(self.stream):
             potential()
         gathered = []
-        for k, (lo, hi) in enumerate(rng):
-            self.stream.wait_event(up[1][k])
+        if finish is None:
+            for k, (lo, hi) in enumerate(rng):
+                self.stream.wait_event(up[1][k])
+                with torch.cuda.stream(self.stream):
+                    kick_drift(lo, hi)
+                gathered.append(self._event(self.stream))
+            n2 = n
+        else:
+            for ev in up[1]:
+                self.stream.wait_event(ev)
             with torch.cuda.stream(self.stream):
-                kick_drift(lo, hi)
-            gathered.append(self._event(self.stream))
+                finish()
+            n2 = n_out() if n_out else n
+            rng = [(n2 * k // self.chunks, n2 * (k + 1) // self.chunks) for k in range(self.chunks)]
+            gathered = [self._event(self.stream)] * self.chunks
         self.done = [[], []]
         for g, (dev, host) in enumerate(self.groups):
             for k, (lo, hi) in enumerate(rng):
@@ -152,6 +169,7 @@ class SplitRoundTrip:
                     for h, d in zip(host, dev):
                         h[lo:hi].copy_(d[lo:hi], non_blocking=True)
                     self.done[g].append(self._event(self.d2h))
+        return n, n2
 
     def finish(self):
         for evs in self.done or []:

@@ -434,6 +434,13 @@ def step(pens, parts, exchange, mass: float, c_poisson: float, c_kick: float, dt
     """One PM step of a pencil-decomposed mesh.  `pens` / `parts` are every
     pencil of the decomposition (LocalExchange) or this rank's one
     (DistExchange)."""
+    step_potential(pens, parts, exchange, mass, c_poisson)
+    step_finish(pens, parts, exchange, c_kick, dt)
+
+
+def step_potential(pens, parts, exchange, mass: float, c_poisson: float):
+    """The first part of `step`: deposit, ghost rows, Poisson solve,
+    potential halo.  Reads only the particles' cell and offset words (0-3)."""
     for p, q in zip(pens, parts):
         p.deposit(q, mass)
     exchange.ghost(pens)
@@ -443,6 +450,10 @@ def step(pens, parts, exchange, mass: float, c_poisson: float, c_kick: float, dt
     exchange.yinv(pens)
     exchange.backward(pens)
     exchange.halo(pens)
+
+
+def step_finish(pens, parts, exchange, c_kick: float, dt: float):
+    """The rest of `step`: gather + kick + drift, migration."""
     for p, q in zip(pens, parts):
         p.kick_drift(q, c_kick, dt)
     exchange.migrate(pens, parts)

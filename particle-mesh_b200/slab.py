@@ -407,6 +407,13 @@ def step(slabs, parts, exchange, mass: float, c_poisson: float, c_kick: float, d
     """One PM step of a decomposed mesh: deposit, Poisson solve, gather +
     kick + drift, migration.  `slabs` / `parts` are every slab of the
     decomposition (LocalExchange) or this rank's one (DistExchange)."""
+    step_potential(slabs, parts, exchange, mass, c_poisson)
+    step_finish(slabs, parts, exchange, c_kick, dt)
+
+
+def step_potential(slabs, parts, exchange, mass: float, c_poisson: float):
+    """The first part of `step`: deposit, ghost fold, Poisson solve, potential
+    halo.  Reads only the particles' cell and offset words (0-3)."""
     for s, q in zip(slabs, parts):
         s.deposit(q, mass)
     exchange.ghost(slabs)
@@ -414,6 +421,10 @@ def step(slabs, parts, exchange, mass: float, c_poisson: float, c_kick: float, d
     exchange.xgreen(slabs, c_poisson)
     exchange.backward(slabs)
     exchange.halo(slabs)
+
+
+def step_finish(slabs, parts, exchange, c_kick: float, dt: float):
+    """The rest of `step`: gather + kick + drift, migration."""
     for s, q in zip(slabs, parts):
         s.kick_drift(q, c_kick, dt)
     exchange.migrate(slabs, parts)

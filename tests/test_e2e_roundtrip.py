@@ -63,3 +63,62 @@ def test_round_trip_state_matches_resident_steps(pmpkg, mode):
     d = max(float((torch.remainder(a - b + ng / 2, ng) - ng / 2).abs().max()) for a, b in zip(xg, xr))
     assert d < 1e-5, d
     plan.close()
+
+
+@pytest.mark.parametrize("decomp", ["slab", "pencil"])
+def test_split_round_trip_of_a_decomposed_step(pmpkg, decomp):
+    """SplitRoundTrip with finish(): a decomposed step at one rank (its
+    potential part, then gather, kick, drift and migration) with the particle
+    words copied up and back every step ends with the state of the same
+    steps on resident words."""
+    ng, nrow, steps, dt = 128, 64, 3, 0.05
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream(dev)
+    mass, cp = ng ** 3 / nrow ** 3, 4 * np.pi
+    D = getattr(pmpkg, decomp)
+    pos, vel = pmpkg.zeldovich_ic(ng, nrow, -1.5, 1.0, seed=13, device="cuda:0")
+    plan = pmpkg.Plan(ng, "fp32", "spectral", 4, stream=stream, device=dev)
+    cell, off = plan.split(*pos)
+    v = [a.float() for a in vel]
+    ids = torch.arange(nrow ** 3, dtype=torch.int32, device=dev)
+
+    def make():
+        if decomp == "slab":
+            dec = D.Slab(ng, 1, 0, "spectral", 4, stream=stream, device=dev)
+            (part,) = D.distribute(cell, off, v, ids, ng, 1, [0])
+            return dec, part, D.DistExchange()
+        dec = D.Pencil(ng, 1, 1, 0, "spectral", 4, stream=stream, device=dev)
+        (part,) = D.distribute(cell, off, v, ids, ng, 1, 1, [0])
+        return dec, part, D.LocalExchange()
+
+    dec_r, part_r, ex_r = make()
+    for _ in range(steps):
+        D.step([dec_r], [part_r], ex_r, mass, cp, dt, dt)
+    dec, part, ex = make()
+    host = torch.empty(part.words.shape, dtype=torch.int32, pin_memory=True)
+    host.copy_(part.words)
+    part.words.zero_()
+    rows_dev = [part.words[w] for w in range(part.words.shape[0])]
+    rows_host = [host[w] for w in range(host.shape[0])]
+    trip = pmpkg.hostio.SplitRoundTrip(stream, rows_dev[:4], rows_dev[4:], rows_host[:4], rows_host[4:])
+    for _ in range(steps):
+        trip.step(part.n, lambda: D.step_potential([dec], [part], ex, mass, cp),
+                  finish=lambda: D.step_finish([dec], [part], ex, dt, dt), n_out=lambda: part.n)
+    trip.finish()
+    torch.cuda.synchronize()
+    dec.check()
+    n = part_r.n
+    assert part.n == n
+    w, wr = host[:, :n].to(dev), part_r.words[:, :n]
+    w, wr = w[:, torch.argsort(w[7])], wr[:, torch.argsort(wr[7])]
+    assert torch.equal(w[7], wr[7])
+    vg, vr = w[4:7].view(torch.float32).double(), wr[4:7].view(torch.float32).double()
+    err = float((vg - vr).norm() / vr.norm())
+    assert err < 1e-6, err
+    xg = plan.join(w[0].contiguous(), [w[1 + a].view(torch.float32).contiguous() for a in range(3)])
+    xr = plan.join(wr[0].contiguous(), [wr[1 + a].view(torch.float32).contiguous() for a in range(3)])
+    d = max(float((torch.remainder(a - b + ng / 2, ng) - ng / 2).abs().max()) for a, b in zip(xg, xr))
+    assert d < 1e-5, d
+    for x in (dec, dec_r):
+        x.close()
+    plan.close()
