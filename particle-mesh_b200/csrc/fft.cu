@@ -152,7 +152,7 @@ template <int N, int TK, int RV = 0> constexpr int strided_smem_elems() { return
 template <typename T, int N, int DIR, int TK, int RV = 0, int AX = -1>
 __global__ void __launch_bounds__(strided_threads<N, TK, RV>(), 2)
 k_fft_strided(typename Cx<T>::t* __restrict__ data, long long es_, long long os_, long long bs, int ncols,
-              const typename Cx<T>::t* __restrict__ tw, typename Cx<T>::t* out) {
+              const typename Cx<T>::t* __restrict__ tw, typename Cx<T>::t* out, PeerMap po = PeerMap{}) {
     using C = typename Cx<T>::t;
     constexpr int R1 = RadixV<N, RV>::R1, R2 = RadixV<N, RV>::R2;
     // AX = 1 (y) or 0 (x): the element and plane strides of the padded
@@ -168,10 +168,12 @@ k_fft_strided(typename Cx<T>::t* __restrict__ data, long long es_, long long os_
     // AX = 4: lines read from `data` at the runtime strides es_, os_ and
     // written along the middle axis of `out` (stride H, planes N H): the
     // x-slab's y inverse pass reading straight from its transpose buffer.
+    // AX = 5: y lines of the planes [x][y][kz] of `data` stored through the
+    // peer map `po` (the x-slab's y forward into the owners' buffers).
     // AX = 0, 1, -1 work in place.
     constexpr long long H = N / 2 + 1;
     constexpr bool OUTER = AX == 0 || AX == 2;
-    constexpr bool MID_IN = AX == 1 || AX == 3, MID_OUT = AX == 2 || AX == 4;
+    constexpr bool MID_IN = AX == 1 || AX == 3 || AX == 5, MID_OUT = AX == 2 || AX == 4;
     const long long es = MID_IN ? H : (OUTER ? (long long)N * H : es_);
     const long long os = MID_IN ? (long long)N * H : (OUTER ? H : os_);
     const long long oes = MID_OUT ? H : (AX == 3 ? es_ : es), oos = MID_OUT ? (long long)N * H : (AX == 3 ? os_ : os);
@@ -193,7 +195,15 @@ k_fft_strided(typename Cx<T>::t* __restrict__ data, long long es_, long long os_
     __syncthreads();
     stockham_pass2<R1, R2, DIR, false, C>(
         ty, [&](int j, int r) { return S[I::p2(j, r, tx)]; },
-        [&](int j, int k, C v) { if (active) obase[j * oes + k * oes2] = v; },
+        [&](int j, int k, C v) {
+            if (!active) return;
+            if constexpr (AX == 5) {
+                const int m = j + k * R1;
+                reinterpret_cast<C*>(po.base[m >> po.sl])[(long long)plane * po.ps + (m & po.mask) * po.s0 + col] = v;
+            } else {
+                obase[j * oes + k * oes2] = v;
+            }
+        },
         pass2_twiddles<DIR, (R2 >= 16 && sizeof(T) == 4)>(tw, ty));
 }
 
@@ -549,6 +559,7 @@ template <typename T, int N, int TK = tk_cols<T, N>(), int RV = 0> struct Launch
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_x_green<T, N, TK, RV, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, +1, TK, RV, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, -1, TK, RV, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
+        PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, -1, TK, RV, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_strided<T, N, +1, TK, RV, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_lines_map<T, N, -1, TK, RV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
         PMB_CUDA_CHECK(cudaFuncSetAttribute(k_fft_lines_map<T, N, -1, TK, RV, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s()));
@@ -613,10 +624,10 @@ template <typename T, int N, int TK = tk_cols<T, N>(), int RV = 0> struct Launch
     // into the rank owning ky (peer map), and x + Green likewise by kx
     static void y_to_peers(const Plan& p, const T* own, const PeerMap& po, int nx) {
         const dim3 grid((H + TK - 1) / TK, nx);
-        const LineMap mi{(long long)N * H, 0, H, 30, (1 << 30) - 1};
         Timed t(p, ST_FFT_Y_FWD);
-        k_fft_lines_map<T, N, -1, TK, RV, true><<<grid, strided_threads<N, TK, RV>(), smem_s(), p.stream>>>(
-            reinterpret_cast<const C*>(own), nullptr, mi, LineMap{}, H, static_cast<const C*>(p.tw), po);
+        k_fft_strided<T, N, -1, TK, RV, 5><<<grid, strided_threads<N, TK, RV>(), smem_s(), p.stream>>>(
+            const_cast<C*>(reinterpret_cast<const C*>(own)), H, (long long)N * H, 0, H, static_cast<const C*>(p.tw),
+            nullptr, po);
     }
     static void xgreen_peers(const Plan& p, const T* in, double cg, LineMap m, const PeerMap& po, int planes,
                              int ncols, int ky0, int kz0) {
