@@ -420,6 +420,7 @@ class PeerExchange(_PencilPeerTransposes, DistExchange):
         n = pen.recv.numel()
         self._bufs = [symm.empty(n, dtype=torch.float32, device=pen.device) for _ in range(2)]
         grp = group if group is not None else self.dist.group.WORLD
+        symm.enable_symm_mem_for_group(grp.group_name)  # (idempotent)
         hs = [symm.rendezvous(b, grp) for b in self._bufs]
         self.a, self.b = (list(h.buffer_ptrs) for h in hs)
         self._handles = hs
