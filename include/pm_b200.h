@@ -421,7 +421,7 @@ int pm_slab_check(pm_slab* slab);
  * forward and the x + Green pass store each output row straight into the
  * buffer of the rank that owns it, through peer device pointers (one per
  * rank, in rank order, each xfer_floats floats and mapped into this
- * process, e.g. symmetric memory), at this rank's block -- the layouts
+ * process, e.g. by pm_ipc_open), at this rank's block -- the layouts
  * exchange B would deliver.  No collective moves the spectrum; the caller
  * puts a barrier across the ranks after each of the two stores (every
  * store done before any rank reads) and before the next step's forward.
@@ -431,6 +431,15 @@ int pm_slab_check(pm_slab* slab);
  *   pm_slab_backward_rows_f32    y inverse from `rows` (this rank's buffer the
  *                                x + Green passes filled), z C2R
  * At most 16 ranks (PM_ERR_SIZE beyond). */
+/* Peer pointers without a collective library: a buffer of this process
+ * (the base of a device allocation, e.g. the `send` / `recv` of
+ * pm_slab_info) exported as an opaque handle of PM_IPC_HANDLE_BYTES bytes,
+ * opened in another process as a device pointer to the same memory (plain
+ * CUDA IPC peer mapping, no multicast), closed when done. */
+#define PM_IPC_HANDLE_BYTES 64
+int pm_ipc_export(const void* dev_ptr, void* handle);
+int pm_ipc_open(const void* handle, void** dev_ptr);
+int pm_ipc_close(void* dev_ptr);
 int pm_slab_forward_peers_f32(pm_slab* slab, void* const* peer_recv, int npeers);
 int pm_slab_xgreen_peers_f32(pm_slab* slab, const void* recv, double c_poisson, void* const* peer_rows,
                              int npeers);

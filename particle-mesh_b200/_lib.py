@@ -15,6 +15,7 @@ PM_OK, PM_ERR_ARG, PM_ERR_SIZE, PM_ERR_CUDA, PM_ERR_NOMEM, PM_ERR_RANGE, PM_ERR_
 PM_FP64, PM_FP32 = 0, 1
 PM_GREEN_DISCRETE, PM_GREEN_SPECTRAL = 0, 1
 PM_GATHER_CACHED, PM_GATHER_TILED = 0, 1
+PM_IPC_HANDLE_BYTES = 64
 
 _STATUS = {PM_ERR_ARG: "PM_ERR_ARG", PM_ERR_SIZE: "PM_ERR_SIZE", PM_ERR_CUDA: "PM_ERR_CUDA",
            PM_ERR_NOMEM: "PM_ERR_NOMEM", PM_ERR_RANGE: "PM_ERR_RANGE", PM_ERR_STATE: "PM_ERR_STATE"}
@@ -83,6 +84,9 @@ SIGNATURES = {
     "pm_slab_migrate_pack": [_V, _V, _I, _L, _V],
     "pm_slab_migrate_unpack": [_V, _V, _L, _V, _I, _L],
     "pm_slab_check": [_V],
+    "pm_ipc_export": [_V, _V],
+    "pm_ipc_open": [_V, ctypes.POINTER(_V)],
+    "pm_ipc_close": [_V],
     "pm_slab_forward_peers_f32": [_V, _V, _I],
     "pm_slab_xgreen_peers_f32": [_V, _V, _D, _V, _I],
     "pm_slab_backward_rows_f32": [_V, _V],

@@ -380,6 +380,33 @@ int pm_slab_migrate_unpack(pm_slab* slab, const uint32_t* packed, int64_t n, voi
     return PM_OK;
 }
 
+// ------------------------------------------------------ CUDA IPC of buffers
+
+int pm_ipc_export(const void* dev_ptr, void* handle) {
+    if (!dev_ptr || !handle) return fail(PM_ERR_ARG, "NULL argument");
+    cudaIpcMemHandle_t h;
+    PMB_CUDA_CHECK(cudaIpcGetMemHandle(&h, const_cast<void*>(dev_ptr)));
+    static_assert(sizeof(h) <= PM_IPC_HANDLE_BYTES, "IPC handle size");
+    std::memset(handle, 0, PM_IPC_HANDLE_BYTES);
+    std::memcpy(handle, &h, sizeof(h));
+    return PM_OK;
+}
+
+int pm_ipc_open(const void* handle, void** dev_ptr) {
+    if (!dev_ptr || !handle) return fail(PM_ERR_ARG, "NULL argument");
+    *dev_ptr = nullptr;
+    cudaIpcMemHandle_t h;
+    std::memcpy(&h, handle, sizeof(h));
+    PMB_CUDA_CHECK(cudaIpcOpenMemHandle(dev_ptr, h, cudaIpcMemLazyEnablePeerAccess));
+    return PM_OK;
+}
+
+int pm_ipc_close(void* dev_ptr) {
+    if (!dev_ptr) return PM_OK;
+    PMB_CUDA_CHECK(cudaIpcCloseMemHandle(dev_ptr));
+    return PM_OK;
+}
+
 int pm_slab_check(pm_slab* slab) {
     if (!slab || !slab->s.plan) return fail(PM_ERR_ARG, "slab is NULL");
     return pm_plan_check(slab->s.plan);

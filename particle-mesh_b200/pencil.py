@@ -410,25 +410,23 @@ class LocalPeerExchange(_PencilPeerTransposes, LocalExchange):
 
 class PeerExchange(_PencilPeerTransposes, DistExchange):
     """DistExchange with the four transposes done by the kernels' stores into
-    the group members' memory: two buffers per rank in torch symmetric memory
-    (peer-mapped; no multicast is used), a host-side barrier between the
-    phases.  Construct it on every rank at the same point (collective)."""
+    the group members' memory: every rank's own recv / send buffers (A / B)
+    mapped into every process by CUDA IPC (slab.PeerBuffers; no multicast),
+    a host-side barrier between the phases.  Construct it on every rank at
+    the same point (collective)."""
 
     def __init__(self, pen, px: int, py: int, group=None):
         DistExchange.__init__(self, px, py, group)
-        import torch.distributed._symmetric_memory as symm
-        n = pen.recv.numel()
-        self._bufs = [symm.empty(n, dtype=torch.float32, device=pen.device) for _ in range(2)]
-        grp = group if group is not None else self.dist.group.WORLD
-        symm.enable_symm_mem_for_group(grp.group_name)  # (idempotent)
-        hs = [symm.rendezvous(b, grp) for b in self._bufs]
-        self.a, self.b = (list(h.buffer_ptrs) for h in hs)
-        self._handles = hs
+        self._peers = _slab.PeerBuffers(pen.lib, self.dist, group, [pen.recv, pen.send])
+        self.a, self.b = self._peers.ptrs
         self._stream = pen.stream
 
     def fence(self):
         self._stream.synchronize()
         self.dist.barrier(group=self.group)
+
+    def close(self):
+        self._peers.close()
 
 
 def step(pens, parts, exchange, mass: float, c_poisson: float, c_kick: float, dt: float):

@@ -21,8 +21,8 @@ steps in the same order), or ``LocalExchange``, which holds every slab of the
 decomposition in one process and moves the data with device copies (the
 slabs run one after another; nothing waits on another slab's kernel).
 ``PeerExchange`` / ``LocalPeerExchange`` replace the two spectrum all-to-alls
-by the FFT passes' own stores into the other ranks' buffers (peer-mapped
-symmetric memory; a barrier between the phases).  ``step`` is written once
+by the FFT passes' own stores into the other ranks' buffers (mapped by CUDA
+IPC; a barrier between the phases).  ``step`` is written once
 against all of them.
 
 Particles: split positions (cell word, three FP32 offsets), FP32
@@ -380,28 +380,68 @@ class LocalPeerExchange(_PeerTransposes, LocalExchange):
         pass
 
 
+class PeerBuffers:
+    """Every rank's copies of some of its own device buffers, mapped into this
+    process: each rank exports its buffers with CUDA IPC (pm_ipc_export), the
+    handles travel by all_gather_object, and each rank opens the others'
+    (pm_ipc_open; its own by address).  Plain peer mappings: no multicast
+    object is bound to the memory.  `ptrs[b][r]` is buffer b of rank r.
+    Collective: every rank of the group constructs it at the same point."""
+
+    def __init__(self, lib, dist, group, buffers):
+        self.lib, self._opened = lib, []
+        handles = []
+        for t in buffers:
+            h = ctypes.create_string_buffer(L.PM_IPC_HANDLE_BYTES)
+            check(lib.pm_ipc_export(ctypes.c_void_p(t.data_ptr()), h))
+            handles.append(h.raw)
+        world = dist.get_world_size(group)
+        me = dist.get_rank(group)
+        allh = [None] * world
+        dist.all_gather_object(allh, handles, group=group)
+        self.ptrs = [[0] * world for _ in buffers]
+        for r in range(world):
+            for b, t in enumerate(buffers):
+                if r == me:
+                    self.ptrs[b][r] = t.data_ptr()
+                else:
+                    p = ctypes.c_void_p()
+                    check(lib.pm_ipc_open(ctypes.create_string_buffer(allh[r][b], L.PM_IPC_HANDLE_BYTES),
+                                          ctypes.byref(p)))
+                    self._opened.append(p)
+                    self.ptrs[b][r] = p.value
+
+    def close(self):
+        for p in self._opened:
+            self.lib.pm_ipc_close(p)
+        self._opened = []
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001
+            pass
+
+
 class PeerExchange(_PeerTransposes, DistExchange):
     """DistExchange with the transposes done by the kernels' stores into the
-    other GPUs' memory: two buffers per rank in torch symmetric memory
-    (peer-mapped; no multicast is used), a host-side barrier (stream
-    synchronize, then dist.barrier) between the phases.  Construct it on
-    every rank at the same point (the rendezvous is collective)."""
+    other GPUs' memory: every rank's own send / recv buffers mapped into
+    every process by CUDA IPC (PeerBuffers; no multicast), a host-side
+    barrier (stream synchronize, then dist.barrier) between the phases.
+    Construct it on every rank at the same point (collective)."""
 
     def __init__(self, slab, group=None):
         DistExchange.__init__(self, group)
-        import torch.distributed._symmetric_memory as symm
-        n = slab.recv.numel()
-        self._bufs = [symm.empty(n, dtype=torch.float32, device=slab.device) for _ in range(2)]
-        grp = group if group is not None else self.dist.group.WORLD
-        symm.enable_symm_mem_for_group(grp.group_name)  # (idempotent)
-        hs = [symm.rendezvous(b, grp) for b in self._bufs]
-        self.recv, self.rows = (list(h.buffer_ptrs) for h in hs)
-        self._handles = hs
+        self._peers = PeerBuffers(slab.lib, self.dist, group, [slab.recv, slab.send])
+        self.recv, self.rows = self._peers.ptrs
         self._stream = slab.stream
 
     def fence(self):
         self._stream.synchronize()
         self.dist.barrier(group=self.group)
+
+    def close(self):
+        self._peers.close()
 
 
 def step(slabs, parts, exchange, mass: float, c_poisson: float, c_kick: float, dt: float):
